@@ -1,0 +1,325 @@
+"""Benchmark of the D2Q9 step: MLUPS and HBM GB/s on the 4096 x 1024 channel
+with one IB cylinder (D = 128, Re 3900), MRT + Smagorinsky (Cs 0.1), FP32.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1); every rank runs an independent
+replica of the lattice (the step does not shard: one domain per GPU), so the
+whole-job value is the sum over ranks and scaling is weak.  Timing: W untimed
+steps, then exactly K steps between a barrier + synchronize on both sides,
+CUDA events on the library's stream, max over ranks.  The populations
+(2 x 151 MB) exceed the 126 MB L2, so no flush is needed between steps.
+
+Keys beyond the base contract:
+  e2e           the same metric through the C ABI with host buffers: initial
+                fields uploaded from pinned host memory, per-step ippi_step +
+                ippi_forces (force read back), final velocity downloaded
+  roofline      bulk stream-collide kernel: 72 algorithmic bytes per node
+                (9 loads + 9 stores of FP32) / its CUDA-event launch time
+  cpu_baseline  the reference's own MRT+Smagorinsky step (compiled from its
+                sources, SINGLE precision) on the same grid, all host cores
+--impl reference runs only that CPU reference arm (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(
+    REPO, "machine-learning-based-implicit-physical-parametric-inference-for-cfd-simulation-promotion_b200")
+sys.path.insert(0, PKG)
+
+NX, NY = 4096, 1024
+BYTES_PER_NODE = 72  # FP32: 9 loads + 9 stores
+METRIC = "MLUPS"
+WORKLOAD = "channel_cylinder_4096x1024_mrt_smagorinsky_ib_fp32"
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for s in self.samples for n, v in zip(names, s[3:7]) if v == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (reference arm and cpu_baseline)
+# ---------------------------------------------------------------------------
+def cpu_reference(steps, warmup, max_seconds=None):
+    """Time the reference's MRT + Smagorinsky step (its own sources compiled by
+    oracle/build_ref.sh, SINGLE precision, flat-plate scene, one MPI rank per
+    host core as threads) on the NX x NY grid.  Falls back to the FP64 oracle
+    port when the reference build is absent.  Returns (MLUPS, info)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pyoracle as po
+
+    cores = os.cpu_count() or 1
+    tau = 0.5 + 3 * 0.04 * 128 / 3900
+    if po.ref_available("mrt_f32"):
+        sim = po.RefSim(NX, NY, tau=tau, cs=0.1, u_in=0.04, ranks=cores, variant="mrt_f32")
+        kind, desc = "reference", "reference MRT+Smagorinsky (SINGLE) flat plate"
+    else:
+        po.build_oracle()
+        sim = po.Oracle(NX, NY, collision=po.MRT, tau0=tau, cs=0.1, u_in=0.04)
+        cores = 1
+        kind, desc = "port", "FP64 oracle port MRT+Smagorinsky flat plate"
+    if warmup:
+        sim.step(warmup, 1)
+    t0 = time.perf_counter()
+    done = 0
+    while done < steps:
+        sim.step(1, warmup + done + 1)
+        done += 1
+        if max_seconds and time.perf_counter() - t0 > max_seconds:
+            break
+    dt = time.perf_counter() - t0
+    mlups = NX * NY * done / dt / 1e6
+    return mlups, dict(kind=kind, cores=cores, steps=done, seconds=dt,
+                       sample=f"{done} steps of {NX}x{NY} ({desc}), {cores} threads")
+
+
+def run_reference_arm(a):
+    rank, _, world = env_rank()
+    if rank != 0:
+        return
+    mlups, info = cpu_reference(a.steps, a.warmup, max_seconds=240)
+    line = {"metric": METRIC, "value": round(mlups, 3), "unit": "MLUPS", "n_gpus": a.gpus,
+            "steps": info["steps"], "warmup": a.warmup,
+            "ms_per_step": round(info["seconds"] / max(info["steps"], 1) * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "nx": NX, "ny": NY, "grid_nodes": NX * NY,
+                       "reference_scene": "flat plate (the reference has no cylinder/IB scene)"},
+            "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": info["cores"],
+                             "kind": info["kind"], "sample": info["sample"]},
+            "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(a):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import ippi_lbm as ip
+
+    rank, local, world = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    sc = ip.scenes.config2()
+    lat = ip.Lattice(NX, NY, device=local, **sc["params"])
+    lat.init_macros(*sc["init"])
+    lat.set_markers(sc["markers"], ds=sc["ds"])
+    stream = torch.cuda.ExternalStream(lat.stream(), device=torch.device("cuda", local))
+
+    # warm-up (also builds the CUDA graphs)
+    lat.step(max(a.warmup, 3), 1)
+    t_next = max(a.warmup, 3) + 1
+
+    # ---- device-resident throughput ---------------------------------------
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        lat.step(a.steps, t_next)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    t_next += a.steps
+    barrier()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = NX * NY * a.steps * world / (ms_max * 1e-3) / 1e6
+
+    # ---- roofline: bulk kernel launch time (per-launch CUDA events) --------
+    nprof = min(max(a.steps // 2, 20), 200)
+    ms_bulk, ms_band, ms_ib = lat.profile_steps(nprof, t_next)
+    t_next += nprof
+    hbm, peak_kind = peaks()
+    achieved = NX * NY * BYTES_PER_NODE / (ms_bulk * 1e-3) / 1e9
+
+    # ---- end to end through the C ABI with host buffers --------------------
+    n_e2e = min(a.steps, 100)
+    rho0, ux0, uy0 = (np.ascontiguousarray(x) for x in sc["init"])
+    pin = [torch.from_numpy(x).pin_memory().numpy() for x in (rho0, ux0, uy0)]
+    fxy = np.zeros(2)
+    nb = C.c_int(0)
+    L = ip.lib()
+    out_u = torch.empty((NY, NX), dtype=torch.float64).pin_memory().numpy()
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    lat.init_macros(*pin)
+    for s in range(n_e2e):
+        rc = L.ippi_step(lat.handle, 1, s + 1)
+        if rc:
+            ip._lib.check(rc, lat.handle)
+        L.ippi_forces(lat.handle, fxy.ctypes.data_as(C.POINTER(C.c_double)), C.byref(nb), None)
+    L.ippi_download(lat.handle, ip.FIELD_UX, out_u.ctypes.data_as(C.c_void_p), out_u.nbytes)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = NX * NY * n_e2e * world / e2e_s / 1e6
+    h2d = (rho0.nbytes + ux0.nbytes + uy0.nbytes) / n_e2e
+    d2h = (16 * n_e2e + 4 * n_e2e + out_u.nbytes) / n_e2e
+
+    cd, cl = ip.scenes.drag_lift(fxy, sc["d"], sc["u_ref"])
+    if rank == 0:
+        cpu = None
+        if world == 1 and not a.no_cpu:
+            mlups_cpu, info = cpu_reference(a.cpu_steps, 1, max_seconds=30)
+            cpu = {"value": round(mlups_cpu, 3), "unit": "MLUPS", "cores": info["cores"],
+                   "kind": info["kind"], "sample": info["sample"]}
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nx": NX, "ny": NY, "collision": "MRT",
+                       "les": "smagorinsky_cs0.1", "cylinder_d": 128, "markers": len(sc["ds"]),
+                       "re": 3900, "u_max": 0.04, "storage": "f32",
+                       "l2": "inputs larger than L2 (2 x 151 MB populations)",
+                       "parallelism": f"replicas{world}"},
+            "hbm_gbs": round(value * BYTES_PER_NODE / 1e3 / world, 1),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
+                         "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
+                         "peak_source": peak_kind, "kernel": "step_kernel<F32,MRT,CHANNEL>",
+                         "kernel_ms": round(ms_bulk, 5), "band_ms": round(ms_band, 5),
+                         "ib_ms": round(ms_ib, 5), "bytes_per_node": BYTES_PER_NODE},
+            "e2e": {"value": round(e2e, 1), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d),
+                    "d2h_bytes_per_step": round(d2h), "steps": n_e2e},
+            "gpu_launches": a.steps * 2,
+            "clocks": clk.summary(),
+            "cd_cl": [round(float(cd[0]), 5), round(float(cl[0]), 5)],
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    lat.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_ncu_case(a):
+    """The command profiled by ncu: the benchmark lattice, `steps` single
+    (non-graph) steps, so each launch of every kernel is a separate entry."""
+    import ippi_lbm as ip
+
+    sc = ip.scenes.config2()
+    lat = ip.Lattice(NX, NY, **sc["params"])
+    lat.init_macros(*sc["init"])
+    lat.set_markers(sc["markers"], ds=sc["ds"])
+    for s in range(a.steps):
+        lat.profile_steps(1, s + 1)
+    lat.close()
+    print(json.dumps({"ncu_case": WORKLOAD, "steps": a.steps}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=20)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="short run of single launches for an ncu capture")
+    a = ap.parse_args()
+    if a.ncu_case:
+        run_ncu_case(a)
+    elif a.impl == "reference":
+        run_reference_arm(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

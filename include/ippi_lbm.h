@@ -1,0 +1,178 @@
+/*
+ * ippi_lbm.h -- C ABI of the B200 D2Q9 time step (libippi_lbm.so).
+ *
+ * The reference (IPPI-LBM) has no plugin or FFI: its boundary is the C++
+ * class API that main.cpp calls.  These entry points are what that API's
+ * methods bind to in the drop-in host layer (host/mesh.cpp):
+ *
+ *   ippi_create        Mesh::InitialLatMesh + Mesh::JudgeStyle
+ *                      (mesh.cpp:60-171, 1391-1454); Parameter.h switches
+ *                      (Parameter.h:8-21) and main.cpp constants (main.cpp:12-65)
+ *                      become ippi_params fields
+ *   ippi_init_macros   Lattice::InitialLatticeFeq over the mesh
+ *                      (NodeAndLattice.cpp:69-123; mesh.cpp:159-166), and the
+ *                      field reset of Mesh::ManageDataFromXflow (mesh.cpp:2189)
+ *   ippi_set_markers   Mesh::InitialIBParticle (mesh.cpp:173-191) -- the IB
+ *                      sub-step InterpolateVel / CalParticleForce / SpreadForce /
+ *                      UpdateVelocity (mesh.cpp:552, 514, 656, 1244) then runs
+ *                      inside every ippi_step
+ *   ippi_load_band_net the model loads of Mesh::NNmodel_Type00..07
+ *                      (mesh.cpp:2767-3259): weights once, not per call
+ *   ippi_step          Mesh::OneLBMStep (mesh.cpp:357-513) followed by
+ *                      Mesh::ComputeAvgVelocity (mesh.cpp:1954-1974), nsteps times
+ *   ippi_download      the LatMesh fields read by Mesh::WriteDatFluid
+ *                      (mesh.cpp:1180-1243) and the flags of JudgeStyle
+ *   ippi_forces        the marker force sums of Mesh::OutputCd's role
+ *                      (mesh.cpp:1461-1526), from the IB marker forces, FP64
+ *   ippi_last_error    cerr messages of the reference (e.g. ErrorCatch,
+ *                      mesh.cpp:2101-2111, which called MPI_Abort)
+ *
+ * Conventions: every call returns IPPI_OK (0) or a negative IPPI_ERR_* code
+ * and never throws.  A handle owns all of its device memory and one CUDA
+ * stream; host pointers are borrowed for the duration of the call.  A handle
+ * is not thread-safe.  Arrays on the lattice are row-major [ny][nx] (x
+ * fastest); populations are [9][ny][nx] in the reference's D2Q9 order
+ * (0 rest, 1 E, 2 N, 3 W, 4 S, 5 NE, 6 NW, 7 SW, 8 SE).
+ */
+#ifndef IPPI_LBM_H
+#define IPPI_LBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IPPI_ABI_VERSION 1
+
+/* status codes */
+#define IPPI_OK 0
+#define IPPI_ERR_ARG (-1)      /* bad argument (sizes, enum values, tau <= 0.5) */
+#define IPPI_ERR_CUDA (-2)     /* a CUDA call failed; see ippi_last_error       */
+#define IPPI_ERR_DIVERGED (-3) /* rho left [0,10] or became NaN (ErrorCatch)    */
+#define IPPI_ERR_STATE (-4)    /* call not valid in the handle's current state  */
+#define IPPI_ERR_NOMEM (-5)    /* device allocation failed                      */
+
+/* collision operator (Parameter.h SRTLBM / MRT / RRLBM) */
+#define IPPI_BGK 0
+#define IPPI_MRT 1
+#define IPPI_RR 2
+/* population storage; arithmetic is FP64 for IPPI_F64, FP32 otherwise, on
+ * populations shifted by w_k * rho0 */
+#define IPPI_F64 0
+#define IPPI_F32 1
+#define IPPI_F16 2
+#define IPPI_BF16 3
+/* boundary set */
+#define IPPI_BC_REF_NEE 0   /* the reference's flat-plate scene (mesh.cpp:228-356) */
+#define IPPI_BC_CHANNEL 1   /* Zou-He parabolic inlet, NEE outlet, bounce-back walls */
+/* subgrid model */
+#define IPPI_LES_NONE 0
+#define IPPI_LES_SMAGORINSKY 1 /* SmagorinskyByHybrid, mesh.cpp:852-911 */
+/* IB interpolation/spreading kernel */
+#define IPPI_DELTA_BILINEAR 0 /* mesh.cpp:606-644 (default of Parameter.h) */
+#define IPPI_DELTA_PESKIN4 1  /* Dirac_Delta, mesh.cpp:555-605, 1354-1389 */
+
+/* fields for ippi_download */
+#define IPPI_FIELD_F 0       /* fnew after the last step, double [9][ny][nx]   */
+#define IPPI_FIELD_RHO 1     /* double [ny][nx]                                 */
+#define IPPI_FIELD_UX 2
+#define IPPI_FIELD_UY 3
+#define IPPI_FIELD_TAU 4     /* relaxation time the next collision uses        */
+#define IPPI_FIELD_AVG_U 5   /* time averages of ComputeAvgVelocity            */
+#define IPPI_FIELD_AVG_V 6
+#define IPPI_FIELD_AVG_RHO 7
+#define IPPI_FIELD_FLAGS 8   /* uint8 [ny][nx]: JudgeStyle chars f i o m d u (w) */
+#define IPPI_FIELD_NNFLAG 9  /* double [ny][nx]: 1 where a boundary net sets tau */
+
+typedef struct ippi_lbm ippi_lbm;
+
+typedef struct {
+    int nx, ny;          /* lattice (main.cpp:20-21 Nx, Ny)                   */
+    int collision;       /* IPPI_BGK / IPPI_MRT / IPPI_RR                     */
+    int storage;         /* IPPI_F64 / IPPI_F32 / IPPI_F16 / IPPI_BF16        */
+    int bc_set;          /* IPPI_BC_REF_NEE / IPPI_BC_CHANNEL                 */
+    int les_model;       /* IPPI_LES_NONE / IPPI_LES_SMAGORINSKY              */
+    double tau0;         /* startTau (main.cpp:43)                            */
+    double cs;           /* Smagorinsky constant (main.cpp:12)                */
+    double u_in;         /* flat plate: inlet velocity (mesh.cpp:244 uses 0.1);
+                            channel: centre-line velocity u_max               */
+    double rho0;         /* reference density and population shift (1.0)    */
+    int plate_x0;        /* flat plate: specular bottom for x < plate_x0
+                            (mesh.cpp:1413 uses 400)                          */
+    int avg_start;       /* startAvg (main.cpp:54)                            */
+    int delta_kernel;    /* IPPI_DELTA_BILINEAR / IPPI_DELTA_PESKIN4          */
+    int mdf_iters;       /* direct-forcing passes per step, >= 1              */
+    int device;          /* CUDA device ordinal                               */
+} ippi_params;
+
+/* ABI version of the loaded library (IPPI_ABI_VERSION). */
+int ippi_abi_version(void);
+
+/* Fill *p with the reference's defaults: BGK, F64, flat plate, Smagorinsky,
+ * tau0 from main.cpp:43 for the given size, cs 0.173, u_in 0.1, rho0 1,
+ * plate_x0 400, avg_start 30000, bilinear delta, one forcing pass. */
+void ippi_params_default(ippi_params* p, int nx, int ny);
+
+/* Create a lattice (flags, buffers, stream) initialised to rho = 1, u = 0. */
+int ippi_create(const ippi_params* p, ippi_lbm** out);
+int ippi_destroy(ippi_lbm* h);
+
+/* Set rho/u on every node and the populations to their equilibrium
+ * (InitialLatticeFeq).  NULL arrays mean rho = 1 / u = 0.  Resets averages. */
+int ippi_init_macros(ippi_lbm* h, const double* rho, const double* ux, const double* uy);
+
+/* Immersed-boundary markers: positions xy[2n], prescribed velocities ub[2n]
+ * (NULL = at rest), body id per marker body[n] (NULL = all 0), arc length per
+ * marker ds[n] (NULL = 1, the reference's force omits the area factor,
+ * mesh.cpp:527).  Every stencil node must lie at least 3 nodes inside the
+ * lattice.  n = 0 removes the markers. */
+int ippi_set_markers(ippi_lbm* h, int n, const double* xy, const double* ub,
+                     const int* body, const double* ds);
+
+/* Weights of boundary net `type` (0..7) in TorchScript parameter order of
+ * NNmodel/AutoT0<type>.pt: hidden_layer1 weight[128][nin], bias[128],
+ * hidden_layer2..7 weight[128][128], bias[128], output_layer weight[1][128],
+ * bias[1]; nin = 15 for types 1, 3, 5, 7 and 9 for 0, 2, 4, 6.  The nets act
+ * with the BGK operator only, as in the reference. */
+int ippi_load_band_net(ippi_lbm* h, int type, const float* w, size_t n);
+
+/* Advance nsteps time steps numbered t0, t0+1, ... (t feeds the averages,
+ * mesh.cpp:1958-1971).  Returns IPPI_ERR_DIVERGED if rho left [0,10] or became
+ * NaN in any of them.  Synchronises the handle's stream. */
+int ippi_step(ippi_lbm* h, int nsteps, int t0);
+
+/* Copy a field to host memory; bytes must equal the field's size. */
+int ippi_download(ippi_lbm* h, int field, void* host, size_t bytes);
+
+/* Force on each body (lattice units, FP64, computed by the IB sub-step on the
+ * current velocity field): force_xy[2 * nbody] = (Fx, Fy); *nbody receives
+ * the body count (may be NULL).  mass (may be NULL) receives sum(rho) over
+ * the lattice in FP64. */
+int ippi_forces(ippi_lbm* h, double* force_xy, int* nbody, double* mass);
+
+/* Per-step body forces recorded by the IB sub-step: out[step][body][2] for
+ * the last min(max_steps, recorded) steps; returns the number of steps
+ * written (>= 0) or an error code. */
+int ippi_force_history(ippi_lbm* h, double* out, int max_steps);
+
+/* The CUDA stream the handle launches on (a cudaStream_t), for event timing. */
+int ippi_get_stream(ippi_lbm* h, void** stream);
+
+/* Device timing of `nsteps` steps launched one by one with CUDA events around
+ * each launch: average milliseconds of the bulk stream-collide kernel, and of
+ * the side-stream chain (prep + boundary nets, or prep + IB) that runs
+ * concurrently with it, reported in ms_band when nets are active and in
+ * ms_ib when markers are (0 when absent).  Advances the simulation like
+ * ippi_step. */
+int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk,
+                       double* ms_band, double* ms_ib);
+
+/* Last error message of the handle (or of the library when h is NULL). */
+int ippi_last_error(ippi_lbm* h, char* buf, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1146 @@
+// ippi_lbm.cu -- the C ABI of include/ippi_lbm.h: lattice handle, device
+// buffers, side-buffer tables for the boundary nets and the immersed
+// boundary, step launches captured in CUDA graphs, downloads.
+//
+// Device layout (one handle):
+//   f[2]      populations, [9][ny][pitch] in the storage type, ping-pong;
+//             buffer `cur` holds the latest post-collision field and the
+//             other one the field before it (needed to reconstruct the
+//             post-stream state for downloads)
+//   nflag     uint8 [ny][nx], slot int32 [ny][nx], tile uint8 [ny][gx]:
+//             nodes whose moments other kernels read (net inputs, marker
+//             stencils) or whose collision is finished by another kernel
+//   side_f    [nslots][9], side_m [2][nslots][3] (compute type)
+//   avg       [3][ny][nx] running means (compute type)
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/ippi_lbm.h"
+#include "launch.h"
+
+using namespace ippi;
+
+namespace {
+
+char g_last_error[512] = "";
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct NetHost {
+    bool loaded = false;
+    int nin = 0;
+    std::vector<float> w;  // TorchScript order
+};
+
+}  // namespace
+
+struct ippi_lbm {
+    ippi_params p;
+    int S;          // storage
+    int csize;      // bytes of the compute type
+    int tsize;      // bytes of the storage type
+    cudaStream_t st = nullptr;
+    long long pitch = 0, plane = 0;
+    int gx = 0;
+    void* f[2] = {nullptr, nullptr};
+    int cur = 0;
+    Ctr* ctr = nullptr;
+    Ctr* ctr_h = nullptr;  // pinned mirror
+    cudaStream_t side = nullptr;   // concurrent prep / net / IB kernels
+    cudaEvent_t fork = nullptr, join = nullptr;
+    uint8_t* nflag = nullptr;
+    uint8_t* tile = nullptr;
+    int nslots = 0;
+    PrepNode* prep_d = nullptr;    // nodes whose post-stream state the side kernels need
+    int nprep = 0;
+    int ib_nst = 4;
+    size_t ib_smem = 0;
+    void* side_f = nullptr;
+    void* side_m = nullptr;
+    void* corner = nullptr;
+    void* avg = nullptr;
+    double* init_m = nullptr;
+    bool pending_init = true;
+    int last_t = 0;     // user step number of the last executed step
+    int kcount = 0;     // internal steps executed (init counts as k = 0)
+    // materialised download fields (valid until the next step)
+    double* dl = nullptr;     // [9 + 4 + 1][ny][nx]: f, rho ux uy nnflag, tau
+    bool dl_valid = false;
+    uint8_t* dl_flags = nullptr;
+    double* red = nullptr;    // reduction partials
+    // boundary nets
+    NetHost nets[8];
+    float* net_dev[8] = {};
+    std::vector<BandNode> band_nodes;
+    BandNode* band_nodes_d = nullptr;
+    int2* band_work_d = nullptr;
+    int* band_type_d = nullptr;
+    int band_blocks = 0;
+    // immersed boundary
+    int nmark = 0, nbody = 0, nforced = 0, ngroups = 0, hist_cap = 0;
+    std::vector<double> mk_xy, mk_ub, mk_ds;
+    std::vector<int> mk_body;
+    std::vector<DevBuf> ib_bufs;
+    IbArgs ib{};
+    double* force_now = nullptr;
+    double* force_hist = nullptr;
+    long long hist_written = 0;
+    // graphs of two steps: [start buffer][step parity]
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    char err[512] = "";
+};
+
+namespace {
+
+int fail(ippi_lbm* h, int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (h) snprintf(h->err, sizeof h->err, "%s", buf);
+    snprintf(g_last_error, sizeof g_last_error, "%s", buf);
+    return code;
+}
+
+#define CK(h, call)                                                                     \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return fail(h, e_ == cudaErrorMemoryAllocation ? IPPI_ERR_NOMEM : IPPI_ERR_CUDA, \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+template <typename P>
+cudaError_t dalloc(P** p, size_t bytes)
+{
+    return cudaMalloc((void**)p, bytes ? bytes : 16);
+}
+
+void dfree(void* p)
+{
+    if (p) cudaFree(p);
+}
+
+void drop_graphs(ippi_lbm* h)
+{
+    for (int b = 0; b < 2; b++)
+        for (int q = 0; q < 2; q++)
+            if (h->graph[b][q]) {
+                cudaGraphExecDestroy(h->graph[b][q]);
+                h->graph[b][q] = nullptr;
+            }
+}
+
+cudaError_t launch(const LaunchSet& L, int S)
+{
+    switch (S) {
+    case ST_F64: return launch_f64(L);
+    case ST_F32: return launch_f32(L);
+    case ST_F16: return launch_f16(L);
+    default: return launch_bf16(L);
+    }
+}
+
+// Mesh::DiracDelta (mesh.cpp:1367-1384), same expressions as the oracle
+double peskin_phi(double x)
+{
+    if (std::fabs(x) < 1) {
+        double R = 1.0 + 4.0 * std::fabs(x) - 4 * (x * x);
+        return (1.0 / 8.0) * (3.0 - 2.0 * std::fabs(x) + std::sqrt(R));
+    } else if (std::fabs(x) < 2) {
+        double R = -7.0 + 12.0 * std::fabs(x) - 4 * (x * x);
+        return (1.0 / 8.0) * (5.0 - 2.0 * std::fabs(x) - std::sqrt(R));
+    }
+    return 0;
+}
+
+// Marker stencil of InterpolateVel / SpreadForce (mesh.cpp:566-585, 618-638):
+// node (X, Y) contributes (value * wa) * wb.
+int marker_stencil(int kernel, double mx, double my, int* xs, int* ys, double* wa, double* wb)
+{
+    const int XInt = (int)mx, YInt = (int)my;
+    int n = 0;
+    if (kernel == IPPI_DELTA_PESKIN4) {
+        for (int X = XInt - 1; X <= XInt + 2; X++)
+            for (int Y = YInt - 1; Y <= YInt + 2; Y++) {
+                xs[n] = X;
+                ys[n] = Y;
+                wa[n] = peskin_phi(mx - X) * peskin_phi(my - Y);
+                wb[n] = 1.0;
+                n++;
+            }
+    } else {
+        for (int X = XInt; X <= XInt + 1; X++)
+            for (int Y = YInt; Y <= YInt + 1; Y++) {
+                xs[n] = X;
+                ys[n] = Y;
+                wa[n] = 1 - std::fabs(mx - X);
+                wb[n] = 1 - std::fabs(my - Y);
+                n++;
+            }
+    }
+    return n;
+}
+
+// ---------------------------------------------------------------------------
+// boundary-net band: nodes, neighbour references, call order
+// ---------------------------------------------------------------------------
+struct NbRef {
+    int x, y;
+    bool stale;
+};
+
+// Node list and neighbour order of Mesh::NNmodel_TypeXX in global
+// coordinates (reference local column i = x + 1).  Neighbours at x = -1 /
+// x = nx are the halo columns, which hold the other edge column's moments
+// from the previous step (mesh.cpp:493-498 with the periodic ring).
+void band_type_nodes(int type, int nx, int ny, std::vector<std::pair<int2, std::vector<NbRef>>>& out)
+{
+    auto ref = [&](int x, int y) {
+        if (x < 0) return NbRef{nx - 1, y, true};
+        if (x >= nx) return NbRef{0, y, true};
+        return NbRef{x, y, false};
+    };
+    auto add = [&](int x, int y, std::initializer_list<int2> nb) {
+        std::vector<NbRef> v;
+        for (auto q : nb) v.push_back(ref(q.x, q.y));
+        out.push_back({make_int2(x, y), v});
+    };
+    switch (type) {
+    case 0: add(0, 0, {{0, 1}, {1, 1}, {1, 0}}); break;
+    case 2: add(0, ny - 1, {{0, ny - 2}, {1, ny - 2}, {1, ny - 1}}); break;
+    case 4: add(nx - 1, ny - 1, {{nx - 2, ny - 1}, {nx - 2, ny - 2}, {nx - 1, ny - 2}}); break;
+    case 6: add(nx - 1, 0, {{nx - 1, 1}, {nx - 2, 1}, {nx - 2, 0}}); break;
+    case 1:
+        for (int y = 1; y < ny - 1; y++) add(0, y, {{0, y + 1}, {1, y + 1}, {1, y}, {1, y - 1}, {0, y - 1}});
+        break;
+    case 5:
+        for (int y = 1; y < ny - 1; y++)
+            add(nx - 1, y, {{nx - 1, y + 1}, {nx - 2, y + 1}, {nx - 2, y}, {nx - 2, y - 1}, {nx - 1, y - 1}});
+        break;
+    case 3:
+        for (int x = 0; x < nx; x++) {
+            int y = ny - 2;
+            add(x, y, {{x + 1, y}, {x + 1, y - 1}, {x, y - 1}, {x - 1, y - 1}, {x - 1, y}});
+        }
+        break;
+    case 7:
+        for (int x = 0; x < nx; x++) {
+            int y = 1;
+            add(x, y, {{x - 1, y}, {x - 1, y + 1}, {x, y + 1}, {x + 1, y + 1}, {x + 1, y}});
+        }
+        break;
+    }
+}
+
+bool nets_active(const ippi_lbm* h)
+{
+    if (h->p.collision != IPPI_BGK || h->p.bc_set != IPPI_BC_REF_NEE) return false;
+    for (int t = 0; t < 8; t++)
+        if (h->nets[t].loaded) return true;
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// rebuild of flags, slots, side buffers, band and IB tables
+// ---------------------------------------------------------------------------
+int rebuild(ippi_lbm* h)
+{
+    const int nx = h->p.nx, ny = h->p.ny;
+    const size_t nn = (size_t)nx * ny;
+    drop_graphs(h);
+    std::vector<uint8_t> flag(nn, 0);
+    std::vector<int> slot(nn, -1);
+    auto id = [&](int x, int y) { return (size_t)y * nx + x; };
+
+    // band nodes: the last loaded type covering a node decides (call order
+    // 00 01 02 04 05 06 03 07, mesh.cpp:364-379)
+    struct BandEntry {
+        int type;
+        std::vector<NbRef> nb;
+    };
+    std::map<size_t, BandEntry> band;
+    if (nets_active(h)) {
+        static const int order[8] = {0, 1, 2, 4, 5, 6, 3, 7};
+        for (int oi = 0; oi < 8; oi++) {
+            int t = order[oi];
+            if (!h->nets[t].loaded) continue;
+            std::vector<std::pair<int2, std::vector<NbRef>>> lst;
+            band_type_nodes(t, nx, ny, lst);
+            for (auto& e : lst) band[id(e.first.x, e.first.y)] = BandEntry{t, e.second};
+        }
+        for (auto& kv : band) {
+            flag[kv.first] |= NF_EXPORT | NF_DEFER;
+            for (auto& r : kv.second.nb) flag[id(r.x, r.y)] |= NF_EXPORT;
+        }
+    }
+
+    // immersed boundary: stencil nodes are exported and deferred
+    std::vector<int> fn_of_node;  // node -> forced index
+    std::vector<int> st_node;     // [nmark][16] node ids
+    std::vector<double> st_wa, st_wb;
+    const int nst = h->p.delta_kernel == IPPI_DELTA_PESKIN4 ? 16 : 4;
+    const int nm = h->nmark;
+    if (nm > 0) {
+        st_node.assign((size_t)nm * 16, -1);
+        st_wa.assign((size_t)nm * 16, 0.0);
+        st_wb.assign((size_t)nm * 16, 0.0);
+        for (int m = 0; m < nm; m++) {
+            int xs[16], ys[16];
+            double wa[16], wb[16];
+            int c = marker_stencil(h->p.delta_kernel, h->mk_xy[2 * m], h->mk_xy[2 * m + 1], xs, ys, wa, wb);
+            for (int q = 0; q < c; q++) {
+                st_node[(size_t)m * 16 + q] = (int)id(xs[q], ys[q]);
+                st_wa[(size_t)m * 16 + q] = wa[q];
+                st_wb[(size_t)m * 16 + q] = wb[q];
+                flag[id(xs[q], ys[q])] |= NF_EXPORT | NF_DEFER;
+            }
+        }
+    }
+
+    // slots in row-major order; every flagged node is a prep node
+    int ns = 0;
+    std::vector<PrepNode> prep;
+    for (size_t i = 0; i < nn; i++)
+        if (flag[i]) {
+            slot[i] = ns++;
+            prep.push_back(PrepNode{(int)(i % nx), (int)(i / nx), slot[i], flag[i]});
+        }
+    h->nslots = ns;
+
+    // the bulk kernel only needs to know which nodes it must skip
+    std::vector<uint8_t> defer(nn, 0);
+    std::vector<uint8_t> tile((size_t)h->gx * ny, 0);
+    for (int y = 0; y < ny; y++)
+        for (int x = 0; x < nx; x++)
+            if (flag[id(x, y)] & NF_DEFER) {
+                defer[id(x, y)] = NF_DEFER;
+                tile[(size_t)y * h->gx + x / kBlockX] = 1;
+            }
+
+    CK(h, cudaMemcpy(h->nflag, defer.data(), nn, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->tile, tile.data(), tile.size(), cudaMemcpyHostToDevice));
+    dfree(h->prep_d);
+    h->prep_d = nullptr;
+    h->nprep = (int)prep.size();
+    CK(h, dalloc(&h->prep_d, std::max<size_t>(prep.size(), 1) * sizeof(PrepNode)));
+    if (!prep.empty())
+        CK(h, cudaMemcpy(h->prep_d, prep.data(), prep.size() * sizeof(PrepNode), cudaMemcpyHostToDevice));
+    dfree(h->side_f);
+    dfree(h->side_m);
+    h->side_f = h->side_m = nullptr;
+    CK(h, dalloc(&h->side_f, (size_t)std::max(ns, 1) * 9 * h->csize));
+    CK(h, dalloc(&h->side_m, (size_t)std::max(ns, 1) * 6 * h->csize));
+    {
+        // the previous-step moments read by the first steps' nets are the
+        // halo's initial rho = 1, u = 0 (mesh.cpp:88-101)
+        std::vector<char> init((size_t)std::max(ns, 1) * 6 * h->csize, 0);
+        for (int s = 0; s < 2 * std::max(ns, 1); s++) {
+            if (h->csize == 8)
+                ((double*)init.data())[3 * s] = 1.0;
+            else
+                ((float*)init.data())[3 * s] = 1.0f;
+        }
+        CK(h, cudaMemcpy(h->side_m, init.data(), init.size(), cudaMemcpyHostToDevice));
+    }
+
+    // band tables
+    dfree(h->band_nodes_d);
+    dfree(h->band_work_d);
+    dfree(h->band_type_d);
+    h->band_nodes_d = nullptr;
+    h->band_work_d = nullptr;
+    h->band_type_d = nullptr;
+    h->band_blocks = 0;
+    if (!band.empty()) {
+        std::vector<BandNode> nodes;
+        std::vector<int2> work;
+        std::vector<int> wtype;
+        for (int t = 0; t < 8; t++) {
+            int first = (int)nodes.size();
+            for (auto& kv : band) {
+                if (kv.second.type != t) continue;
+                BandNode b{};
+                b.x = (int)(kv.first % nx);
+                b.y = (int)(kv.first / nx);
+                b.slot = slot[kv.first];
+                b.nin = (int)kv.second.nb.size() * 3;
+                b.nb_stale = 0;
+                for (size_t q = 0; q < kv.second.nb.size(); q++) {
+                    const NbRef& r = kv.second.nb[q];
+                    b.nb_slot[q] = slot[id(r.x, r.y)];
+                    if (r.stale) b.nb_stale |= 1 << q;
+                }
+                nodes.push_back(b);
+            }
+            for (int s0 = first; s0 < (int)nodes.size(); s0 += kBandNodes) {
+                work.push_back(make_int2(s0, std::min(kBandNodes, (int)nodes.size() - s0)));
+                wtype.push_back(t);
+            }
+        }
+        h->band_nodes = nodes;
+        CK(h, dalloc(&h->band_nodes_d, nodes.size() * sizeof(BandNode)));
+        CK(h, dalloc(&h->band_work_d, work.size() * sizeof(int2)));
+        CK(h, dalloc(&h->band_type_d, wtype.size() * sizeof(int)));
+        CK(h, cudaMemcpy(h->band_nodes_d, nodes.data(), nodes.size() * sizeof(BandNode), cudaMemcpyHostToDevice));
+        CK(h, cudaMemcpy(h->band_work_d, work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice));
+        CK(h, cudaMemcpy(h->band_type_d, wtype.data(), wtype.size() * sizeof(int), cudaMemcpyHostToDevice));
+        h->band_blocks = (int)work.size();
+    }
+
+    // immersed-boundary tables
+    for (auto& b : h->ib_bufs) dfree(b.p);
+    h->ib_bufs.clear();
+    h->ngroups = 0;
+    h->nforced = 0;
+    if (nm > 0) {
+        // markers grouped by body, keeping their order within a body
+        std::vector<int> order(nm);
+        for (int m = 0; m < nm; m++) order[m] = m;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return h->mk_body[a] < h->mk_body[b]; });
+        const int nb = h->nbody;
+        // bodies sharing a stencil node must be finished by the same block
+        std::vector<int> parent(nb);
+        for (int b = 0; b < nb; b++) parent[b] = b;
+        std::function<int(int)> findp = [&](int b) { return parent[b] == b ? b : parent[b] = findp(parent[b]); };
+        std::map<int, int> node_body;
+        for (int m = 0; m < nm; m++)
+            for (int q = 0; q < nst; q++) {
+                int nd = st_node[(size_t)m * 16 + q];
+                auto it = node_body.find(nd);
+                if (it == node_body.end())
+                    node_body[nd] = h->mk_body[m];
+                else
+                    parent[findp(it->second)] = findp(h->mk_body[m]);
+            }
+        // groups of bodies; bodies numbered so that each group is contiguous
+        std::map<int, std::vector<int>> groups;
+        for (int b = 0; b < nb; b++) groups[findp(b)].push_back(b);
+        std::vector<int4> grp;
+        std::vector<int2> gbody, body_m(nb, make_int2(0, 0));
+        std::vector<int> morder;  // marker order on the device
+        std::vector<int> fnode;   // forced node ids
+        std::vector<int> fptr(1, 0), fe_marker;
+        std::vector<double2> fe_w;
+        std::vector<int> st_loc((size_t)nm * 16, 0);  // device order, group-local node index
+        std::vector<double2> st_w((size_t)nm * 16, make_double2(0, 0));
+        std::vector<int> new_index(nm);
+        std::map<int, int> forced_index;
+        for (auto& g : groups) {
+            int4 G;
+            G.x = (int)morder.size();
+            G.z = (int)fnode.size();
+            int b0 = g.second.front(), b1 = g.second.back() + 1;
+            gbody.push_back(make_int2(b0, b1));
+            for (int b : g.second) {
+                int m0 = (int)morder.size();
+                for (int m : order)
+                    if (h->mk_body[m] == b) {
+                        new_index[m] = (int)morder.size();
+                        morder.push_back(m);
+                    }
+                body_m[b] = make_int2(m0, (int)morder.size());
+            }
+            G.y = (int)morder.size();
+            // forced nodes of the group in first-use order, CSR in marker order
+            std::vector<std::vector<std::pair<int, double2>>> entries;
+            for (int mi = G.x; mi < G.y; mi++) {
+                int m = morder[mi];
+                for (int q = 0; q < nst; q++) {
+                    int nd = st_node[(size_t)m * 16 + q];
+                    auto it = forced_index.find(nd);
+                    int fi;
+                    if (it == forced_index.end()) {
+                        fi = (int)fnode.size();
+                        forced_index[nd] = fi;
+                        fnode.push_back(nd);
+                        entries.emplace_back();
+                    } else {
+                        fi = it->second;
+                    }
+                    double2 w = make_double2(st_wa[(size_t)m * 16 + q], st_wb[(size_t)m * 16 + q]);
+                    entries[fi - G.z].push_back({mi - G.x, w});
+                    st_loc[(size_t)mi * 16 + q] = fi - G.z;
+                    st_w[(size_t)mi * 16 + q] = w;
+                }
+            }
+            for (auto& e : entries) {
+                for (auto& pr : e) {
+                    fe_marker.push_back(pr.first);
+                    fe_w.push_back(pr.second);
+                }
+                fptr.push_back((int)fe_marker.size());
+            }
+            G.w = (int)fnode.size();
+            grp.push_back(G);
+        }
+        // bodies must be numbered contiguously inside each group
+        for (size_t gi = 0; gi < grp.size(); gi++) {
+            int2 gb = gbody[gi];
+            int cnt = 0;
+            for (auto& g : groups)
+                if (g.second.front() == gb.x) cnt = (int)g.second.size();
+            if (gb.y - gb.x != cnt)
+                return fail(h, IPPI_ERR_ARG, "bodies sharing stencil nodes must have consecutive ids");
+        }
+        const int nf = (int)fnode.size();
+        std::vector<int> fn_slot(nf);
+        std::vector<int2> fn_xy(nf);
+        for (int i = 0; i < nf; i++) {
+            fn_slot[i] = slot[fnode[i]];
+            fn_xy[i] = make_int2(fnode[i] % nx, fnode[i] / nx);
+        }
+        std::vector<double2> ub(nm);
+        std::vector<double> ds(nm);
+        for (int mi = 0; mi < nm; mi++) {
+            int m = morder[mi];
+            ub[mi] = make_double2(h->mk_ub[2 * m], h->mk_ub[2 * m + 1]);
+            ds[mi] = h->mk_ds[m];
+        }
+        auto up = [&](const void* src, size_t bytes) -> void* {
+            DevBuf b;
+            b.bytes = bytes;
+            if (dalloc(&b.p, bytes) != cudaSuccess) return nullptr;
+            if (src && cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
+            if (!src) cudaMemset(b.p, 0, bytes);
+            h->ib_bufs.push_back(b);
+            return b.p;
+        };
+        IbArgs& I = h->ib;
+        I = IbArgs{};
+        I.nmark = nm;
+        I.ub = (const double2*)up(ub.data(), nm * sizeof(double2));
+        I.ds = (const double*)up(ds.data(), nm * sizeof(double));
+        I.st_node = (const int*)up(st_loc.data(), st_loc.size() * sizeof(int));
+        I.st_w = (const double2*)up(st_w.data(), st_w.size() * sizeof(double2));
+        I.fn_slot = (const int*)up(fn_slot.data(), nf * sizeof(int));
+        I.fn_xy = (const int2*)up(fn_xy.data(), nf * sizeof(int2));
+        I.fn_ptr = (const int*)up(fptr.data(), fptr.size() * sizeof(int));
+        I.fe_marker = (const int*)up(fe_marker.data(), fe_marker.size() * sizeof(int));
+        I.fe_w = (const double2*)up(fe_w.data(), fe_w.size() * sizeof(double2));
+        I.group = (const int4*)up(grp.data(), grp.size() * sizeof(int4));
+        I.gbody = (const int2*)up(gbody.data(), gbody.size() * sizeof(int2));
+        I.body_m = (const int2*)up(body_m.data(), body_m.size() * sizeof(int2));
+        h->hist_cap = (int)std::max<long long>(16, std::min<long long>(1 << 16, (1ll << 24) / std::max(1, nb)));
+        I.force_now = (double*)up(nullptr, (size_t)nb * 2 * sizeof(double));
+        I.force_hist = (double*)up(nullptr, (size_t)h->hist_cap * nb * 2 * sizeof(double));
+        I.nbody = nb;
+        I.hist_cap = h->hist_cap;
+        I.mdf_iters = std::max(1, h->p.mdf_iters);
+        for (auto& b : h->ib_bufs)
+            if (!b.p) return fail(h, IPPI_ERR_NOMEM, "IB table allocation failed");
+        h->force_now = I.force_now;
+        h->force_hist = I.force_hist;
+        h->hist_written = 0;
+        h->ngroups = (int)grp.size();
+        h->nforced = nf;
+        h->ib_nst = nst;
+        size_t smem = 0;
+        for (auto& G : grp) smem = std::max(smem, ib_smem_bytes(G.w - G.z, G.y - G.x));
+        int dev_smem = 0;
+        cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->p.device);
+        if (smem + sizeof(double) * 2 * kIbThreads > (size_t)dev_smem)
+            return fail(h, IPPI_ERR_ARG, "a body group needs %zu bytes of shared memory (limit %d); "
+                        "split it into several bodies", smem, dev_smem);
+        cudaError_t e = cudaSuccess;
+        switch (h->S) {
+        case ST_F64: e = prepare_f64(smem); break;
+        case ST_F32: e = prepare_f32(smem); break;
+        case ST_F16: e = prepare_f16(smem); break;
+        default: e = prepare_bf16(smem); break;
+        }
+        CK(h, e);
+        h->ib_smem = smem;
+    }
+    h->dl_valid = false;
+    return IPPI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launches
+// ---------------------------------------------------------------------------
+LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int par)
+{
+    LaunchSet L{};
+    StepArgs& a = L.step;
+    a.f_in = fin;
+    a.f_out = fout;
+    a.pitch = h->pitch;
+    a.plane = h->plane;
+    a.nx = h->p.nx;
+    a.ny = h->p.ny;
+    a.les = h->p.les_model == IPPI_LES_SMAGORINSKY;
+    a.plate_x0 = h->p.plate_x0;
+    a.tau0 = h->p.tau0;
+    a.cs = h->p.cs;
+    a.u_in = h->p.u_in;
+    a.rho0 = h->p.rho0;
+    a.f_tau0 = (float)h->p.tau0;
+    a.f_cs = (float)h->p.cs;
+    a.f_u_in = (float)h->p.u_in;
+    a.f_rho0 = (float)h->p.rho0;
+    a.tile = h->tile;
+    a.tiles_x = h->gx;
+    a.nflag = h->nflag;
+    a.side_f = h->side_f;
+    a.side_m = h->side_m;
+    a.nslots = h->nslots;
+    a.corner = h->corner;
+    a.avg = h->avg;
+    a.avg_start = h->p.avg_start;
+    a.ctr = h->ctr;
+    a.mode = mode;
+    a.par = par;
+    a.fixed_t = h->last_t;
+    a.init_m = h->init_m;
+    const size_t nn = (size_t)h->p.nx * h->p.ny;
+    a.dl_f = h->dl;
+    a.dl_m = h->dl ? h->dl + 9 * nn : nullptr;
+    a.dl_tau = h->dl ? h->dl + 13 * nn : nullptr;
+    L.grid = dim3(h->gx, h->p.ny);
+    L.coll = h->p.collision;
+    L.scene = h->p.bc_set == IPPI_BC_CHANNEL ? SC_CHANNEL : SC_REF;
+    L.stream = h->st;
+    L.side = h->side;
+    L.fork = h->fork;
+    L.join = h->join;
+    L.prep = h->prep_d;
+    L.nprep = h->nprep;
+    L.band = h->band_blocks > 0;
+    L.ib = h->ngroups > 0;
+    if (L.band) {
+        BandArgs& B = L.band_args;
+        B.nodes = h->band_nodes_d;
+        B.work = h->band_work_d;
+        B.work_type = h->band_type_d;
+        for (int t = 0; t < 8; t++) {
+            if (!h->nets[t].loaded) continue;
+            const int nin = h->nets[t].nin;
+            float* base = h->net_dev[t];
+            B.net[t].w1t = base;
+            B.net[t].b1 = base + nin * kHidden;
+            B.net[t].wht = B.net[t].b1 + kHidden;
+            B.net[t].bh = B.net[t].wht + 6 * kHidden * kHidden;
+            B.net[t].wo = B.net[t].bh + 6 * kHidden;
+            B.net[t].bo = h->nets[t].w.back();
+        }
+        B.s = a;
+        L.band_blocks = h->band_blocks;
+    }
+    if (L.ib) {
+        L.ib_args = h->ib;
+        L.ib_args.s = a;
+        L.ib_blocks = h->ngroups;
+        L.ib_nst = h->ib_nst;
+        L.ib_smem = h->ib_smem;
+    }
+    return L;
+}
+
+// the user step number t of the next step, into the counter entry of its parity
+int set_time(ippi_lbm* h, int t)
+{
+    const int par = h->kcount & 1;
+    h->ctr_h->t[par] = t;
+    CK(h, cudaMemcpyAsync(&h->ctr->t[par], &h->ctr_h->t[par], sizeof(int), cudaMemcpyHostToDevice, h->st));
+    return IPPI_OK;
+}
+
+// the first collision, from the equilibrium of the initial moments (k = 0)
+int run_init(ippi_lbm* h)
+{
+    std::memset(h->ctr_h, 0, sizeof(Ctr));
+    CK(h, cudaMemcpyAsync(h->ctr, h->ctr_h, sizeof(Ctr), cudaMemcpyHostToDevice, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    LaunchSet L = make_launch(h, MODE_INIT, nullptr, h->f[0], 0);
+    CK(h, launch(L, h->S));
+    h->cur = 0;
+    h->kcount = 1;
+    h->last_t = 0;
+    h->pending_init = false;
+    h->dl_valid = false;
+    return IPPI_OK;
+}
+
+// two steps starting from buffer b with parity q, as one CUDA graph
+int build_graph(ippi_lbm* h, int b, int q)
+{
+    cudaGraph_t g;
+    CK(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    LaunchSet L0 = make_launch(h, MODE_STEP, h->f[b], h->f[b ^ 1], q);
+    LaunchSet L1 = make_launch(h, MODE_STEP, h->f[b ^ 1], h->f[b], q ^ 1);
+    cudaError_t e0 = launch(L0, h->S);
+    cudaError_t e1 = launch(L1, h->S);
+    cudaError_t ec = cudaStreamEndCapture(h->st, &g);
+    if (e0 != cudaSuccess || e1 != cudaSuccess || ec != cudaSuccess)
+        return fail(h, IPPI_ERR_CUDA, "graph capture failed: %s",
+                    cudaGetErrorString(e0 ? e0 : (e1 ? e1 : ec)));
+    cudaError_t ei = cudaGraphInstantiate(&h->graph[b][q], g, 0);
+    cudaGraphDestroy(g);
+    CK(h, ei);
+    return IPPI_OK;
+}
+
+// post-stream state of the last step (populations, moments, next tau) into
+// the download buffers: the last step re-run from its input field with its
+// outputs redirected (nothing of the state changes)
+int materialize(ippi_lbm* h)
+{
+    if (h->dl_valid) return IPPI_OK;
+    const size_t nn = (size_t)h->p.nx * h->p.ny;
+    if (!h->dl) CK(h, dalloc(&h->dl, 14 * nn * sizeof(double)));
+    CK(h, cudaMemsetAsync(h->dl + 12 * nn, 0, nn * sizeof(double), h->st));  // net-flag plane
+    LaunchSet L;
+    if (h->pending_init) {
+        h->last_t = 0;
+        L = make_launch(h, MODE_MAT_INIT, nullptr, nullptr, 0);
+    } else {
+        L = make_launch(h, MODE_MAT, h->f[h->cur ^ 1], nullptr, (h->kcount - 1) & 1);
+    }
+    CK(h, launch(L, h->S));
+    CK(h, cudaStreamSynchronize(h->st));
+    h->dl_valid = true;
+    return IPPI_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int ippi_abi_version(void) { return IPPI_ABI_VERSION; }
+
+void ippi_params_default(ippi_params* p, int nx, int ny)
+{
+    std::memset(p, 0, sizeof *p);
+    p->nx = nx;
+    p->ny = ny;
+    p->collision = IPPI_BGK;
+    p->storage = IPPI_F64;
+    p->bc_set = IPPI_BC_REF_NEE;
+    p->les_model = IPPI_LES_SMAGORINSKY;
+    p->tau0 = 0.5 + 6.0 * ((ny * 0.1) / 5e5);  // main.cpp:38-43
+    p->cs = 0.173;
+    p->u_in = 0.1;
+    p->rho0 = 1.0;
+    p->plate_x0 = 400;
+    p->avg_start = 30000;
+    p->delta_kernel = IPPI_DELTA_BILINEAR;
+    p->mdf_iters = 1;
+    p->device = 0;
+}
+
+int ippi_create(const ippi_params* p, ippi_lbm** out)
+{
+    if (!p || !out) return fail(nullptr, IPPI_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (p->nx < 4 || p->ny < 4) return fail(nullptr, IPPI_ERR_ARG, "lattice must be at least 4 x 4");
+    if (9ll * (((long long)p->nx + 63) / 64 * 64) * p->ny >= (1ll << 31))
+        return fail(nullptr, IPPI_ERR_ARG, "lattice too large for 32-bit population offsets");
+    if (p->collision < 0 || p->collision > 2) return fail(nullptr, IPPI_ERR_ARG, "bad collision");
+    if (p->storage < 0 || p->storage > 3) return fail(nullptr, IPPI_ERR_ARG, "bad storage");
+    if (p->bc_set < 0 || p->bc_set > 1) return fail(nullptr, IPPI_ERR_ARG, "bad bc_set");
+    if (p->les_model < 0 || p->les_model > 1) return fail(nullptr, IPPI_ERR_ARG, "bad les_model");
+    if (p->delta_kernel < 0 || p->delta_kernel > 1) return fail(nullptr, IPPI_ERR_ARG, "bad delta_kernel");
+    if (!(p->tau0 > 0.5)) return fail(nullptr, IPPI_ERR_ARG, "tau0 must exceed 0.5");
+    if (!(p->rho0 > 0)) return fail(nullptr, IPPI_ERR_ARG, "rho0 must be positive");
+    if (p->bc_set == IPPI_BC_CHANNEL && !(std::fabs(p->u_in) < 0.5))
+        return fail(nullptr, IPPI_ERR_ARG, "channel inlet velocity must be below 0.5");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(nullptr, IPPI_ERR_CUDA, "no CUDA device available");
+    if (p->device < 0 || p->device >= ndev) return fail(nullptr, IPPI_ERR_ARG, "bad device ordinal");
+
+    ippi_lbm* h = new ippi_lbm();
+    h->p = *p;
+    if (h->p.mdf_iters < 1) h->p.mdf_iters = 1;
+    h->S = p->storage;
+    h->csize = p->storage == IPPI_F64 ? 8 : 4;
+    h->tsize = p->storage == IPPI_F64 ? 8 : (p->storage == IPPI_F32 ? 4 : 2);
+    const int nx = p->nx, ny = p->ny;
+    const size_t nn = (size_t)nx * ny;
+    h->pitch = ((long long)nx + 63) / 64 * 64;
+    h->plane = h->pitch * ny;
+    h->gx = (nx + kBlockX - 1) / kBlockX;
+    int rc = IPPI_OK;
+    auto bail = [&](int code) {
+        ippi_destroy(h);
+        return code;
+    };
+    if (cudaSetDevice(p->device) != cudaSuccess) return bail(fail(nullptr, IPPI_ERR_CUDA, "cudaSetDevice failed"));
+    int lo_prio = 0, hi_prio = 0;
+    cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+    // the side stream (a handful of small blocks) outranks the bulk kernel so
+    // its blocks are scheduled as soon as an SM has room
+    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, hi_prio) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming) != cudaSuccess)
+        return bail(fail(nullptr, IPPI_ERR_CUDA, "stream creation failed"));
+    const size_t fbytes = (size_t)9 * h->plane * h->tsize;
+    for (int b = 0; b < 2; b++)
+        if (dalloc(&h->f[b], fbytes) != cudaSuccess || cudaMemset(h->f[b], 0, fbytes) != cudaSuccess)
+            return bail(fail(nullptr, IPPI_ERR_NOMEM, "population buffers (%zu bytes each)", fbytes));
+    if (dalloc(&h->ctr, sizeof(Ctr)) != cudaSuccess || cudaMallocHost(&h->ctr_h, sizeof(Ctr)) != cudaSuccess ||
+        dalloc(&h->nflag, nn) != cudaSuccess ||
+        dalloc(&h->tile, (size_t)h->gx * ny) != cudaSuccess ||
+        dalloc(&h->corner, 24 * (size_t)h->csize) != cudaSuccess ||
+        dalloc(&h->avg, 3 * nn * h->csize) != cudaSuccess ||
+        dalloc(&h->init_m, 3 * nn * sizeof(double)) != cudaSuccess ||
+        dalloc(&h->red, 4096 * sizeof(double)) != cudaSuccess)
+        return bail(fail(nullptr, IPPI_ERR_NOMEM, "device allocation failed"));
+    cudaMemset(h->ctr, 0, sizeof(Ctr));
+    cudaMemset(h->corner, 0, 24 * (size_t)h->csize);
+    rc = rebuild(h);
+    if (rc != IPPI_OK) return bail(rc);
+    rc = ippi_init_macros(h, nullptr, nullptr, nullptr);
+    if (rc != IPPI_OK) return bail(rc);
+    *out = h;
+    return IPPI_OK;
+}
+
+int ippi_destroy(ippi_lbm* h)
+{
+    if (!h) return IPPI_OK;
+    if (h->st) cudaStreamSynchronize(h->st);
+    drop_graphs(h);
+    for (int b = 0; b < 2; b++) dfree(h->f[b]);
+    dfree(h->ctr);
+    if (h->ctr_h) cudaFreeHost(h->ctr_h);
+    dfree(h->nflag);
+    dfree(h->prep_d);
+    dfree(h->tile);
+    dfree(h->side_f);
+    dfree(h->side_m);
+    dfree(h->corner);
+    dfree(h->avg);
+    dfree(h->init_m);
+    dfree(h->dl);
+    dfree(h->dl_flags);
+    dfree(h->red);
+    for (int t = 0; t < 8; t++) dfree(h->net_dev[t]);
+    dfree(h->band_nodes_d);
+    dfree(h->band_work_d);
+    dfree(h->band_type_d);
+    for (auto& b : h->ib_bufs) dfree(b.p);
+    if (h->fork) cudaEventDestroy(h->fork);
+    if (h->join) cudaEventDestroy(h->join);
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+    return IPPI_OK;
+}
+
+int ippi_init_macros(ippi_lbm* h, const double* rho, const double* ux, const double* uy)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    const size_t nn = (size_t)h->p.nx * h->p.ny;
+    std::vector<double> m(3 * nn);
+    for (size_t i = 0; i < nn; i++) {
+        m[i] = rho ? rho[i] : 1.0;
+        m[nn + i] = ux ? ux[i] : 0.0;
+        m[2 * nn + i] = uy ? uy[i] : 0.0;
+        if (!(m[i] > 0) || !std::isfinite(m[nn + i]) || !std::isfinite(m[2 * nn + i]))
+            return fail(h, IPPI_ERR_ARG, "initial rho must be positive and u finite (node %zu)", i);
+    }
+    if (!h->init_m) CK(h, dalloc(&h->init_m, 3 * nn * sizeof(double)));
+    CK(h, cudaMemcpy(h->init_m, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h, cudaMemset(h->avg, 0, 3 * nn * h->csize));
+    h->pending_init = true;
+    h->dl_valid = false;
+    h->hist_written = 0;
+    drop_graphs(h);
+    return IPPI_OK;
+}
+
+int ippi_set_markers(ippi_lbm* h, int n, const double* xy, const double* ub, const int* body,
+                     const double* ds)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (n < 0 || (n > 0 && !xy)) return fail(h, IPPI_ERR_ARG, "bad marker arrays");
+    const int nst = h->p.delta_kernel == IPPI_DELTA_PESKIN4 ? 16 : 4;
+    int nbody = 0;
+    for (int m = 0; m < n; m++) {
+        const double mx = xy[2 * m], my = xy[2 * m + 1];
+        if (!(mx >= 0 && mx < h->p.nx && my >= 0 && my < h->p.ny))
+            return fail(h, IPPI_ERR_ARG, "marker %d outside the lattice", m);
+        int xs[16], ys[16];
+        double wa[16], wb[16];
+        int c = marker_stencil(h->p.delta_kernel, mx, my, xs, ys, wa, wb);
+        for (int q = 0; q < c; q++)
+            if (xs[q] < 3 || xs[q] > h->p.nx - 4 || ys[q] < 3 || ys[q] > h->p.ny - 4)
+                return fail(h, IPPI_ERR_ARG, "marker %d stencil is closer than 3 nodes to the edge", m);
+        const int b = body ? body[m] : 0;
+        if (b < 0) return fail(h, IPPI_ERR_ARG, "negative body id");
+        nbody = std::max(nbody, b + 1);
+        (void)nst;
+    }
+    h->nmark = n;
+    h->nbody = n > 0 ? nbody : 0;
+    h->mk_xy.assign(xy, xy + 2 * (size_t)n);
+    h->mk_ub.assign(2 * (size_t)n, 0.0);
+    if (ub) h->mk_ub.assign(ub, ub + 2 * (size_t)n);
+    h->mk_ds.assign(n, 1.0);
+    if (ds) h->mk_ds.assign(ds, ds + n);
+    h->mk_body.assign(n, 0);
+    if (body) h->mk_body.assign(body, body + n);
+    CK(h, cudaStreamSynchronize(h->st));
+    return rebuild(h);
+}
+
+int ippi_load_band_net(ippi_lbm* h, int type, const float* w, size_t n)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (type < 0 || type > 7 || !w) return fail(h, IPPI_ERR_ARG, "bad net type");
+    const int nin = (type % 2 == 0) ? 9 : 15;
+    const size_t need = (size_t)kHidden * nin + kHidden + 6 * (kHidden * kHidden + kHidden) + kHidden + 1;
+    if (n != need) return fail(h, IPPI_ERR_ARG, "net %d expects %zu floats, got %zu", type, need, n);
+    NetHost& net = h->nets[type];
+    net.loaded = true;
+    net.nin = nin;
+    net.w.assign(w, w + n);
+    // device layout: w1t[nin][128], b1, wht[6][128][128], bh[6][128], wo[128]
+    std::vector<float> d((size_t)nin * kHidden + kHidden + 6 * kHidden * kHidden + 6 * kHidden + kHidden);
+    const float* p = w;
+    size_t o = 0;
+    for (int i = 0; i < nin; i++)
+        for (int j = 0; j < kHidden; j++) d[o++] = p[j * nin + i];
+    p += kHidden * nin;
+    for (int j = 0; j < kHidden; j++) d[o++] = p[j];
+    p += kHidden;
+    const float* hp = p;
+    size_t ob = o + 6 * kHidden * kHidden;
+    for (int l = 0; l < 6; l++) {
+        const float* W = hp + (size_t)l * (kHidden * kHidden + kHidden);
+        for (int i = 0; i < kHidden; i++)
+            for (int j = 0; j < kHidden; j++) d[o++] = W[j * kHidden + i];
+        for (int j = 0; j < kHidden; j++) d[ob++] = W[kHidden * kHidden + j];
+    }
+    o = ob;
+    p = hp + 6 * (size_t)(kHidden * kHidden + kHidden);
+    for (int j = 0; j < kHidden; j++) d[o++] = p[j];
+    CK(h, cudaStreamSynchronize(h->st));
+    dfree(h->net_dev[type]);
+    h->net_dev[type] = nullptr;
+    CK(h, dalloc(&h->net_dev[type], d.size() * sizeof(float)));
+    CK(h, cudaMemcpy(h->net_dev[type], d.data(), d.size() * sizeof(float), cudaMemcpyHostToDevice));
+    return rebuild(h);
+}
+
+int ippi_step(ippi_lbm* h, int nsteps, int t0)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (nsteps < 0) return fail(h, IPPI_ERR_ARG, "negative step count");
+    if (nsteps == 0) return IPPI_OK;
+    CK(h, cudaSetDevice(h->p.device));
+    if (h->pending_init) {
+        int rc = run_init(h);
+        if (rc) return rc;
+    }
+    int rc = set_time(h, t0);
+    if (rc) return rc;
+    int left = nsteps;
+    const int q = h->kcount & 1;  // parity of the first step; graphs keep it
+    while (left >= 2) {
+        if (!h->graph[h->cur][q]) {
+            rc = build_graph(h, h->cur, q);
+            if (rc) return rc;
+        }
+        CK(h, cudaGraphLaunch(h->graph[h->cur][q], h->st));
+        left -= 2;
+    }
+    if (left) {
+        LaunchSet L = make_launch(h, MODE_STEP, h->f[h->cur], h->f[h->cur ^ 1], q);
+        CK(h, launch(L, h->S));
+        h->cur ^= 1;
+    }
+    h->kcount += nsteps;
+    h->last_t = t0 + nsteps - 1;
+    h->hist_written += nsteps;
+    h->dl_valid = false;
+    CK(h, cudaMemcpyAsync(h->ctr_h, h->ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    if (h->ctr_h->err)
+        return fail(h, IPPI_ERR_DIVERGED, "Simulation Error! rho left [0,10] at step %d", h->ctr_h->err_t);
+    return IPPI_OK;
+}
+
+int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk, double* ms_band, double* ms_ib)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (nsteps <= 0) return fail(h, IPPI_ERR_ARG, "nsteps must be positive");
+    CK(h, cudaSetDevice(h->p.device));
+    if (h->pending_init) {
+        int rc = run_init(h);
+        if (rc) return rc;
+    }
+    int rc = set_time(h, t0);
+    if (rc) return rc;
+    std::vector<cudaEvent_t> ev((size_t)nsteps * 4);
+    for (auto& e : ev) CK(h, cudaEventCreate(&e));
+    for (int s = 0; s < nsteps; s++) {
+        LaunchSet L = make_launch(h, MODE_STEP, h->f[h->cur], h->f[h->cur ^ 1], (h->kcount + s) & 1);
+        L.events = &ev[(size_t)s * 4];
+        CK(h, launch(L, h->S));
+        h->cur ^= 1;
+    }
+    CK(h, cudaStreamSynchronize(h->st));
+    CK(h, cudaStreamSynchronize(h->side));
+    // bulk kernel: events 0-1 on the main stream; side chain (prep + nets /
+    // IB), concurrent with it: events 2-3 on the side stream
+    double tb = 0, tn = 0, ti = 0;
+    const bool band = h->band_blocks > 0, ib = h->ngroups > 0, side = h->nprep > 0;
+    for (int s = 0; s < nsteps; s++) {
+        float ms;
+        cudaEventElapsedTime(&ms, ev[s * 4 + 0], ev[s * 4 + 1]);
+        tb += ms;
+        if (side) {
+            cudaEventElapsedTime(&ms, ev[s * 4 + 2], ev[s * 4 + 3]);
+            if (band) tn += ms;
+            if (ib) ti += ms;
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    h->kcount += nsteps;
+    h->last_t = t0 + nsteps - 1;
+    h->hist_written += nsteps;
+    h->dl_valid = false;
+    if (ms_bulk) *ms_bulk = tb / nsteps;
+    if (ms_band) *ms_band = tn / nsteps;
+    if (ms_ib) *ms_ib = ti / nsteps;
+    CK(h, cudaMemcpy(h->ctr_h, h->ctr, sizeof(Ctr), cudaMemcpyDeviceToHost));
+    if (h->ctr_h->err)
+        return fail(h, IPPI_ERR_DIVERGED, "Simulation Error! rho left [0,10] at step %d", h->ctr_h->err_t);
+    return IPPI_OK;
+}
+
+int ippi_download(ippi_lbm* h, int field, void* host, size_t bytes)
+{
+    if (!h || !host) return fail(h, IPPI_ERR_ARG, "null argument");
+    CK(h, cudaSetDevice(h->p.device));
+    const size_t nn = (size_t)h->p.nx * h->p.ny;
+    size_t need = field == IPPI_FIELD_F ? 9 * nn * sizeof(double)
+                                        : (field == IPPI_FIELD_FLAGS ? nn : nn * sizeof(double));
+    if (field < 0 || field > 9) return fail(h, IPPI_ERR_ARG, "bad field %d", field);
+    if (bytes != need) return fail(h, IPPI_ERR_ARG, "field %d needs %zu bytes, got %zu", field, need, bytes);
+    switch (field) {
+    case IPPI_FIELD_FLAGS: {
+        if (!h->dl_flags) CK(h, dalloc(&h->dl_flags, nn));
+        style_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, h->st>>>(
+            h->dl_flags, h->p.nx, h->p.ny, h->p.plate_x0,
+            h->p.bc_set == IPPI_BC_CHANNEL ? SC_CHANNEL : SC_REF);
+        CK(h, cudaGetLastError());
+        CK(h, cudaMemcpyAsync(host, h->dl_flags, nn, cudaMemcpyDeviceToHost, h->st));
+        CK(h, cudaStreamSynchronize(h->st));
+        return IPPI_OK;
+    }
+    case IPPI_FIELD_AVG_U:
+    case IPPI_FIELD_AVG_V:
+    case IPPI_FIELD_AVG_RHO: {
+        const size_t off = (size_t)(field - IPPI_FIELD_AVG_U) * nn;
+        if (h->csize == 8) {
+            CK(h, cudaMemcpyAsync(host, (double*)h->avg + off, nn * 8, cudaMemcpyDeviceToHost, h->st));
+        } else {
+            if (!h->dl) CK(h, dalloc(&h->dl, 14 * nn * sizeof(double)));
+            h->dl_valid = false;
+            to_double_kernel<float><<<(unsigned)((nn + 255) / 256), 256, 0, h->st>>>((const float*)h->avg + off,
+                                                                                      h->dl, (long long)nn);
+            CK(h, cudaGetLastError());
+            CK(h, cudaMemcpyAsync(host, h->dl, nn * 8, cudaMemcpyDeviceToHost, h->st));
+        }
+        CK(h, cudaStreamSynchronize(h->st));
+        return IPPI_OK;
+    }
+    default: break;
+    }
+    int rc = materialize(h);
+    if (rc) return rc;
+    const double* src;
+    switch (field) {
+    case IPPI_FIELD_F: src = h->dl; break;
+    case IPPI_FIELD_RHO: src = h->dl + 9 * nn; break;
+    case IPPI_FIELD_UX: src = h->dl + 10 * nn; break;
+    case IPPI_FIELD_UY: src = h->dl + 11 * nn; break;
+    case IPPI_FIELD_NNFLAG: src = h->dl + 12 * nn; break;
+    default: src = h->dl + 13 * nn; break;  // TAU
+    }
+    CK(h, cudaMemcpy(host, src, need, cudaMemcpyDeviceToHost));
+    return IPPI_OK;
+}
+
+int ippi_forces(ippi_lbm* h, double* force_xy, int* nbody, double* mass)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    CK(h, cudaSetDevice(h->p.device));
+    if (nbody) *nbody = h->nbody;
+    if (h->pending_init && (force_xy || mass)) {
+        int rc = materialize(h);
+        if (rc) return rc;
+    }
+    if (force_xy && h->nbody > 0) {
+        CK(h, cudaStreamSynchronize(h->st));
+        CK(h, cudaMemcpy(force_xy, h->force_now, (size_t)h->nbody * 2 * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    if (mass) {
+        int rc = materialize(h);
+        if (rc) return rc;
+        const size_t nn = (size_t)h->p.nx * h->p.ny;
+        const int nblk = 1024;
+        sum_partial_kernel<<<nblk, 256, 0, h->st>>>(h->dl + 9 * nn, (long long)nn, h->red);
+        sum_partial_kernel<<<1, 256, 0, h->st>>>(h->red, nblk, h->red + nblk);
+        CK(h, cudaGetLastError());
+        CK(h, cudaMemcpyAsync(mass, h->red + nblk, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+        CK(h, cudaStreamSynchronize(h->st));
+    }
+    return IPPI_OK;
+}
+
+int ippi_force_history(ippi_lbm* h, double* out, int max_steps)
+{
+    if (!h || (!out && max_steps > 0)) return fail(h, IPPI_ERR_ARG, "null argument");
+    if (h->nbody == 0) return 0;
+    CK(h, cudaSetDevice(h->p.device));
+    CK(h, cudaStreamSynchronize(h->st));
+    const long long avail = std::min<long long>(h->hist_written + (h->pending_init ? 0 : 1), h->hist_cap);
+    const int n = (int)std::min<long long>(avail, max_steps);
+    const int nb = h->nbody;
+    std::vector<double> all((size_t)h->hist_cap * nb * 2);
+    CK(h, cudaMemcpy(all.data(), h->force_hist, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; i++) {
+        const long long t = (long long)h->last_t - (n - 1) + i;
+        const long long slot = ((t % h->hist_cap) + h->hist_cap) % h->hist_cap;
+        std::memcpy(out + (size_t)i * nb * 2, all.data() + (size_t)slot * nb * 2, nb * 2 * sizeof(double));
+    }
+    return n;
+}
+
+int ippi_get_stream(ippi_lbm* h, void** stream)
+{
+    if (!h || !stream) return fail(h, IPPI_ERR_ARG, "null argument");
+    *stream = (void*)h->st;
+    return IPPI_OK;
+}
+
+int ippi_last_error(ippi_lbm* h, char* buf, size_t n)
+{
+    if (!buf || n == 0) return IPPI_ERR_ARG;
+    snprintf(buf, n, "%s", h ? h->err : g_last_error);
+    return IPPI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,42 @@
+// launch.h -- host-side launch descriptors shared by the per-storage kernel
+// translation units (kernels_f64.cu, kernels_f32.cu, kernels_f16.cu,
+// kernels_bf16.cu) and the C-ABI layer (ippi_lbm.cu).
+#pragma once
+
+#include "lbm_kernels.cuh"
+
+namespace ippi {
+
+struct LaunchSet {
+    StepArgs step;
+    dim3 grid;
+    int coll, scene;
+    // side-stream work: prep -> (band) -> (ib), forked from and joined to `stream`
+    const PrepNode* prep;
+    int nprep;
+    bool band;
+    BandArgs band_args;
+    int band_blocks;
+    bool ib;
+    IbArgs ib_args;
+    int ib_blocks;
+    int ib_nst;          // 4 or 16 stencil nodes per marker
+    size_t ib_smem;      // dynamic shared memory of ib_kernel
+    cudaStream_t stream, side;
+    cudaEvent_t fork, join;
+    // optional device timing: events[0..3] around the bulk kernel and the
+    // side-stream chain (only when not capturing)
+    cudaEvent_t* events;
+};
+
+cudaError_t launch_f64(const LaunchSet& L);
+cudaError_t launch_f32(const LaunchSet& L);
+cudaError_t launch_f16(const LaunchSet& L);
+cudaError_t launch_bf16(const LaunchSet& L);
+// raise the dynamic shared-memory limit of the IB kernels (once per device)
+cudaError_t prepare_f64(size_t ib_smem);
+cudaError_t prepare_f32(size_t ib_smem);
+cudaError_t prepare_f16(size_t ib_smem);
+cudaError_t prepare_bf16(size_t ib_smem);
+
+}  // namespace ippi

@@ -1,0 +1,264 @@
+// lbm_common.cuh -- device-side building blocks of the D2Q9 step for sm_100a.
+//
+// Populations live in HBM as structure-of-arrays planes f[k][y][pitch] (x
+// fastest).  FP32/FP16/BF16 storage keeps them shifted by w_k * rho0 (the
+// lattice weight times the reference density) and FP16 additionally scaled by
+// 1024, so the stored numbers are the small deviations from rest; arithmetic
+// is FP32 on those shifted values.  FP64 storage keeps the reference's plain
+// populations and FP64 arithmetic, for parity with the FP64 CPU path.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ippi {
+
+enum { ST_F64 = 0, ST_F32 = 1, ST_F16 = 2, ST_BF16 = 3 };
+enum { CO_BGK = 0, CO_MRT = 1, CO_RR = 2 };
+enum { SC_REF = 0, SC_CHANNEL = 1 };
+
+// per-node side flags (only read in tiles marked special)
+enum : uint8_t { NF_EXPORT = 1, NF_DEFER = 2 };
+
+// step kernel modes
+enum { MODE_STEP = 0, MODE_INIT = 1, MODE_MAT = 2, MODE_MAT_INIT = 3 };
+
+// D2Q9 velocity order of the reference (NodeAndLattice.cpp:3-13):
+// 0 rest, 1 E, 2 N, 3 W, 4 S, 5 NE, 6 NW, 7 SW, 8 SE.
+__host__ __device__ constexpr int EX(int k)
+{
+    return k == 1 || k == 5 || k == 8 ? 1 : (k == 3 || k == 6 || k == 7 ? -1 : 0);
+}
+__host__ __device__ constexpr int EY(int k)
+{
+    return k == 2 || k == 5 || k == 6 ? 1 : (k == 4 || k == 7 || k == 8 ? -1 : 0);
+}
+__host__ __device__ constexpr int OPP(int k)
+{
+    return k == 0 ? 0 : (k <= 4 ? ((k + 1) % 4) + 1 : ((k - 5 + 2) % 4) + 5);
+}
+static_assert(OPP(1) == 3 && OPP(2) == 4 && OPP(3) == 1 && OPP(4) == 2, "opp");
+static_assert(OPP(5) == 7 && OPP(6) == 8 && OPP(7) == 5 && OPP(8) == 6, "opp");
+
+template <typename C>
+__host__ __device__ constexpr C WK(int k)
+{
+    return k == 0 ? C(4.0 / 9.0) : (k <= 4 ? C(1.0 / 9.0) : C(1.0 / 36.0));
+}
+
+// device step counter / status word, one per lattice
+// The kernels of a step with parity p read the user step number from t[p]
+// and one thread of the bulk kernel writes t[p] + 1 into t[p ^ 1] for the
+// next step, so concurrent kernels of one step never see a changing value.
+struct Ctr {
+    int t[2];         // user time step (feeds the averages), by step parity
+    int err;          // 1 once rho left [0,10] or became NaN
+    int err_t;        // first step where that happened
+};
+
+// ----------------------------------------------------------------------------
+// storage traits
+// ----------------------------------------------------------------------------
+template <int S> struct Store;
+template <> struct Store<ST_F64> {
+    using T = double;
+    using C = double;
+    static constexpr bool kShift = false;
+    __device__ static C ld(T v) { return v; }
+    __device__ static T st(C v) { return v; }
+};
+template <> struct Store<ST_F32> {
+    using T = float;
+    using C = float;
+    static constexpr bool kShift = true;
+    __device__ static C ld(T v) { return v; }
+    __device__ static T st(C v) { return v; }
+};
+template <> struct Store<ST_F16> {
+    using T = __half;
+    using C = float;
+    static constexpr bool kShift = true;
+    __device__ static C ld(T v) { return __half2float(v) * (1.0f / 1024.0f); }
+    __device__ static T st(C v) { return __float2half_rn(v * 1024.0f); }
+};
+template <> struct Store<ST_BF16> {
+    using T = __nv_bfloat16;
+    using C = float;
+    static constexpr bool kShift = true;
+    __device__ static C ld(T v) { return __bfloat162float(v); }
+    __device__ static T st(C v) { return __float2bfloat16_rn(v); }
+};
+
+// ----------------------------------------------------------------------------
+// node physics (C = compute type).  `rb` is the population shift base: rho0
+// for shifted storage, 0 for FP64.  Populations f[] are f_k - w_k * rb.
+// ----------------------------------------------------------------------------
+
+// Moments: rho = rb + sum f, u = sum f e / rho (zero below rho 1e-6), the
+// rule of Lattice::CalMacro (NodeAndLattice.cpp:196-227).
+template <typename C>
+__device__ __forceinline__ void macros(const C* f, C rb, C& rho, C& ux, C& uy)
+{
+    C s = ((f[0] + f[1]) + (f[2] + f[3])) + ((f[4] + f[5]) + (f[6] + f[7])) + f[8];
+    C jx = (f[1] - f[3]) + (f[5] - f[6]) + (f[8] - f[7]);
+    C jy = (f[2] - f[4]) + (f[5] + f[6]) - (f[7] + f[8]);
+    rho = rb + s;
+    if (rho < C(1e-6)) {
+        ux = C(0);
+        uy = C(0);
+    } else {
+        C inv = C(1) / rho;
+        ux = jx * inv;
+        uy = jy * inv;
+    }
+}
+
+// Second-order equilibrium (Lattice::Compute_feq, NodeAndLattice.cpp:124-149)
+// in shifted form: feq_k - w_k rb = w_k (rho - rb) + w_k rho (3 eu + 4.5 eu^2 - 1.5 u^2).
+template <typename C>
+__device__ __forceinline__ void equilibrium(C rho, C ux, C uy, C rb, C* feq)
+{
+    const C dr = rho - rb;
+    const C usq = C(1.5) * (ux * ux + uy * uy);
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const C eu = C(EX(k)) * ux + C(EY(k)) * uy;
+        feq[k] = WK<C>(k) * dr + WK<C>(k) * rho * (C(3) * eu + C(4.5) * eu * eu - usq);
+    }
+}
+
+// Non-equilibrium stress Pi_neq = sum e e (f - feq) from moments: the
+// second moments of the 2nd-order equilibrium are rho/3 + rho u u exactly.
+template <typename C>
+__device__ __forceinline__ void pi_neq(const C* f, C rho, C ux, C uy, C rb, C& pxx, C& pxy,
+                                       C& pyy)
+{
+    const C dr3 = (rho - rb) * C(1.0 / 3.0);
+    const C diag = f[5] + f[6] + f[7] + f[8];
+    pxx = (f[1] + f[3] + diag) - dr3 - rho * ux * ux;
+    pyy = (f[2] + f[4] + diag) - dr3 - rho * uy * uy;
+    pxy = (f[5] - f[6] + f[7] - f[8]) - rho * ux * uy;
+}
+
+// Smagorinsky "hybrid" relaxation time (Mesh::CaculateLESTau, mesh.cpp:877-910):
+// S = -3/(2 rho tau0) Pi_neq, Q = sqrt(2 S:S), tau = (sqrt(tau0^2 + 18 Cs^2 Q/rho) + tau0)/2.
+template <typename C>
+__device__ __forceinline__ C les_tau(C pxx, C pxy, C pyy, C rho, C tau0, C cs)
+{
+    const C c = C(-1.5) / (rho * tau0);
+    const C sxx = pxx * c, sxy = pxy * c, syy = pyy * c;
+    const C s2 = sxx * sxx + C(2) * sxy * sxy + syy * syy;
+    const C q = sqrt(C(2) * s2);
+    const C inv_rho = -c * tau0 * C(2.0 / 3.0);  // 1/rho without a second division
+    const C g1 = tau0 * tau0 + C(18) * cs * cs * q * inv_rho;
+    return (sqrt(g1) + tau0) * C(0.5);
+}
+
+// BGK (Lattice::ComputeBGKCollision, NodeAndLattice.cpp:150-161).
+template <typename C>
+__device__ __forceinline__ void collide_bgk(C* f, const C* feq, C tau)
+{
+    const C om = C(1) / tau;
+    const C a = C(1) - om;
+#pragma unroll
+    for (int k = 0; k < 9; k++) f[k] = a * f[k] + feq[k] * om;
+}
+
+// Regularised collision (Lattice::ComputeRRCollision, NodeAndLattice.cpp:228-288):
+// fcol = feq + (1 - 1/tau) 4.5 w_k Q_k : Pi_neq,  Q_k = e_k e_k - I/3.
+template <typename C>
+__device__ __forceinline__ void collide_rr(C* f, const C* feq, C pxx, C pxy, C pyy, C tau)
+{
+    const C a = C(1) - C(1) / tau;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const C qxx = C(EX(k) * EX(k)) - C(1.0 / 3.0);
+        const C qyy = C(EY(k) * EY(k)) - C(1.0 / 3.0);
+        const C qxy = C(EX(k) * EY(k));
+        const C f1 = C(4.5) * WK<C>(k) * (qxx * pxx + C(2) * qxy * pxy + qyy * pyy);
+        f[k] = feq[k] + a * f1;
+    }
+}
+
+// Lallemand-Luo MRT with the reference's rates s = {0, 1.2, 1.1, 0, 1.2, 0,
+// 1.2, 1/tau, 1/tau} (NodeAndLattice.cpp:290-360).  Only the six
+// non-conserved moments relax, so fcol = f - M^-1 S (m - m_eq) reduces to six
+// moment differences and the columns of M^-1 = M^T diag(1/|row|^2).
+template <typename C>
+__device__ __forceinline__ void collide_mrt(C* f, C rho, C ux, C uy, C rb, C tau)
+{
+    const C dr = rho - rb;
+    const C u2 = ux * ux + uy * uy;
+    const C s15 = f[1] + f[2] + f[3] + f[4];
+    const C s58 = f[5] + f[6] + f[7] + f[8];
+    const C m1 = C(-4) * f[0] - s15 + C(2) * s58;
+    const C m2 = C(4) * f[0] - C(2) * s15 + s58;
+    const C m4 = C(-2) * (f[1] - f[3]) + (f[5] - f[6] - f[7] + f[8]);
+    const C m6 = C(-2) * (f[2] - f[4]) + (f[5] + f[6] - f[7] - f[8]);
+    const C m7 = (f[1] + f[3]) - (f[2] + f[4]);
+    const C m8 = f[5] - f[6] + f[7] - f[8];
+    const C om = C(1) / tau;
+    const C a1 = C(1.2) * (m1 + C(2) * dr - C(3) * rho * u2) * C(1.0 / 36.0);
+    const C a2 = C(1.1) * (m2 - dr + C(3) * rho * u2) * C(1.0 / 36.0);
+    const C a4 = C(1.2) * (m4 + rho * ux) * C(1.0 / 12.0);
+    const C a6 = C(1.2) * (m6 + rho * uy) * C(1.0 / 12.0);
+    const C a7 = om * (m7 - rho * (ux * ux - uy * uy)) * C(0.25);
+    const C a8 = om * (m8 - rho * ux * uy) * C(0.25);
+    f[0] -= C(-4) * a1 + C(4) * a2;
+    f[1] -= -a1 - C(2) * a2 - C(2) * a4 + a7;
+    f[2] -= -a1 - C(2) * a2 - C(2) * a6 - a7;
+    f[3] -= -a1 - C(2) * a2 + C(2) * a4 + a7;
+    f[4] -= -a1 - C(2) * a2 + C(2) * a6 - a7;
+    f[5] -= C(2) * a1 + a2 + a4 + a6 + a8;
+    f[6] -= C(2) * a1 + a2 - a4 + a6 - a8;
+    f[7] -= C(2) * a1 + a2 - a4 - a6 + a8;
+    f[8] -= C(2) * a1 + a2 + a4 - a6 - a8;
+}
+
+// Guo forcing term (Lattice::Compute_Disforce, NodeAndLattice.cpp:162-195),
+// with omega from the initial relaxation time: added to the post-collision
+// populations of forced nodes.
+template <typename C>
+__device__ __forceinline__ void add_guo(C* f, C ux, C uy, C fx, C fy, C tau0)
+{
+    const C om = C(1) - C(0.5) * (C(1) / tau0);
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const C eu = C(EX(k)) * ux + C(EY(k)) * uy;
+        const C gx = (C(3) * (C(EX(k)) - ux) + C(9) * eu * C(EX(k))) * fx;
+        const C gy = (C(3) * (C(EY(k)) - uy) + C(9) * eu * C(EY(k))) * fy;
+        f[k] += WK<C>(k) * om * (gx + gy);
+    }
+}
+
+// Relax one node's populations in place with the chosen operator.
+template <typename C, int CO>
+__device__ __forceinline__ void collide_node(C* f, C rho, C ux, C uy, C rb, C tau)
+{
+    if (CO == CO_MRT) {
+        collide_mrt<C>(f, rho, ux, uy, rb, tau);
+    } else {
+        C feq[9];
+        equilibrium<C>(rho, ux, uy, rb, feq);
+        if (CO == CO_RR) {
+            C pxx, pxy, pyy;
+            pi_neq<C>(f, rho, ux, uy, rb, pxx, pxy, pyy);
+            collide_rr<C>(f, feq, pxx, pxy, pyy, tau);
+        } else {
+            collide_bgk<C>(f, feq, tau);
+        }
+    }
+}
+
+template <typename C>
+__device__ __forceinline__ C node_tau(const C* f, C rho, C ux, C uy, C rb, int les, C tau0, C cs)
+{
+    if (!les) return tau0;
+    C pxx, pxy, pyy;
+    pi_neq<C>(f, rho, ux, uy, rb, pxx, pxy, pyy);
+    return les_tau<C>(pxx, pxy, pyy, rho, tau0, cs);
+}
+
+}  // namespace ippi

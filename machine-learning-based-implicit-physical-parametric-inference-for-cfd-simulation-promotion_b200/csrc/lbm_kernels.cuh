@@ -1,0 +1,810 @@
+// lbm_kernels.cuh -- the time-step kernels (sm_100a).
+//
+// One time step is
+//   step_kernel   every node that is not deferred: pull-stream the 9
+//                 post-collision populations of its neighbours, apply the
+//                 boundary rule of its kind, take the moments, Smagorinsky
+//                 tau + collision, store the 9 new post-collision
+//                 populations.  HBM traffic per node: 9 loads + 9 stores.
+// and, on a side stream running concurrently with it,
+//   prep_kernel   the post-stream state of the few nodes other kernels need
+//                 (boundary-net inputs, IB stencil nodes) into side buffers
+//   band_kernel   (flat plate with boundary nets) the nets' MLP on the band
+//                 nodes, then their collision
+//   ib_kernel     (immersed boundary) interpolation, direct forcing,
+//                 spreading, velocity correction, forced collision with the
+//                 Guo term, per-body force sums
+// A node is "deferred" when its collision needs moments of other nodes of
+// the same step (net inputs, marker forces); step_kernel skips it and the
+// side-stream kernels own it.  All kernels of a step read only the previous
+// field and write disjoint nodes of the next one.
+//
+// The stored state between steps is the post-collision field; one launch of
+// step_kernel performs Mesh::Streaming + Mesh::BoundaryCondition of step t
+// (mesh.cpp:192-356) and the LES + collision loop of step t+1
+// (mesh.cpp:386-437).
+#pragma once
+
+#include "lbm_common.cuh"
+
+namespace ippi {
+
+constexpr int kBlockX = 256;
+
+struct StepArgs {
+    const void* f_in;   // post-collision populations of the previous step
+    void* f_out;        // post-collision populations of this step
+    long long pitch;    // row pitch (elements)
+    long long plane;    // plane stride (elements)
+    int nx, ny;
+    int les;
+    int plate_x0;
+    double tau0, cs, u_in, rho0;
+    float f_tau0, f_cs, f_u_in, f_rho0;  // the same in FP32 (no conversions per node)
+    const uint8_t* tile;  // [gy][gx] 1 = some node of this block is deferred
+    int tiles_x;
+    const uint8_t* nflag; // [ny][nx] NF_* bits
+    void* side_f;         // [nslots][9] compute type: fnew of deferred nodes
+    void* side_m;         // [2][nslots][3] compute type: rho, ux, uy (by step parity)
+    int nslots;
+    void* corner;         // flat plate: [2][12] fixed bottom corners (f[9], rho, ux, uy)
+    void* avg;            // [3][ny][nx] compute type: running means of ux, uy, rho
+    int avg_start;
+    Ctr* ctr;
+    int mode;             // MODE_*
+    int par;              // step parity: side-buffer half and ctr->t entry
+    int fixed_t;          // step number for the MAT modes
+    const double* init_m; // [3][ny][nx] initial rho, ux, uy (INIT modes)
+    double* dl_f;         // MAT: fnew [9][ny][nx]
+    double* dl_m;         // MAT: rho, ux, uy, boundary-net flag [4][ny][nx]
+    double* dl_tau;       // MAT: tau of the next collision [ny][nx]
+};
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+// a run parameter in the compute type (FP64 or its FP32 copy)
+template <typename C> __device__ __forceinline__ C prm(double d, float f);
+template <> __device__ __forceinline__ double prm<double>(double d, float) { return d; }
+template <> __device__ __forceinline__ float prm<float>(double, float f) { return f; }
+
+// element offsets fit in 32 bits (ippi_create bounds 9 * pitch * ny)
+template <int S>
+__device__ __forceinline__ typename Store<S>::C ldf(const StepArgs& a, int k, int x, int y)
+{
+    using T = typename Store<S>::T;
+    const T* p = reinterpret_cast<const T*>(a.f_in);
+    return Store<S>::ld(__ldg(p + (unsigned)(k * (int)a.plane + y * (int)a.pitch + x)));
+}
+
+template <int S>
+__device__ __forceinline__ void stf(const StepArgs& a, int k, int x, int y, typename Store<S>::C v)
+{
+    using T = typename Store<S>::T;
+    T* p = reinterpret_cast<T*>(a.f_out);
+    p[(unsigned)(k * (int)a.plane + y * (int)a.pitch + x)] = Store<S>::st(v);
+}
+
+template <int S>
+__device__ __forceinline__ typename Store<S>::C rbase(const StepArgs& a)
+{
+    using C = typename Store<S>::C;
+    return Store<S>::kShift ? prm<C>(a.rho0, a.f_rho0) : C(0);
+}
+
+// plain pull of all 9 populations (all sources inside the lattice)
+template <int S>
+__device__ __forceinline__ void pull(const StepArgs& a, int x, int y, typename Store<S>::C* f)
+{
+#pragma unroll
+    for (int k = 0; k < 9; k++) f[k] = ldf<S>(a, k, x - EX(k), y - EY(k));
+}
+
+// non-equilibrium extrapolation: f(A) = feq(A) + f(B) - feq(B)
+template <typename C>
+__device__ __forceinline__ void nee(C* f, C rhoA, C uxA, C uyA, C rhoB, C uxB, C uyB, C rb)
+{
+    C ea[9], eb[9];
+    equilibrium<C>(rhoA, uxA, uyA, rb, ea);
+    equilibrium<C>(rhoB, uxB, uyB, rb, eb);
+#pragma unroll
+    for (int k = 0; k < 9; k++) f[k] = (ea[k] + f[k]) - eb[k];
+}
+
+// ---------------------------------------------------------------------------
+// flat-plate scene (Mesh::JudgeStyle mesh.cpp:1398-1425 and
+// Mesh::BoundaryCondition mesh.cpp:228-356, one rank, global coordinates)
+// ---------------------------------------------------------------------------
+enum RefKind { RK_FLUID, RK_INLET, RK_OUTLET, RK_TOP, RK_TOP_IN, RK_TOP_OUT, RK_BOT_SPEC,
+               RK_BOT_NEE, RK_FIXED };
+
+__host__ __device__ __forceinline__ int ref_kind(int x, int y, int nx, int ny, int plate_x0)
+{
+    if (y == 0 && (x == 0 || x == nx - 1)) return RK_FIXED;  // 'i'/'o' corners never updated
+    if (x == 0) return y == ny - 1 ? RK_TOP_IN : RK_INLET;
+    if (x == nx - 1) return y == ny - 1 ? RK_TOP_OUT : RK_OUTLET;
+    if (y == ny - 1) return RK_TOP;
+    if (y == 0) return x < plate_x0 ? RK_BOT_SPEC : RK_BOT_NEE;
+    return RK_FLUID;
+}
+
+__host__ __device__ __forceinline__ char ref_style(int x, int y, int nx, int ny, int plate_x0)
+{
+    switch (ref_kind(x, y, nx, ny, plate_x0)) {
+    case RK_FIXED: return x == 0 ? 'i' : 'o';
+    case RK_INLET:
+    case RK_TOP_IN: return 'i';
+    case RK_OUTLET:
+    case RK_TOP_OUT: return 'o';
+    case RK_TOP: return 'u';
+    case RK_BOT_SPEC: return 'm';
+    case RK_BOT_NEE: return 'd';
+    default: return 'f';
+    }
+}
+
+// pulled fluid node (x, y) with its moments
+template <int S>
+__device__ __forceinline__ void ref_fluid(const StepArgs& a, int x, int y, typename Store<S>::C* f,
+                                          typename Store<S>::C& rho, typename Store<S>::C& ux,
+                                          typename Store<S>::C& uy)
+{
+    using C = typename Store<S>::C;
+    pull<S>(a, x, y, f);
+    macros<C>(f, rbase<S>(a), rho, ux, uy);
+}
+
+// inlet node (0, y), 1 <= y <= ny-2: rho = 1, u = (u_in, 0), NEE from (1, y)
+template <int S>
+__device__ __forceinline__ void ref_inlet(const StepArgs& a, int y, typename Store<S>::C* f,
+                                          typename Store<S>::C& rho, typename Store<S>::C& ux,
+                                          typename Store<S>::C& uy)
+{
+    using C = typename Store<S>::C;
+    C rb, ub, vb;
+    ref_fluid<S>(a, 1, y, f, rb, ub, vb);
+    rho = C(1);
+    ux = prm<C>(a.u_in, a.f_u_in);
+    uy = C(0);
+    nee<C>(f, rho, ux, uy, rb, ub, vb, rbase<S>(a));
+}
+
+// outlet node (nx-1, y), 1 <= y <= ny-2: rho = 1, u = u(nx-2, y), NEE
+template <int S>
+__device__ __forceinline__ void ref_outlet(const StepArgs& a, int y, typename Store<S>::C* f,
+                                           typename Store<S>::C& rho, typename Store<S>::C& ux,
+                                           typename Store<S>::C& uy)
+{
+    using C = typename Store<S>::C;
+    C rb, ub, vb;
+    ref_fluid<S>(a, a.nx - 2, y, f, rb, ub, vb);
+    rho = C(1);
+    ux = ub;
+    uy = vb;
+    nee<C>(f, rho, ux, uy, rb, ub, vb, rbase<S>(a));
+}
+
+template <int S>
+__device__ void ref_state(const StepArgs& a, int x, int y, typename Store<S>::C* f,
+                          typename Store<S>::C& rho, typename Store<S>::C& ux,
+                          typename Store<S>::C& uy)
+{
+    using C = typename Store<S>::C;
+    const C rbs = rbase<S>(a);
+    const int kind = ref_kind(x, y, a.nx, a.ny, a.plate_x0);
+    switch (kind) {
+    case RK_FLUID: ref_fluid<S>(a, x, y, f, rho, ux, uy); break;
+    case RK_INLET: ref_inlet<S>(a, y, f, rho, ux, uy); break;
+    case RK_OUTLET: ref_outlet<S>(a, y, f, rho, ux, uy); break;
+    case RK_TOP: {
+        C rb, ub, vb;
+        ref_fluid<S>(a, x, a.ny - 2, f, rb, ub, vb);
+        rho = C(1);
+        ux = ub;
+        uy = vb;
+        nee<C>(f, rho, ux, uy, rb, ub, vb, rbs);
+    } break;
+    case RK_TOP_IN: {
+        C rb, ub, vb;
+        ref_inlet<S>(a, a.ny - 2, f, rb, ub, vb);
+        rho = C(1);
+        ux = ub;
+        uy = vb;
+        nee<C>(f, rho, ux, uy, rb, ub, vb, rbs);
+    } break;
+    case RK_TOP_OUT: {
+        C rb, ub, vb;
+        ref_outlet<S>(a, a.ny - 2, f, rb, ub, vb);
+        rho = C(1);
+        ux = ub;
+        uy = vb;
+        nee<C>(f, rho, ux, uy, rb, ub, vb, rbs);
+    } break;
+    case RK_BOT_SPEC: {
+        // specular reflection pulls of mesh.cpp:327-335
+        f[0] = ldf<S>(a, 0, x, 0);
+        f[1] = ldf<S>(a, 1, x - 1, 0);
+        f[2] = ldf<S>(a, 4, x, 1);
+        f[3] = ldf<S>(a, 3, x + 1, 0);
+        f[4] = ldf<S>(a, 4, x, 1);
+        f[5] = ldf<S>(a, 8, x - 1, 1);
+        f[6] = ldf<S>(a, 7, x + 1, 1);
+        f[7] = ldf<S>(a, 7, x + 1, 1);
+        f[8] = ldf<S>(a, 8, x - 1, 1);
+        macros<C>(f, rbs, rho, ux, uy);
+    } break;
+    case RK_BOT_NEE: {
+        C rb, ub, vb;
+        ref_fluid<S>(a, x, 1, f, rb, ub, vb);
+        rho = rb;
+        ux = C(0);
+        uy = C(0);
+        nee<C>(f, rho, ux, uy, rb, ub, vb, rbs);
+    } break;
+    default: {  // RK_FIXED: populations and moments as initialised
+        const C* c = reinterpret_cast<const C*>(a.corner) + (x == 0 ? 0 : 12);
+#pragma unroll
+        for (int k = 0; k < 9; k++) f[k] = c[k];
+        rho = c[9];
+        ux = c[10];
+        uy = c[11];
+    } break;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// channel scene: halfway bounce-back walls at y = -1/2 and ny - 1/2,
+// parabolic Zou-He velocity inlet at x = 0, the reference's NEE outlet
+// (rho0, u from x = nx-2) at x = nx-1.
+// ---------------------------------------------------------------------------
+template <typename C>
+__device__ __forceinline__ C inlet_profile(int y, int ny, C umax)
+{
+    const C H = C(ny);
+    const C yy = C(y) + C(0.5);
+    return C(4) * umax * yy * (H - yy) / (H * H);
+}
+
+template <int S>
+__device__ __forceinline__ void ch_pull(const StepArgs& a, int x, int y, typename Store<S>::C* f)
+{
+    if (x >= 1 && y >= 1 && y <= a.ny - 2) {  // x <= nx - 2 for every caller
+        pull<S>(a, x, y, f);
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const int sx = x - EX(k), sy = y - EY(k);
+        if (sy < 0 || sy >= a.ny)
+            f[k] = ldf<S>(a, OPP(k), x, y);
+        else if (sx < 0)
+            f[k] = 0;
+        else
+            f[k] = ldf<S>(a, k, sx, sy);
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void ch_fluid(const StepArgs& a, int x, int y, typename Store<S>::C* f,
+                                         typename Store<S>::C& rho, typename Store<S>::C& ux,
+                                         typename Store<S>::C& uy)
+{
+    using C = typename Store<S>::C;
+    const C rbs = rbase<S>(a);
+    ch_pull<S>(a, x, y, f);
+    if (x == 0) {
+        // Zou-He velocity inlet (west): unknown 1, 5, 8.  In shifted
+        // populations rho - rb = (S + rb u)/(1 - u), the rest is unchanged.
+        const C u = inlet_profile<C>(y, a.ny, prm<C>(a.u_in, a.f_u_in));
+        const C sk = f[0] + f[2] + f[4] + C(2) * (f[3] + f[6] + f[7]);
+        const C r = rbs + (sk + rbs * u) / (C(1) - u);
+        f[1] = f[3] + C(2.0 / 3.0) * r * u;
+        f[5] = f[7] - C(0.5) * (f[2] - f[4]) + C(1.0 / 6.0) * r * u;
+        f[8] = f[6] + C(0.5) * (f[2] - f[4]) + C(1.0 / 6.0) * r * u;
+    }
+    macros<C>(f, rbs, rho, ux, uy);
+}
+
+template <int S>
+__device__ void ch_state(const StepArgs& a, int x, int y, typename Store<S>::C* f,
+                         typename Store<S>::C& rho, typename Store<S>::C& ux,
+                         typename Store<S>::C& uy)
+{
+    using C = typename Store<S>::C;
+    if (x == a.nx - 1) {
+        C rb, ub, vb;
+        ch_fluid<S>(a, a.nx - 2, y, f, rb, ub, vb);
+        rho = prm<C>(a.rho0, a.f_rho0);
+        ux = ub;
+        uy = vb;
+        nee<C>(f, rho, ux, uy, rb, ub, vb, rbase<S>(a));
+    } else {
+        ch_fluid<S>(a, x, y, f, rho, ux, uy);
+    }
+}
+// ---------------------------------------------------------------------------
+// shared epilogue pieces
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void flag_error(Ctr* c, int t)
+{
+    if (atomicExch(&c->err, 1) == 0) c->err_t = t;
+}
+
+__device__ __forceinline__ int step_time(const StepArgs& a)
+{
+    return a.mode >= MODE_MAT ? a.fixed_t : __ldcg(&a.ctr->t[a.par]);
+}
+
+// post-stream state of node (x, y): the boundary rule of its kind and its
+// moments, or (INIT modes) the equilibrium of the initial moments
+template <int S, int SC>
+__device__ __forceinline__ void node_state(const StepArgs& a, int x, int y, typename Store<S>::C* f,
+                                           typename Store<S>::C& rho, typename Store<S>::C& ux,
+                                           typename Store<S>::C& uy)
+{
+    using C = typename Store<S>::C;
+    if (a.mode == MODE_INIT || a.mode == MODE_MAT_INIT) {
+        // Lattice::InitialLatticeFeq: populations at equilibrium of the given moments
+        const long long node = (long long)y * a.nx + x;
+        const long long pl = (long long)a.nx * a.ny;
+        rho = C(a.init_m[node]);
+        ux = C(a.init_m[pl + node]);
+        uy = C(a.init_m[2 * pl + node]);
+        equilibrium<C>(rho, ux, uy, rbase<S>(a), f);
+        if (SC == SC_REF && a.mode == MODE_INIT &&
+            ref_kind(x, y, a.nx, a.ny, a.plate_x0) == RK_FIXED) {
+            C* c = reinterpret_cast<C*>(a.corner) + (x == 0 ? 0 : 12);
+#pragma unroll
+            for (int q = 0; q < 9; q++) c[q] = f[q];
+            c[9] = rho;
+            c[10] = ux;
+            c[11] = uy;
+        }
+    } else if (SC == SC_REF) {
+        ref_state<S>(a, x, y, f, rho, ux, uy);
+    } else {
+        ch_state<S>(a, x, y, f, rho, ux, uy);
+    }
+}
+
+// averages, error check and download outputs of one node's post-stream state
+template <int S>
+__device__ __forceinline__ void node_epilogue(const StepArgs& a, long long node, int t,
+                                              const typename Store<S>::C* f,
+                                              typename Store<S>::C rho, typename Store<S>::C ux,
+                                              typename Store<S>::C uy)
+{
+    using C = typename Store<S>::C;
+    const long long pl = (long long)a.nx * a.ny;
+    if (a.mode < MODE_MAT) {
+        if (a.mode == MODE_STEP && t >= a.avg_start) {
+            // Mesh::ComputeAvgVelocity (mesh.cpp:1969-1971)
+            C* av = reinterpret_cast<C*>(a.avg);
+            const C n0 = C(t - a.avg_start), n1 = C(t - a.avg_start + 1);
+            av[node] = (av[node] * n0 + ux) / n1;
+            av[pl + node] = (av[pl + node] * n0 + uy) / n1;
+            av[2 * pl + node] = (av[2 * pl + node] * n0 + rho) / n1;
+        }
+        // Mesh::ErrorCatch (mesh.cpp:2103): rho outside [0, 10]; NaN too
+        if (!(rho <= C(10) && rho >= C(0))) flag_error(a.ctr, t);
+    } else {
+        const C rbs = rbase<S>(a);
+#pragma unroll
+        for (int q = 0; q < 9; q++) a.dl_f[q * pl + node] = double(f[q] + WK<C>(q) * rbs);
+        a.dl_m[node] = double(rho);
+        a.dl_m[pl + node] = double(ux);
+        a.dl_m[2 * pl + node] = double(uy);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// the fused stream + boundary + collide kernel (every node not deferred)
+// ---------------------------------------------------------------------------
+template <int S, int CO, int SC>
+__global__ void __launch_bounds__(kBlockX) step_kernel(const StepArgs a)
+{
+    using C = typename Store<S>::C;
+    const int x = blockIdx.x * kBlockX + threadIdx.x;
+    const int y = blockIdx.y;
+    const int t = step_time(a);
+    if (x < a.nx) {
+        const long long node = (long long)y * a.nx + x;
+        uint8_t nf = 0;
+        if (a.tile[blockIdx.y * a.tiles_x + blockIdx.x]) nf = a.nflag[node];
+        const bool deferred = nf & NF_DEFER;
+        if (!deferred || a.mode == MODE_INIT) {
+            const C rbs = rbase<S>(a);
+            C f[9], rho, ux, uy;
+            node_state<S, SC>(a, x, y, f, rho, ux, uy);
+            if (!deferred) {
+                node_epilogue<S>(a, node, t, f, rho, ux, uy);
+                const C tau = node_tau<C>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0), prm<C>(a.cs, a.f_cs));
+                if (a.mode >= MODE_MAT) {
+                    a.dl_tau[node] = double(tau);
+                } else {
+                    collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
+#pragma unroll
+                    for (int q = 0; q < 9; q++) stf<S>(a, q, x, y, f[q]);
+                }
+            }
+        }
+    }
+    if (a.mode < MODE_MAT && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+        a.ctr->t[a.par ^ 1] = t + 1;
+}
+
+// ---------------------------------------------------------------------------
+// side-stream prep: post-stream state of the nodes other kernels need --
+// inputs of the boundary nets and IB stencil nodes (moments into side_m) and
+// deferred nodes (populations into side_f, plus their averages / outputs).
+// Runs concurrently with step_kernel: both only read f_in.
+// ---------------------------------------------------------------------------
+struct PrepNode {
+    int x, y, slot, flags;
+};
+
+template <int S, int SC>
+__global__ void __launch_bounds__(256) prep_kernel(const StepArgs a, const PrepNode* nodes, int n)
+{
+    using C = typename Store<S>::C;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const PrepNode pn = nodes[i];
+    const int t = step_time(a);
+    C f[9], rho, ux, uy;
+    node_state<S, SC>(a, pn.x, pn.y, f, rho, ux, uy);
+    C* sm = reinterpret_cast<C*>(a.side_m) + ((long long)a.par * a.nslots + pn.slot) * 3;
+    sm[0] = rho;
+    sm[1] = ux;
+    sm[2] = uy;
+    if (pn.flags & NF_DEFER) {
+        C* sf = reinterpret_cast<C*>(a.side_f) + (long long)pn.slot * 9;
+#pragma unroll
+        for (int q = 0; q < 9; q++) sf[q] = f[q];
+        node_epilogue<S>(a, (long long)pn.y * a.nx + pn.x, t, f, rho, ux, uy);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// boundary nets (Mesh::NNmodel_Type00..07, mesh.cpp:2767-3259)
+// ---------------------------------------------------------------------------
+constexpr int kBandNodes = 32;     // band nodes per block
+constexpr int kBandThreads = 256;  // 128 neurons x 2 node halves
+constexpr int kHidden = 128;
+
+struct BandNode {
+    int x, y, slot, nin;   // nin = 15 or 9
+    int nb_slot[5];
+    int nb_stale;          // bit q: neighbour q reads the previous step's moments
+};
+
+struct BandNet {            // weights transposed to [in][out] for coalesced reads
+    const float* w1t;       // [nin][128]
+    const float* b1;        // [128]
+    const float* wht;       // [6][128][128]
+    const float* bh;        // [6][128]
+    const float* wo;        // [128]
+    float bo;
+};
+
+struct BandArgs {
+    const BandNode* nodes;
+    const int2* work;       // per block: (first node, count); all of one net type
+    const int* work_type;
+    BandNet net[8];
+    StepArgs s;
+};
+
+template <int S, int CO>
+__global__ void __launch_bounds__(kBandThreads) band_kernel(const BandArgs ba)
+{
+    using C = typename Store<S>::C;
+    const StepArgs& a = ba.s;
+    __shared__ __align__(16) float act[2][kBandNodes][kHidden];
+    __shared__ float out[kBandNodes];
+    const int2 w = ba.work[blockIdx.x];
+    const BandNet& net = ba.net[ba.work_type[blockIdx.x]];
+    const C* sm_cur = reinterpret_cast<const C*>(a.side_m) + (long long)a.par * a.nslots * 3;
+    const C* sm_old = reinterpret_cast<const C*>(a.side_m) + (long long)(a.par ^ 1) * a.nslots * 3;
+    const int tid = threadIdx.x;
+    const int nin = ba.nodes[w.x].nin;
+
+    // inputs: (u_x, u_y, rho) of each neighbour cast to float (mesh.cpp:2805-2808)
+    for (int i = tid; i < kBandNodes * 15; i += kBandThreads) {
+        const int n = i / 15, q = i % 15;
+        float v = 0.f;
+        if (n < w.y && q < nin) {
+            const BandNode& bn = ba.nodes[w.x + n];
+            const int nb = q / 3, comp = q % 3;
+            const C* m = ((bn.nb_stale >> nb) & 1) ? sm_old : sm_cur;
+            const C* mm = m + (long long)bn.nb_slot[nb] * 3;
+            v = float(comp == 0 ? mm[1] : (comp == 1 ? mm[2] : mm[0]));
+        }
+        act[0][n][q] = v;
+    }
+    __syncthreads();
+
+    const int o = tid & (kHidden - 1);
+    const int half = tid >> 7;  // nodes half*16 .. half*16+15
+    float acc[16];
+    // layer 1: Linear(nin, 128) + ReLU
+#pragma unroll
+    for (int n = 0; n < 16; n++) acc[n] = net.b1[o];
+    for (int i = 0; i < nin; i++) {
+        const float wv = net.w1t[i * kHidden + o];
+#pragma unroll
+        for (int n = 0; n < 16; n++) acc[n] = fmaf(wv, act[0][half * 16 + n][i], acc[n]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int n = 0; n < 16; n++) act[1][half * 16 + n][o] = fmaxf(acc[n], 0.f);
+    __syncthreads();
+    // hidden layers 2..7: Linear(128, 128) + ReLU
+    int cur = 1;
+    for (int l = 0; l < 6; l++) {
+        const float* wt = net.wht + (long long)l * kHidden * kHidden;
+#pragma unroll
+        for (int n = 0; n < 16; n++) acc[n] = net.bh[l * kHidden + o];
+        for (int i = 0; i < kHidden; i += 4) {
+            const float w0 = wt[(i + 0) * kHidden + o];
+            const float w1 = wt[(i + 1) * kHidden + o];
+            const float w2 = wt[(i + 2) * kHidden + o];
+            const float w3 = wt[(i + 3) * kHidden + o];
+#pragma unroll
+            for (int n = 0; n < 16; n++) {
+                const float4 x4 = *reinterpret_cast<const float4*>(&act[cur][half * 16 + n][i]);
+                acc[n] = fmaf(w0, x4.x, acc[n]);
+                acc[n] = fmaf(w1, x4.y, acc[n]);
+                acc[n] = fmaf(w2, x4.z, acc[n]);
+                acc[n] = fmaf(w3, x4.w, acc[n]);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int n = 0; n < 16; n++) act[cur ^ 1][half * 16 + n][o] = fmaxf(acc[n], 0.f);
+        cur ^= 1;
+        __syncthreads();
+    }
+    // output layer: Linear(128, 1), one warp per 4 nodes
+    {
+        const int warp = tid >> 5, lane = tid & 31;
+        for (int n = warp; n < kBandNodes; n += kBandThreads / 32) {
+            float v = 0.f;
+            for (int i = lane; i < kHidden; i += 32) v = fmaf(net.wo[i], act[cur][n][i], v);
+#pragma unroll
+            for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            if (lane == 0) out[n] = v + net.bo;
+        }
+    }
+    __syncthreads();
+
+    // tau (net output if >= 0.501, else Smagorinsky; mesh.cpp:2821-2827,
+    // 392-396) and the collision of the band node
+    if (tid < w.y) {
+        const BandNode& bn = ba.nodes[w.x + tid];
+        const double nn_tau = (double)out[tid];
+        const C* sf = reinterpret_cast<const C*>(a.side_f) + (long long)bn.slot * 9;
+        const C* mm = sm_cur + (long long)bn.slot * 3;
+        C f[9];
+#pragma unroll
+        for (int q = 0; q < 9; q++) f[q] = sf[q];
+        const C rho = mm[0], ux = mm[1], uy = mm[2];
+        const C rbs = rbase<S>(a);
+        const bool use_nn = nn_tau >= 0.501;
+        const C tau = use_nn ? C(nn_tau) : node_tau<C>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0), prm<C>(a.cs, a.f_cs));
+        const long long node = (long long)bn.y * a.nx + bn.x;
+        if (a.mode >= MODE_MAT) {
+            a.dl_tau[node] = double(tau);
+            a.dl_m[3ll * a.nx * a.ny + node] = use_nn ? 1.0 : 0.0;
+        } else {
+            collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
+#pragma unroll
+            for (int q = 0; q < 9; q++) stf<S>(a, q, bn.x, bn.y, f[q]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// immersed boundary (mesh.cpp:514-832, 1244-1281 and NodeAndLattice.cpp:162-195)
+// One block per group of bodies that share no stencil node with another
+// group; per-node and per-marker work arrays live in shared memory.
+// ---------------------------------------------------------------------------
+constexpr int kIbThreads = 512;
+
+struct IbArgs {
+    // markers (sorted by group, then body)
+    int nmark;
+    const double2* ub;          // prescribed velocity
+    const double* ds;           // arc length (force weight)
+    const int* st_node;         // [nmark][16] stencil node: index within the group's nodes
+    const double2* st_w;        // [nmark][16] (wa, wb): contribution (v * wa) * wb
+    // forced nodes (one per stencil node), CSR node -> (marker, wa, wb)
+    const int* fn_slot;         // side-buffer slot
+    const int2* fn_xy;
+    const int* fn_ptr;          // [nforced + 1]
+    const int* fe_marker;       // marker index within the group
+    const double2* fe_w;
+    const int4* group;          // (first marker, end marker, first node, end node)
+    const int2* gbody;          // per group: (first body, end body)
+    const int2* body_m;         // per body: (first marker, end marker)
+    double* force_now;          // [nbody][2]
+    double* force_hist;         // [hist_cap][nbody][2]
+    int nbody, hist_cap;
+    int mdf_iters;
+    StepArgs s;
+};
+
+template <int S, int CO, int NST>
+__global__ void __launch_bounds__(kIbThreads) ib_kernel(const IbArgs ia)
+{
+    using C = typename Store<S>::C;
+    const StepArgs& a = ia.s;
+    const int4 g = ia.group[blockIdx.x];
+    const int t = step_time(a);
+    const int nm = g.y - g.x, nn = g.w - g.z;
+    const C* sm = reinterpret_cast<const C*>(a.side_m) + (long long)a.par * a.nslots * 3;
+    const int tid = threadIdx.x;
+    extern __shared__ __align__(16) double ib_smem[];
+    // node arrays padded to an even length so the double2 marker arrays
+    // after them start on a 16-byte boundary (layout of ib_smem_bytes)
+    const int nnp = (nn + 1) & ~1;
+    double* ucx = ib_smem;
+    double* ucy = ucx + nnp;
+    double* fx = ucy + nnp;
+    double* fy = fx + nnp;
+    double* rh = fy + nnp;
+    double2* dmf = reinterpret_cast<double2*>(rh + nnp);
+    double2* mft = dmf + nm;
+    __shared__ double red[2][kIbThreads];
+
+    for (int n = tid; n < nn; n += kIbThreads) {
+        const C* m = sm + (long long)ia.fn_slot[g.z + n] * 3;
+        rh[n] = double(m[0]);
+        ucx[n] = double(m[1]);
+        ucy[n] = double(m[2]);
+        fx[n] = 0.0;
+        fy[n] = 0.0;
+    }
+    for (int m = tid; m < nm; m += kIbThreads) mft[m] = make_double2(0.0, 0.0);
+    __syncthreads();
+
+    for (int it = 0; it < ia.mdf_iters; it++) {
+        // InterpolateVel + CalParticleForce: F = 2 (U_b - sum u delta)
+        for (int m = tid; m < nm; m += kIbThreads) {
+            const int gm = g.x + m;
+            int sn[NST];
+            double2 sw[NST];
+#pragma unroll
+            for (int q = 0; q < NST; q++) {
+                sn[q] = ia.st_node[gm * 16 + q];
+                sw[q] = ia.st_w[gm * 16 + q];
+            }
+            double vx = 0.0, vy = 0.0;
+#pragma unroll
+            for (int q = 0; q < NST; q++) {
+                vx += ucx[sn[q]] * sw[q].x * sw[q].y;
+                vy += ucy[sn[q]] * sw[q].x * sw[q].y;
+            }
+            const double2 u = ia.ub[gm];
+            const double2 d = make_double2(2.0 * (u.x - vx), 2.0 * (u.y - vy));
+            dmf[m] = d;
+            mft[m] = make_double2(mft[m].x + d.x, mft[m].y + d.y);
+        }
+        __syncthreads();
+        // SpreadForce + UpdateVelocity: u += F / (2 rho), markers in order
+        for (int n = tid; n < nn; n += kIbThreads) {
+            double dfx = 0.0, dfy = 0.0;
+            const int e1 = ia.fn_ptr[g.z + n + 1];
+            for (int e = ia.fn_ptr[g.z + n]; e < e1; e++) {
+                const double2 d = dmf[ia.fe_marker[e]];
+                const double2 wq = ia.fe_w[e];
+                dfx += d.x * wq.x * wq.y;
+                dfy += d.y * wq.x * wq.y;
+            }
+            ucx[n] = ucx[n] + 0.5 * 1 * dfx / rh[n];
+            ucy[n] = ucy[n] + 0.5 * 1 * dfy / rh[n];
+            fx[n] += dfx;
+            fy[n] += dfy;
+        }
+        __syncthreads();
+    }
+
+    // body forces: -sum F ds per body (tree reduction in FP64)
+    const int2 gb = ia.gbody[blockIdx.x];
+    for (int b = gb.x; b < gb.y; b++) {
+        const int2 mr = ia.body_m[b];
+        double sx = 0.0, sy = 0.0;
+        for (int m = mr.x + tid; m < mr.y; m += kIbThreads) {
+            sx -= mft[m - g.x].x * ia.ds[m];
+            sy -= mft[m - g.x].y * ia.ds[m];
+        }
+        red[0][tid] = sx;
+        red[1][tid] = sy;
+        __syncthreads();
+        for (int w = kIbThreads / 2; w; w >>= 1) {
+            if (tid < w) {
+                red[0][tid] += red[0][tid + w];
+                red[1][tid] += red[1][tid + w];
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            ia.force_now[2 * b] = red[0][0];
+            ia.force_now[2 * b + 1] = red[1][0];
+            if (a.mode == MODE_STEP || a.mode == MODE_INIT) {
+                const long long h = (long long)(((t % ia.hist_cap) + ia.hist_cap) % ia.hist_cap);
+                ia.force_hist[(h * ia.nbody + b) * 2] = red[0][0];
+                ia.force_hist[(h * ia.nbody + b) * 2 + 1] = red[1][0];
+            }
+        }
+        __syncthreads();
+    }
+
+    // collision of the forced nodes with the corrected velocity and Guo term
+    for (int n = tid; n < nn; n += kIbThreads) {
+        const int s = ia.fn_slot[g.z + n];
+        const C* sf = reinterpret_cast<const C*>(a.side_f) + (long long)s * 9;
+        C f[9];
+#pragma unroll
+        for (int q = 0; q < 9; q++) f[q] = sf[q];
+        const C rho = C(rh[n]);
+        const C ux = C(ucx[n]), uy = C(ucy[n]);
+        const C rbs = rbase<S>(a);
+        const C tau = node_tau<C>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0), prm<C>(a.cs, a.f_cs));
+        const int2 xy = ia.fn_xy[g.z + n];
+        if (a.mode >= MODE_MAT) {
+            a.dl_tau[(long long)xy.y * a.nx + xy.x] = double(tau);
+        } else {
+            collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
+            add_guo<C>(f, ux, uy, C(fx[n]), C(fy[n]), prm<C>(a.tau0, a.f_tau0));
+#pragma unroll
+            for (int q = 0; q < 9; q++) stf<S>(a, q, xy.x, xy.y, f[q]);
+        }
+    }
+}
+
+// dynamic shared memory of ib_kernel for a group of nn nodes and nm markers
+__host__ __device__ constexpr size_t ib_smem_bytes(int nn, int nm)
+{
+    return (size_t)((nn + 1) & ~1) * 5 * sizeof(double) + (size_t)nm * 2 * sizeof(double2);
+}
+
+// ---------------------------------------------------------------------------
+// small utility kernels
+// ---------------------------------------------------------------------------
+static __global__ void style_kernel(uint8_t* out, int nx, int ny, int plate_x0, int scene)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)nx * ny) return;
+    const int x = (int)(i % nx), y = (int)(i / nx);
+    if (scene == SC_REF) {
+        out[i] = (uint8_t)ref_style(x, y, nx, ny, plate_x0);
+    } else {
+        out[i] = (uint8_t)(x == 0 ? 'i' : (x == nx - 1 ? 'o' : ((y == 0 || y == ny - 1) ? 'w' : 'f')));
+    }
+}
+
+template <typename C>
+__global__ void to_double_kernel(const C* in, double* out, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = double(in[i]);
+}
+
+// deterministic FP64 sum: per-block partial sums, then one block
+static __global__ void sum_partial_kernel(const double* in, long long n, double* part)
+{
+    __shared__ double red[256];
+    double s = 0.0;
+    for (long long i = (long long)blockIdx.x * 256 + threadIdx.x; i < n; i += (long long)gridDim.x * 256)
+        s += in[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+}  // namespace ippi

@@ -1,0 +1,123 @@
+"""Lattice: a Python handle on one ippi_lbm lattice (thin, over the C ABI)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+
+def _f64(a, n=None):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+def _p(a, ct=C.c_double):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ct))
+
+
+class Lattice:
+    """One D2Q9 lattice on the GPU.  Keyword arguments fill ippi_params
+    (defaults: the reference's main.cpp constants for the given size)."""
+
+    def __init__(self, nx, ny, **kw):
+        p = L.Params()
+        L.lib().ippi_params_default(C.byref(p), nx, ny)
+        for k, v in kw.items():
+            if not hasattr(p, k):
+                raise TypeError(f"unknown parameter {k}")
+            setattr(p, k, v)
+        self.params = p
+        self.nx, self.ny = nx, ny
+        h = C.c_void_p()
+        L.check(L.lib().ippi_create(C.byref(p), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().ippi_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def init_macros(self, rho=None, ux=None, uy=None):
+        n = self.nx * self.ny
+        rho, ux, uy = _f64(rho, n), _f64(ux, n), _f64(uy, n)
+        L.check(L.lib().ippi_init_macros(self._h, _p(rho), _p(ux), _p(uy)), self._h)
+
+    def set_markers(self, xy, ub=None, body=None, ds=None):
+        xy = _f64(xy).reshape(-1)
+        n = xy.size // 2
+        ub = _f64(ub, 2 * n)
+        ds = _f64(ds, n)
+        bd = None if body is None else np.ascontiguousarray(body, dtype=np.int32)
+        L.check(L.lib().ippi_set_markers(self._h, n, _p(xy), _p(ub),
+                                         None if bd is None else bd.ctypes.data_as(C.POINTER(C.c_int)),
+                                         _p(ds)), self._h)
+
+    def load_band_net(self, t, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        L.check(L.lib().ippi_load_band_net(self._h, t, _p(w, C.c_float), w.size), self._h)
+
+    def step(self, n=1, t0=1):
+        L.check(L.lib().ippi_step(self._h, n, t0), self._h)
+
+    def profile_steps(self, n, t0=1):
+        b, nb, ib = C.c_double(), C.c_double(), C.c_double()
+        L.check(L.lib().ippi_profile_steps(self._h, n, t0, C.byref(b), C.byref(nb), C.byref(ib)),
+                self._h)
+        return b.value, nb.value, ib.value
+
+    def download(self, field):
+        if field == L.FIELD_FLAGS:
+            out = np.zeros((self.ny, self.nx), np.uint8)
+        elif field == L.FIELD_F:
+            out = np.zeros((9, self.ny, self.nx), np.float64)
+        else:
+            out = np.zeros((self.ny, self.nx), np.float64)
+        L.check(L.lib().ippi_download(self._h, field, out.ctypes.data_as(C.c_void_p), out.nbytes),
+                self._h)
+        return out
+
+    def forces(self, with_mass=False):
+        nb = C.c_int(0)
+        L.check(L.lib().ippi_forces(self._h, None, C.byref(nb), None), self._h)
+        f = np.zeros(max(2 * nb.value, 2))
+        m = C.c_double(0)
+        L.check(L.lib().ippi_forces(self._h, _p(f), C.byref(nb), C.byref(m) if with_mass else None),
+                self._h)
+        f = f[: 2 * nb.value].reshape(-1, 2)
+        return (f, m.value) if with_mass else f
+
+    def force_history(self, max_steps):
+        nb = C.c_int(0)
+        L.check(L.lib().ippi_forces(self._h, None, C.byref(nb), None), self._h)
+        out = np.zeros((max_steps, max(nb.value, 1), 2))
+        n = L.lib().ippi_force_history(self._h, _p(out), max_steps)
+        if n < 0:
+            L.check(n, self._h)
+        return out[:n, : nb.value]
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        L.check(L.lib().ippi_get_stream(self._h, C.byref(s)), self._h)
+        return s.value or 0

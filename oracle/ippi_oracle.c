@@ -485,7 +485,7 @@ int orc_set_markers(orc* s, int n, const double* xy, const double* ub,
         if (!(mx >= 0 && mx < s->p.nx && my >= 0 && my < s->p.ny)) return -1;
         int c = orc_marker_stencil(s->p.delta_kernel, mx, my, xs, ys, ws);
         for (int q = 0; q < c; q++)
-            if (xs[q] < 1 || xs[q] > s->p.nx - 2 || ys[q] < 1 || ys[q] > s->p.ny - 2) return -1;
+            if (xs[q] < 3 || xs[q] > s->p.nx - 4 || ys[q] < 3 || ys[q] > s->p.ny - 4) return -1;
     }
     free(s->mk);
     free(s->body_force);
@@ -962,10 +962,25 @@ void orc_get(orc* s, int field, double* out)
         }
 }
 
+/* Body forces of an IB sub-step evaluated on the current velocity field
+ * (the forces the next collision will apply); the state is left untouched. */
 int orc_forces(orc* s, double* force_xy, double* mass)
 {
-    if (force_xy)
+    if (force_xy && s->nmark > 0) {
+        size_t n = (size_t)s->NX * s->NY;
+        double* sv[4] = {s->ux, s->uy, s->fxn, s->fyn};
+        double* cp[4];
+        for (int q = 0; q < 4; q++) {
+            cp[q] = (double*)malloc(n * sizeof(double));
+            memcpy(cp[q], sv[q], n * sizeof(double));
+        }
+        ib_substep(s);
         for (int b = 0; b < 2 * s->nbody; b++) force_xy[b] = s->body_force[b];
+        for (int q = 0; q < 4; q++) {
+            memcpy(sv[q], cp[q], n * sizeof(double));
+            free(cp[q]);
+        }
+    }
     if (mass) {
         update_mass(s);
         *mass = s->mass;

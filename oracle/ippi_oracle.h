@@ -67,7 +67,8 @@ void orc_destroy(orc* s);
 /* rho/ux/uy are [ny][nx] row-major (x fastest); NULL means rho=1, u=0. */
 void orc_init_macros(orc* s, const double* rho, const double* ux, const double* uy);
 /* Markers: xy[2n], ub[2n] (prescribed marker velocity), body[n] (or NULL), ds[n]
- * (or NULL for 1).  Returns 0 or -1 if a stencil leaves the interior. */
+ * (or NULL for 1).  Returns 0, or -1 if a stencil node lies closer than 3
+ * nodes to the lattice edge. */
 int orc_set_markers(orc* s, int n, const double* xy, const double* ub,
                     const int* body, const double* ds);
 /* TorchScript-layout weights of one boundary net (see band-net layout). */
@@ -78,8 +79,8 @@ int orc_step(orc* s, int nsteps, int t0);
 /* Fields on the global grid, x fastest: F is [9][ny][nx], the rest [ny][nx].
  * TAU / NNFLAG give the relaxation time the next collision will use. */
 void orc_get(orc* s, int field, double* out);
-/* Force on each body (lattice units, FP64) from the most recent step, and
- * the total mass sum(rho) over the grid. */
+/* Force on each body (lattice units, FP64) from an IB sub-step evaluated on
+ * the current velocity field (state untouched), and the mass sum(rho). */
 int orc_forces(orc* s, double* force_xy, double* mass);
 /* One IB sub-step on the current state (interpolate, force, spread, velocity
  * update) for unit parity with the reference IB primitives: writes marker
