@@ -172,6 +172,20 @@ int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk,
 /* Last error message of the handle (or of the library when h is NULL). */
 int ippi_last_error(ippi_lbm* h, char* buf, size_t n);
 
+/* No counterpart in the reference.  Deterministic FP64 sum of a density
+ * field rho[ny][nx] (device memory) into *mass (device memory), enqueued on
+ * `stream` (a cudaStream_t, NULL = default stream), without allocating any
+ * device memory: for callers that cannot call cudaMalloc where they need the
+ * mass checksum (inside stream capture, under another allocator's ownership
+ * of device memory, in loops that forbid allocation after start-up).  Its
+ * scratch is a fixed device array of IPPI_NOALLOC_MAX_ROWS row sums that the
+ * library keeps on every GPU it is loaded on; ny beyond that is rejected
+ * with IPPI_ERR_ARG.  The first call on a device looks up that array's
+ * device address, so make it before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU race. */
+#define IPPI_NOALLOC_MAX_ROWS 16384
+int ippi_mass_noalloc(const double* rho, int nx, int ny, double* mass, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
