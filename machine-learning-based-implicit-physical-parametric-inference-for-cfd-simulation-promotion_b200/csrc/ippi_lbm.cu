@@ -57,6 +57,7 @@ struct ippi_lbm {
     Ctr* ctr = nullptr;
     Ctr* ctr_h = nullptr;  // pinned mirror
     cudaStream_t side = nullptr;   // concurrent prep / net / IB kernels
+    int side_prio = 0;             // their launch priority (the device's highest)
     cudaEvent_t fork = nullptr, join = nullptr;
     uint8_t* nflag = nullptr;
     uint8_t* tile = nullptr;
@@ -64,7 +65,7 @@ struct ippi_lbm {
     PrepNode* prep_d = nullptr;    // nodes whose post-stream state the side kernels need
     int nprep = 0;
     int ib_nst = 4;
-    size_t ib_smem = 0;
+    bool ib_active = false;
     void* side_f = nullptr;
     void* side_m = nullptr;
     void* corner = nullptr;
@@ -87,7 +88,7 @@ struct ippi_lbm {
     int* band_type_d = nullptr;
     int band_blocks = 0;
     // immersed boundary
-    int nmark = 0, nbody = 0, nforced = 0, ngroups = 0, hist_cap = 0;
+    int nmark = 0, nbody = 0, nforced = 0, hist_cap = 0;
     std::vector<double> mk_xy, mk_ub, mk_ds;
     std::vector<int> mk_body;
     std::vector<DevBuf> ib_bufs;
@@ -305,18 +306,20 @@ int rebuild(ippi_lbm* h)
                 st_node[(size_t)m * 16 + q] = (int)id(xs[q], ys[q]);
                 st_wa[(size_t)m * 16 + q] = wa[q];
                 st_wb[(size_t)m * 16 + q] = wb[q];
-                flag[id(xs[q], ys[q])] |= NF_EXPORT | NF_DEFER;
+                flag[id(xs[q], ys[q])] |= NF_IB | NF_DEFER;
             }
         }
     }
 
-    // slots in row-major order; every flagged node is a prep node
+    // slots in row-major order; boundary-net nodes (inputs and band) are
+    // prep nodes, IB stencil nodes are computed by ib_nodes itself
     int ns = 0;
     std::vector<PrepNode> prep;
     for (size_t i = 0; i < nn; i++)
         if (flag[i]) {
             slot[i] = ns++;
-            prep.push_back(PrepNode{(int)(i % nx), (int)(i / nx), slot[i], flag[i]});
+            if (flag[i] & NF_EXPORT)
+                prep.push_back(PrepNode{(int)(i % nx), (int)(i / nx), slot[i], flag[i]});
         }
     h->nslots = ns;
 
@@ -403,98 +406,53 @@ int rebuild(ippi_lbm* h)
     // immersed-boundary tables
     for (auto& b : h->ib_bufs) dfree(b.p);
     h->ib_bufs.clear();
-    h->ngroups = 0;
     h->nforced = 0;
+    h->ib_active = false;
     if (nm > 0) {
-        // markers grouped by body, keeping their order within a body
-        std::vector<int> order(nm);
-        for (int m = 0; m < nm; m++) order[m] = m;
-        std::stable_sort(order.begin(), order.end(),
+        // markers sorted by body, keeping their order within a body
+        std::vector<int> morder(nm);
+        for (int m = 0; m < nm; m++) morder[m] = m;
+        std::stable_sort(morder.begin(), morder.end(),
                          [&](int a, int b) { return h->mk_body[a] < h->mk_body[b]; });
         const int nb = h->nbody;
-        // bodies sharing a stencil node must be finished by the same block
-        std::vector<int> parent(nb);
-        for (int b = 0; b < nb; b++) parent[b] = b;
-        std::function<int(int)> findp = [&](int b) { return parent[b] == b ? b : parent[b] = findp(parent[b]); };
-        std::map<int, int> node_body;
-        for (int m = 0; m < nm; m++)
-            for (int q = 0; q < nst; q++) {
-                int nd = st_node[(size_t)m * 16 + q];
-                auto it = node_body.find(nd);
-                if (it == node_body.end())
-                    node_body[nd] = h->mk_body[m];
-                else
-                    parent[findp(it->second)] = findp(h->mk_body[m]);
-            }
-        // groups of bodies; bodies numbered so that each group is contiguous
-        std::map<int, std::vector<int>> groups;
-        for (int b = 0; b < nb; b++) groups[findp(b)].push_back(b);
-        std::vector<int4> grp;
-        std::vector<int2> gbody, body_m(nb, make_int2(0, 0));
-        std::vector<int> morder;  // marker order on the device
-        std::vector<int> fnode;   // forced node ids
-        std::vector<int> fptr(1, 0), fe_marker;
-        std::vector<double2> fe_w;
-        std::vector<int> st_loc((size_t)nm * 16, 0);  // device order, group-local node index
-        std::vector<double2> st_w((size_t)nm * 16, make_double2(0, 0));
-        std::vector<int> new_index(nm);
-        std::map<int, int> forced_index;
-        for (auto& g : groups) {
-            int4 G;
-            G.x = (int)morder.size();
-            G.z = (int)fnode.size();
-            int b0 = g.second.front(), b1 = g.second.back() + 1;
-            gbody.push_back(make_int2(b0, b1));
-            for (int b : g.second) {
-                int m0 = (int)morder.size();
-                for (int m : order)
-                    if (h->mk_body[m] == b) {
-                        new_index[m] = (int)morder.size();
-                        morder.push_back(m);
-                    }
-                body_m[b] = make_int2(m0, (int)morder.size());
-            }
-            G.y = (int)morder.size();
-            // forced nodes of the group in first-use order, CSR in marker order
-            std::vector<std::vector<std::pair<int, double2>>> entries;
-            for (int mi = G.x; mi < G.y; mi++) {
-                int m = morder[mi];
-                for (int q = 0; q < nst; q++) {
-                    int nd = st_node[(size_t)m * 16 + q];
-                    auto it = forced_index.find(nd);
-                    int fi;
-                    if (it == forced_index.end()) {
-                        fi = (int)fnode.size();
-                        forced_index[nd] = fi;
-                        fnode.push_back(nd);
-                        entries.emplace_back();
-                    } else {
-                        fi = it->second;
-                    }
-                    double2 w = make_double2(st_wa[(size_t)m * 16 + q], st_wb[(size_t)m * 16 + q]);
-                    entries[fi - G.z].push_back({mi - G.x, w});
-                    st_loc[(size_t)mi * 16 + q] = fi - G.z;
-                    st_w[(size_t)mi * 16 + q] = w;
-                }
-            }
-            for (auto& e : entries) {
-                for (auto& pr : e) {
-                    fe_marker.push_back(pr.first);
-                    fe_w.push_back(pr.second);
-                }
-                fptr.push_back((int)fe_marker.size());
-            }
-            G.w = (int)fnode.size();
-            grp.push_back(G);
+        std::vector<int2> body_m(nb, make_int2(0, 0));
+        for (int mi = 0; mi < nm; mi++) {
+            const int b = h->mk_body[morder[mi]];
+            if (mi == 0 || h->mk_body[morder[mi - 1]] != b) body_m[b].x = mi;
+            body_m[b].y = mi + 1;
         }
-        // bodies must be numbered contiguously inside each group
-        for (size_t gi = 0; gi < grp.size(); gi++) {
-            int2 gb = gbody[gi];
-            int cnt = 0;
-            for (auto& g : groups)
-                if (g.second.front() == gb.x) cnt = (int)g.second.size();
-            if (gb.y - gb.x != cnt)
-                return fail(h, IPPI_ERR_ARG, "bodies sharing stencil nodes must have consecutive ids");
+        // forced nodes in first-use order; CSR entries in marker order, the
+        // accumulation order of SpreadForce (mesh.cpp:757-781)
+        std::vector<int> fnode, fptr(1, 0), fe_marker, st_loc((size_t)nm * 16, 0);
+        std::vector<double2> fe_w, st_w((size_t)nm * 16, make_double2(0, 0));
+        std::map<int, int> forced_index;
+        std::vector<std::vector<std::pair<int, double2>>> entries;
+        for (int mi = 0; mi < nm; mi++) {
+            const int m = morder[mi];
+            for (int q = 0; q < nst; q++) {
+                const int nd = st_node[(size_t)m * 16 + q];
+                auto it = forced_index.find(nd);
+                int fi;
+                if (it == forced_index.end()) {
+                    fi = (int)fnode.size();
+                    forced_index[nd] = fi;
+                    fnode.push_back(nd);
+                    entries.emplace_back();
+                } else {
+                    fi = it->second;
+                }
+                const double2 w = make_double2(st_wa[(size_t)m * 16 + q], st_wb[(size_t)m * 16 + q]);
+                entries[fi].push_back({mi, w});
+                st_loc[(size_t)mi * 16 + q] = fi;
+                st_w[(size_t)mi * 16 + q] = w;
+            }
+        }
+        for (auto& e : entries) {
+            for (auto& pr : e) {
+                fe_marker.push_back(pr.first);
+                fe_w.push_back(pr.second);
+            }
+            fptr.push_back((int)fe_marker.size());
         }
         const int nf = (int)fnode.size();
         std::vector<int> fn_slot(nf);
@@ -506,7 +464,7 @@ int rebuild(ippi_lbm* h)
         std::vector<double2> ub(nm);
         std::vector<double> ds(nm);
         for (int mi = 0; mi < nm; mi++) {
-            int m = morder[mi];
+            const int m = morder[mi];
             ub[mi] = make_double2(h->mk_ub[2 * m], h->mk_ub[2 * m + 1]);
             ds[mi] = h->mk_ds[m];
         }
@@ -522,48 +480,37 @@ int rebuild(ippi_lbm* h)
         IbArgs& I = h->ib;
         I = IbArgs{};
         I.nmark = nm;
+        I.nforced = nf;
+        I.nbody = nb;
         I.ub = (const double2*)up(ub.data(), nm * sizeof(double2));
         I.ds = (const double*)up(ds.data(), nm * sizeof(double));
         I.st_node = (const int*)up(st_loc.data(), st_loc.size() * sizeof(int));
         I.st_w = (const double2*)up(st_w.data(), st_w.size() * sizeof(double2));
+        I.body_m = (const int2*)up(body_m.data(), body_m.size() * sizeof(int2));
         I.fn_slot = (const int*)up(fn_slot.data(), nf * sizeof(int));
         I.fn_xy = (const int2*)up(fn_xy.data(), nf * sizeof(int2));
         I.fn_ptr = (const int*)up(fptr.data(), fptr.size() * sizeof(int));
         I.fe_marker = (const int*)up(fe_marker.data(), fe_marker.size() * sizeof(int));
         I.fe_w = (const double2*)up(fe_w.data(), fe_w.size() * sizeof(double2));
-        I.group = (const int4*)up(grp.data(), grp.size() * sizeof(int4));
-        I.gbody = (const int2*)up(gbody.data(), gbody.size() * sizeof(int2));
-        I.body_m = (const int2*)up(body_m.data(), body_m.size() * sizeof(int2));
+        I.rho = (double*)up(nullptr, nf * sizeof(double));
+        I.ucx = (double*)up(nullptr, nf * sizeof(double));
+        I.ucy = (double*)up(nullptr, nf * sizeof(double));
+        I.fx = (double*)up(nullptr, nf * sizeof(double));
+        I.fy = (double*)up(nullptr, nf * sizeof(double));
+        I.dmf = (double2*)up(nullptr, nm * sizeof(double2));
+        I.mft = (double2*)up(nullptr, nm * sizeof(double2));
         h->hist_cap = (int)std::max<long long>(16, std::min<long long>(1 << 16, (1ll << 24) / std::max(1, nb)));
         I.force_now = (double*)up(nullptr, (size_t)nb * 2 * sizeof(double));
         I.force_hist = (double*)up(nullptr, (size_t)h->hist_cap * nb * 2 * sizeof(double));
-        I.nbody = nb;
         I.hist_cap = h->hist_cap;
-        I.mdf_iters = std::max(1, h->p.mdf_iters);
         for (auto& b : h->ib_bufs)
             if (!b.p) return fail(h, IPPI_ERR_NOMEM, "IB table allocation failed");
         h->force_now = I.force_now;
         h->force_hist = I.force_hist;
         h->hist_written = 0;
-        h->ngroups = (int)grp.size();
         h->nforced = nf;
         h->ib_nst = nst;
-        size_t smem = 0;
-        for (auto& G : grp) smem = std::max(smem, ib_smem_bytes(G.w - G.z, G.y - G.x));
-        int dev_smem = 0;
-        cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->p.device);
-        if (smem + sizeof(double) * 2 * kIbThreads > (size_t)dev_smem)
-            return fail(h, IPPI_ERR_ARG, "a body group needs %zu bytes of shared memory (limit %d); "
-                        "split it into several bodies", smem, dev_smem);
-        cudaError_t e = cudaSuccess;
-        switch (h->S) {
-        case ST_F64: e = prepare_f64(smem); break;
-        case ST_F32: e = prepare_f32(smem); break;
-        case ST_F16: e = prepare_f16(smem); break;
-        default: e = prepare_bf16(smem); break;
-        }
-        CK(h, e);
-        h->ib_smem = smem;
+        h->ib_active = true;
     }
     h->dl_valid = false;
     return IPPI_OK;
@@ -615,12 +562,13 @@ LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int pa
     L.scene = h->p.bc_set == IPPI_BC_CHANNEL ? SC_CHANNEL : SC_REF;
     L.stream = h->st;
     L.side = h->side;
+    L.side_prio = h->side_prio;
     L.fork = h->fork;
     L.join = h->join;
     L.prep = h->prep_d;
     L.nprep = h->nprep;
     L.band = h->band_blocks > 0;
-    L.ib = h->ngroups > 0;
+    L.ib = h->ib_active;
     if (L.band) {
         BandArgs& B = L.band_args;
         B.nodes = h->band_nodes_d;
@@ -643,9 +591,8 @@ LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int pa
     if (L.ib) {
         L.ib_args = h->ib;
         L.ib_args.s = a;
-        L.ib_blocks = h->ngroups;
         L.ib_nst = h->ib_nst;
-        L.ib_smem = h->ib_smem;
+        L.ib_passes = std::max(1, h->p.mdf_iters);
     }
     return L;
 }
@@ -792,6 +739,7 @@ int ippi_create(const ippi_params* p, ippi_lbm** out)
         cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming) != cudaSuccess)
         return bail(fail(nullptr, IPPI_ERR_CUDA, "stream creation failed"));
+    h->side_prio = hi_prio;
     const size_t fbytes = (size_t)9 * h->plane * h->tsize;
     for (int b = 0; b < 2; b++)
         if (dalloc(&h->f[b], fbytes) != cudaSuccess || cudaMemset(h->f[b], 0, fbytes) != cudaSuccess)
@@ -1004,7 +952,8 @@ int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk, double*
     // bulk kernel: events 0-1 on the main stream; side chain (prep + nets /
     // IB), concurrent with it: events 2-3 on the side stream
     double tb = 0, tn = 0, ti = 0;
-    const bool band = h->band_blocks > 0, ib = h->ngroups > 0, side = h->nprep > 0;
+    const bool band = h->band_blocks > 0, ib = h->ib_active;
+    const bool side = h->nprep > 0 || band || ib;
     for (int s = 0; s < nsteps; s++) {
         float ms;
         cudaEventElapsedTime(&ms, ev[s * 4 + 0], ev[s * 4 + 1]);

@@ -3,5 +3,4 @@
 
 namespace ippi {
 cudaError_t launch_bf16(const LaunchSet& L) { return launch_store<ST_BF16>(L); }
-cudaError_t prepare_bf16(size_t ib_smem) { return prepare_store<ST_BF16>(ib_smem); }
 }  // namespace ippi

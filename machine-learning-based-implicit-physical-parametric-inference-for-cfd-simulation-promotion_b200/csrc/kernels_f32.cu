@@ -3,5 +3,4 @@
 
 namespace ippi {
 cudaError_t launch_f32(const LaunchSet& L) { return launch_store<ST_F32>(L); }
-cudaError_t prepare_f32(size_t ib_smem) { return prepare_store<ST_F32>(ib_smem); }
 }  // namespace ippi

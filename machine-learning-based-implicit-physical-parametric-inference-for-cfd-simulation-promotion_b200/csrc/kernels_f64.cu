@@ -3,5 +3,4 @@
 
 namespace ippi {
 cudaError_t launch_f64(const LaunchSet& L) { return launch_store<ST_F64>(L); }
-cudaError_t prepare_f64(size_t ib_smem) { return prepare_store<ST_F64>(ib_smem); }
 }  // namespace ippi

@@ -6,21 +6,53 @@
 
 namespace ippi {
 
+// Side-stream kernels carry an explicit launch priority, so the priority
+// survives stream capture into the step graphs and their blocks take the
+// first free slots while the bulk kernel fills the GPU.
+template <typename... KArgs, typename... Args>
+static void launch_prio(void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStream_t st,
+                        int prio, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = prio;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <int S, int CO, int SC>
 static cudaError_t launch_tpl(const LaunchSet& L)
 {
-    const bool side = L.nprep > 0;
+    const bool side = L.nprep > 0 || L.band || L.ib;
     if (side) {
         cudaEventRecord(L.fork, L.stream);
         cudaStreamWaitEvent(L.side, L.fork, 0);
         if (L.events) cudaEventRecord(L.events[2], L.side);
-        prep_kernel<S, SC><<<(L.nprep + 255) / 256, 256, 0, L.side>>>(L.step, L.prep, L.nprep);
-        if (L.band) band_kernel<S, CO><<<L.band_blocks, kBandThreads, 0, L.side>>>(L.band_args);
+        if (L.nprep > 0)
+            launch_prio(prep_kernel<S, SC>, (L.nprep + 255) / 256, 256, L.side, L.side_prio, L.step,
+                        L.prep, L.nprep);
+        if (L.band)
+            launch_prio(band_kernel<S, CO>, L.band_blocks, kBandThreads, L.side, L.side_prio,
+                        L.band_args);
         if (L.ib) {
-            if (L.ib_nst == 16)
-                ib_kernel<S, CO, 16><<<L.ib_blocks, kIbThreads, L.ib_smem, L.side>>>(L.ib_args);
-            else
-                ib_kernel<S, CO, 4><<<L.ib_blocks, kIbThreads, L.ib_smem, L.side>>>(L.ib_args);
+            const IbArgs& I = L.ib_args;
+            const unsigned gn = (I.nforced + kIbThreads - 1) / kIbThreads;
+            const unsigned gm = (I.nmark + kIbThreads - 1) / kIbThreads;
+            launch_prio(ib_nodes<S, SC>, gn, kIbThreads, L.side, L.side_prio, I);
+            for (int it = 0; it < L.ib_passes; it++) {
+                if (L.ib_nst == 16)
+                    launch_prio(ib_markers<16>, gm, kIbThreads, L.side, L.side_prio, I, int(it == 0));
+                else
+                    launch_prio(ib_markers<4>, gm, kIbThreads, L.side, L.side_prio, I, int(it == 0));
+                launch_prio(ib_spread, gn, kIbThreads, L.side, L.side_prio, I);
+            }
+            launch_prio(ib_finish<S, CO>, (unsigned)I.nbody + gn, kIbThreads, L.side, L.side_prio, I);
         }
         if (L.events) cudaEventRecord(L.events[3], L.side);
         cudaEventRecord(L.join, L.side);
@@ -47,20 +79,6 @@ static cudaError_t launch_store(const LaunchSet& L)
     case CO_RR: return launch_tpl<S, CO_RR, SC_CHANNEL>(L);
     default: return launch_tpl<S, CO_BGK, SC_CHANNEL>(L);
     }
-}
-
-template <int S>
-static cudaError_t prepare_store(size_t smem)
-{
-    const int v = (int)smem;
-    cudaError_t e = cudaSuccess;
-#define IPPI_SMEM(CO, N)                                                                     \
-    if (e == cudaSuccess)                                                                    \
-        e = cudaFuncSetAttribute(ib_kernel<S, CO, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-    IPPI_SMEM(CO_BGK, 4) IPPI_SMEM(CO_BGK, 16) IPPI_SMEM(CO_MRT, 4) IPPI_SMEM(CO_MRT, 16)
-    IPPI_SMEM(CO_RR, 4) IPPI_SMEM(CO_RR, 16)
-#undef IPPI_SMEM
-    return e;
 }
 
 }  // namespace ippi

@@ -11,7 +11,8 @@ struct LaunchSet {
     StepArgs step;
     dim3 grid;
     int coll, scene;
-    // side-stream work: prep -> (band) -> (ib), forked from and joined to `stream`
+    // side-stream work: (prep -> band) and/or the IB chain, forked from and
+    // joined to `stream`
     const PrepNode* prep;
     int nprep;
     bool band;
@@ -19,10 +20,10 @@ struct LaunchSet {
     int band_blocks;
     bool ib;
     IbArgs ib_args;
-    int ib_blocks;
     int ib_nst;          // 4 or 16 stencil nodes per marker
-    size_t ib_smem;      // dynamic shared memory of ib_kernel
+    int ib_passes;       // direct-forcing passes
     cudaStream_t stream, side;
+    int side_prio;       // launch priority of the side-stream kernels
     cudaEvent_t fork, join;
     // optional device timing: events[0..3] around the bulk kernel and the
     // side-stream chain (only when not capturing)
@@ -33,10 +34,5 @@ cudaError_t launch_f64(const LaunchSet& L);
 cudaError_t launch_f32(const LaunchSet& L);
 cudaError_t launch_f16(const LaunchSet& L);
 cudaError_t launch_bf16(const LaunchSet& L);
-// raise the dynamic shared-memory limit of the IB kernels (once per device)
-cudaError_t prepare_f64(size_t ib_smem);
-cudaError_t prepare_f32(size_t ib_smem);
-cudaError_t prepare_f16(size_t ib_smem);
-cudaError_t prepare_bf16(size_t ib_smem);
 
 }  // namespace ippi

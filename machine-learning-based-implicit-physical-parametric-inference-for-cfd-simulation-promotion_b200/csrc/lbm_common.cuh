@@ -19,8 +19,10 @@ enum { ST_F64 = 0, ST_F32 = 1, ST_F16 = 2, ST_BF16 = 3 };
 enum { CO_BGK = 0, CO_MRT = 1, CO_RR = 2 };
 enum { SC_REF = 0, SC_CHANNEL = 1 };
 
-// per-node side flags (only read in tiles marked special)
-enum : uint8_t { NF_EXPORT = 1, NF_DEFER = 2 };
+// per-node side flags: NF_DEFER is the only one on the device (the bulk
+// kernel skips those nodes); NF_EXPORT marks boundary-net inputs and NF_IB
+// immersed-boundary stencil nodes (host-side tables only)
+enum : uint8_t { NF_EXPORT = 1, NF_DEFER = 2, NF_IB = 4 };
 
 // step kernel modes
 enum { MODE_STEP = 0, MODE_INIT = 1, MODE_MAT = 2, MODE_MAT_INIT = 3 };

@@ -7,13 +7,13 @@
 //                 tau + collision, store the 9 new post-collision
 //                 populations.  HBM traffic per node: 9 loads + 9 stores.
 // and, on a side stream running concurrently with it,
-//   prep_kernel   the post-stream state of the few nodes other kernels need
-//                 (boundary-net inputs, IB stencil nodes) into side buffers
+//   prep_kernel   the post-stream state of the boundary nets' input nodes
+//                 into side buffers
 //   band_kernel   (flat plate with boundary nets) the nets' MLP on the band
 //                 nodes, then their collision
-//   ib_kernel     (immersed boundary) interpolation, direct forcing,
-//                 spreading, velocity correction, forced collision with the
-//                 Guo term, per-body force sums
+//   ib_*          (immersed boundary) stencil-node states, interpolation and
+//                 direct forcing, spreading and velocity correction, forced
+//                 collision with the Guo term, per-body force sums
 // A node is "deferred" when its collision needs moments of other nodes of
 // the same step (net inputs, marker forces); step_kernel skips it and the
 // side-stream kernels own it.  All kernels of a step read only the previous
@@ -401,7 +401,7 @@ __device__ __forceinline__ void node_epilogue(const StepArgs& a, long long node,
 // the fused stream + boundary + collide kernel (every node not deferred)
 // ---------------------------------------------------------------------------
 template <int S, int CO, int SC>
-__global__ void __launch_bounds__(kBlockX) step_kernel(const StepArgs a)
+__global__ void __launch_bounds__(kBlockX, 8) step_kernel(const StepArgs a)
 {
     using C = typename Store<S>::C;
     const int x = blockIdx.x * kBlockX + threadIdx.x;
@@ -444,7 +444,7 @@ struct PrepNode {
 };
 
 template <int S, int SC>
-__global__ void __launch_bounds__(256) prep_kernel(const StepArgs a, const PrepNode* nodes, int n)
+__global__ void __launch_bounds__(256, 8) prep_kernel(const StepArgs a, const PrepNode* nodes, int n)
 {
     using C = typename Store<S>::C;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -606,117 +606,128 @@ __global__ void __launch_bounds__(kBandThreads) band_kernel(const BandArgs ba)
 
 // ---------------------------------------------------------------------------
 // immersed boundary (mesh.cpp:514-832, 1244-1281 and NodeAndLattice.cpp:162-195)
-// One block per group of bodies that share no stencil node with another
-// group; per-node and per-marker work arrays live in shared memory.
+// as a chain of short, fully parallel kernels on the side stream:
+//   ib_nodes    post-stream state of every stencil node, from the previous
+//               field (the bulk kernel skips these nodes)
+//   ib_markers  InterpolateVel + CalParticleForce: F_m = 2 (U_b - sum u delta)
+//   ib_spread   SpreadForce + UpdateVelocity: node force, u += F / (2 rho)
+//               (markers and spread repeat for each direct-forcing pass)
+//   ib_finish   per-body force sums (FP64 tree, one block per body) and the
+//               forced nodes' collision with the corrected velocity + Guo term
+// Blocks are small (kIbThreads threads, at most 32 registers), so they fit
+// the first slots that retiring bulk blocks free.
 // ---------------------------------------------------------------------------
-constexpr int kIbThreads = 512;
+constexpr int kIbThreads = 128;
 
 struct IbArgs {
-    // markers (sorted by group, then body)
-    int nmark;
+    int nmark, nforced, nbody;
+    // markers, sorted by body
     const double2* ub;          // prescribed velocity
     const double* ds;           // arc length (force weight)
-    const int* st_node;         // [nmark][16] stencil node: index within the group's nodes
+    const int* st_node;         // [nmark][16] stencil -> forced-node index
     const double2* st_w;        // [nmark][16] (wa, wb): contribution (v * wa) * wb
-    // forced nodes (one per stencil node), CSR node -> (marker, wa, wb)
+    const int2* body_m;         // per body: (first marker, end marker)
+    // forced nodes, CSR node -> (marker, wa, wb) in marker order
     const int* fn_slot;         // side-buffer slot
     const int2* fn_xy;
     const int* fn_ptr;          // [nforced + 1]
-    const int* fe_marker;       // marker index within the group
+    const int* fe_marker;
     const double2* fe_w;
-    const int4* group;          // (first marker, end marker, first node, end node)
-    const int2* gbody;          // per group: (first body, end body)
-    const int2* body_m;         // per body: (first marker, end marker)
+    // work arrays
+    double* rho;                // per forced node
+    double* ucx;
+    double* ucy;
+    double* fx;
+    double* fy;
+    double2* dmf;               // per marker: force of the current pass
+    double2* mft;               // per marker: total force
+    // outputs
     double* force_now;          // [nbody][2]
     double* force_hist;         // [hist_cap][nbody][2]
-    int nbody, hist_cap;
-    int mdf_iters;
+    int hist_cap;
     StepArgs s;
 };
 
-template <int S, int CO, int NST>
-__global__ void __launch_bounds__(kIbThreads) ib_kernel(const IbArgs ia)
+template <int S, int SC>
+__global__ void __launch_bounds__(kIbThreads, 8) ib_nodes(const IbArgs ia)
 {
     using C = typename Store<S>::C;
     const StepArgs& a = ia.s;
-    const int4 g = ia.group[blockIdx.x];
+    const int n = blockIdx.x * kIbThreads + threadIdx.x;
+    if (n >= ia.nforced) return;
     const int t = step_time(a);
-    const int nm = g.y - g.x, nn = g.w - g.z;
-    const C* sm = reinterpret_cast<const C*>(a.side_m) + (long long)a.par * a.nslots * 3;
-    const int tid = threadIdx.x;
-    extern __shared__ __align__(16) double ib_smem[];
-    // node arrays padded to an even length so the double2 marker arrays
-    // after them start on a 16-byte boundary (layout of ib_smem_bytes)
-    const int nnp = (nn + 1) & ~1;
-    double* ucx = ib_smem;
-    double* ucy = ucx + nnp;
-    double* fx = ucy + nnp;
-    double* fy = fx + nnp;
-    double* rh = fy + nnp;
-    double2* dmf = reinterpret_cast<double2*>(rh + nnp);
-    double2* mft = dmf + nm;
-    __shared__ double red[2][kIbThreads];
-
-    for (int n = tid; n < nn; n += kIbThreads) {
-        const C* m = sm + (long long)ia.fn_slot[g.z + n] * 3;
-        rh[n] = double(m[0]);
-        ucx[n] = double(m[1]);
-        ucy[n] = double(m[2]);
-        fx[n] = 0.0;
-        fy[n] = 0.0;
-    }
-    for (int m = tid; m < nm; m += kIbThreads) mft[m] = make_double2(0.0, 0.0);
-    __syncthreads();
-
-    for (int it = 0; it < ia.mdf_iters; it++) {
-        // InterpolateVel + CalParticleForce: F = 2 (U_b - sum u delta)
-        for (int m = tid; m < nm; m += kIbThreads) {
-            const int gm = g.x + m;
-            int sn[NST];
-            double2 sw[NST];
+    const int2 xy = ia.fn_xy[n];
+    C f[9], rho, ux, uy;
+    node_state<S, SC>(a, xy.x, xy.y, f, rho, ux, uy);
+    C* sf = reinterpret_cast<C*>(a.side_f) + (long long)ia.fn_slot[n] * 9;
 #pragma unroll
-            for (int q = 0; q < NST; q++) {
-                sn[q] = ia.st_node[gm * 16 + q];
-                sw[q] = ia.st_w[gm * 16 + q];
-            }
-            double vx = 0.0, vy = 0.0;
-#pragma unroll
-            for (int q = 0; q < NST; q++) {
-                vx += ucx[sn[q]] * sw[q].x * sw[q].y;
-                vy += ucy[sn[q]] * sw[q].x * sw[q].y;
-            }
-            const double2 u = ia.ub[gm];
-            const double2 d = make_double2(2.0 * (u.x - vx), 2.0 * (u.y - vy));
-            dmf[m] = d;
-            mft[m] = make_double2(mft[m].x + d.x, mft[m].y + d.y);
-        }
-        __syncthreads();
-        // SpreadForce + UpdateVelocity: u += F / (2 rho), markers in order
-        for (int n = tid; n < nn; n += kIbThreads) {
-            double dfx = 0.0, dfy = 0.0;
-            const int e1 = ia.fn_ptr[g.z + n + 1];
-            for (int e = ia.fn_ptr[g.z + n]; e < e1; e++) {
-                const double2 d = dmf[ia.fe_marker[e]];
-                const double2 wq = ia.fe_w[e];
-                dfx += d.x * wq.x * wq.y;
-                dfy += d.y * wq.x * wq.y;
-            }
-            ucx[n] = ucx[n] + 0.5 * 1 * dfx / rh[n];
-            ucy[n] = ucy[n] + 0.5 * 1 * dfy / rh[n];
-            fx[n] += dfx;
-            fy[n] += dfy;
-        }
-        __syncthreads();
-    }
+    for (int q = 0; q < 9; q++) sf[q] = f[q];
+    node_epilogue<S>(a, (long long)xy.y * a.nx + xy.x, t, f, rho, ux, uy);
+    ia.rho[n] = double(rho);
+    ia.ucx[n] = double(ux);
+    ia.ucy[n] = double(uy);
+    ia.fx[n] = 0.0;
+    ia.fy[n] = 0.0;
+}
 
-    // body forces: -sum F ds per body (tree reduction in FP64)
-    const int2 gb = ia.gbody[blockIdx.x];
-    for (int b = gb.x; b < gb.y; b++) {
+template <int NST>
+__global__ void __launch_bounds__(kIbThreads, 8) ib_markers(const IbArgs ia, int first_pass)
+{
+    const int m = blockIdx.x * kIbThreads + threadIdx.x;
+    if (m >= ia.nmark) return;
+    int sn[NST];
+    double2 sw[NST];
+#pragma unroll
+    for (int q = 0; q < NST; q++) {
+        sn[q] = ia.st_node[m * 16 + q];
+        sw[q] = ia.st_w[m * 16 + q];
+    }
+    double vx = 0.0, vy = 0.0;
+#pragma unroll
+    for (int q = 0; q < NST; q++) {
+        vx += ia.ucx[sn[q]] * sw[q].x * sw[q].y;
+        vy += ia.ucy[sn[q]] * sw[q].x * sw[q].y;
+    }
+    const double2 u = ia.ub[m];
+    const double2 d = make_double2(2.0 * (u.x - vx), 2.0 * (u.y - vy));
+    ia.dmf[m] = d;
+    const double2 tot = first_pass ? make_double2(0.0, 0.0) : ia.mft[m];
+    ia.mft[m] = make_double2(tot.x + d.x, tot.y + d.y);
+}
+
+static __global__ void __launch_bounds__(kIbThreads, 8) ib_spread(const IbArgs ia)
+{
+    const int n = blockIdx.x * kIbThreads + threadIdx.x;
+    if (n >= ia.nforced) return;
+    double dfx = 0.0, dfy = 0.0;
+    const int e1 = ia.fn_ptr[n + 1];
+    for (int e = ia.fn_ptr[n]; e < e1; e++) {
+        const double2 d = ia.dmf[ia.fe_marker[e]];
+        const double2 wq = ia.fe_w[e];
+        dfx += d.x * wq.x * wq.y;
+        dfy += d.y * wq.x * wq.y;
+    }
+    const double r = ia.rho[n];
+    ia.ucx[n] = ia.ucx[n] + 0.5 * 1 * dfx / r;
+    ia.ucy[n] = ia.ucy[n] + 0.5 * 1 * dfy / r;
+    ia.fx[n] += dfx;
+    ia.fy[n] += dfy;
+}
+
+template <int S, int CO>
+__global__ void __launch_bounds__(kIbThreads, 8) ib_finish(const IbArgs ia)
+{
+    using C = typename Store<S>::C;
+    const StepArgs& a = ia.s;
+    if ((int)blockIdx.x < ia.nbody) {
+        // body force: -sum F ds over the body's markers (fixed-order tree)
+        __shared__ double red[2][kIbThreads];
+        const int b = blockIdx.x, tid = threadIdx.x;
         const int2 mr = ia.body_m[b];
         double sx = 0.0, sy = 0.0;
         for (int m = mr.x + tid; m < mr.y; m += kIbThreads) {
-            sx -= mft[m - g.x].x * ia.ds[m];
-            sy -= mft[m - g.x].y * ia.ds[m];
+            sx -= ia.mft[m].x * ia.ds[m];
+            sy -= ia.mft[m].y * ia.ds[m];
         }
         red[0][tid] = sx;
         red[1][tid] = sy;
@@ -732,41 +743,34 @@ __global__ void __launch_bounds__(kIbThreads) ib_kernel(const IbArgs ia)
             ia.force_now[2 * b] = red[0][0];
             ia.force_now[2 * b + 1] = red[1][0];
             if (a.mode == MODE_STEP || a.mode == MODE_INIT) {
+                const int t = step_time(a);
                 const long long h = (long long)(((t % ia.hist_cap) + ia.hist_cap) % ia.hist_cap);
                 ia.force_hist[(h * ia.nbody + b) * 2] = red[0][0];
                 ia.force_hist[(h * ia.nbody + b) * 2 + 1] = red[1][0];
             }
         }
-        __syncthreads();
+        return;
     }
-
     // collision of the forced nodes with the corrected velocity and Guo term
-    for (int n = tid; n < nn; n += kIbThreads) {
-        const int s = ia.fn_slot[g.z + n];
-        const C* sf = reinterpret_cast<const C*>(a.side_f) + (long long)s * 9;
-        C f[9];
+    const int n = (blockIdx.x - ia.nbody) * kIbThreads + threadIdx.x;
+    if (n >= ia.nforced) return;
+    const C* sf = reinterpret_cast<const C*>(a.side_f) + (long long)ia.fn_slot[n] * 9;
+    C f[9];
 #pragma unroll
-        for (int q = 0; q < 9; q++) f[q] = sf[q];
-        const C rho = C(rh[n]);
-        const C ux = C(ucx[n]), uy = C(ucy[n]);
-        const C rbs = rbase<S>(a);
-        const C tau = node_tau<C>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0), prm<C>(a.cs, a.f_cs));
-        const int2 xy = ia.fn_xy[g.z + n];
-        if (a.mode >= MODE_MAT) {
-            a.dl_tau[(long long)xy.y * a.nx + xy.x] = double(tau);
-        } else {
-            collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
-            add_guo<C>(f, ux, uy, C(fx[n]), C(fy[n]), prm<C>(a.tau0, a.f_tau0));
+    for (int q = 0; q < 9; q++) f[q] = sf[q];
+    const C rho = C(ia.rho[n]);
+    const C ux = C(ia.ucx[n]), uy = C(ia.ucy[n]);
+    const C rbs = rbase<S>(a);
+    const C tau = node_tau<C>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0), prm<C>(a.cs, a.f_cs));
+    const int2 xy = ia.fn_xy[n];
+    if (a.mode >= MODE_MAT) {
+        a.dl_tau[(long long)xy.y * a.nx + xy.x] = double(tau);
+    } else {
+        collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
+        add_guo<C>(f, ux, uy, C(ia.fx[n]), C(ia.fy[n]), prm<C>(a.tau0, a.f_tau0));
 #pragma unroll
-            for (int q = 0; q < 9; q++) stf<S>(a, q, xy.x, xy.y, f[q]);
-        }
+        for (int q = 0; q < 9; q++) stf<S>(a, q, xy.x, xy.y, f[q]);
     }
-}
-
-// dynamic shared memory of ib_kernel for a group of nn nodes and nm markers
-__host__ __device__ constexpr size_t ib_smem_bytes(int nn, int nm)
-{
-    return (size_t)((nn + 1) & ~1) * 5 * sizeof(double) + (size_t)nm * 2 * sizeof(double2);
 }
 
 // ---------------------------------------------------------------------------
