@@ -12,8 +12,8 @@ CUDA events on the library's stream, max over ranks.  The populations
 
 Keys beyond the base contract:
   e2e           the same metric through the C ABI with host buffers: initial
-                fields uploaded from pinned host memory, per-step ippi_step +
-                ippi_forces (force read back), final velocity downloaded
+                fields uploaded from pinned host memory, the K steps, the
+                per-step body forces read back, rho / ux / uy downloaded
   roofline      bulk stream-collide kernel: 72 algorithmic bytes per node
                 (9 loads + 9 stores of FP32) / its CUDA-event launch time
   cpu_baseline  the reference's own MRT+Smagorinsky step (compiled from its
@@ -38,6 +38,11 @@ sys.path.insert(0, PKG)
 
 NX, NY = 4096, 1024
 BYTES_PER_NODE = 72  # FP32: 9 loads + 9 stores
+# DRAM bytes (read + write) of one step_kernel launch on this workload, from
+# the ncu capture summarised under profiles/ (dram__bytes_read.sum 151.22 MB +
+# dram__bytes_write.sum 104.20 MB; part of the writes is still in L2 when the
+# kernel ends)
+NCU_TRAFFIC_BYTES = 255.42e6
 METRIC = "MLUPS"
 WORKLOAD = "channel_cylinder_4096x1024_mrt_smagorinsky_ib_fp32"
 
@@ -107,7 +112,29 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU reference (reference arm and cpu_baseline)
 # ---------------------------------------------------------------------------
+class quiet_stdout:
+    """Send file descriptor 1 to /dev/null (the reference's own progress
+    prints) so that stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
+        os.close(devnull)
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
 def cpu_reference(steps, warmup, max_seconds=None):
+    with quiet_stdout():
+        return _cpu_reference(steps, warmup, max_seconds)
+
+
+def _cpu_reference(steps, warmup, max_seconds=None):
     """Time the reference's MRT + Smagorinsky step (its own sources compiled by
     oracle/build_ref.sh, SINGLE precision, flat-plate scene, one MPI rank per
     host core as threads) on the NX x NY grid.  Falls back to the FP64 oracle
@@ -187,6 +214,10 @@ def run_ours(a):
 
     sc = ip.scenes.config2()
     lat = ip.Lattice(NX, NY, device=local, **sc["params"])
+    kernel_name = "step_kernel<F32,MRT,CHANNEL>"
+    # bulk kernel + IB chain (stencil nodes, markers + spread per direct-forcing
+    # pass, forced collision + force sums) on the side stream
+    launches_per_step = 1 + 2 + 2 * sc["params"].get("mdf_iters", 1)
     lat.init_macros(*sc["init"])
     lat.set_markers(sc["markers"], ds=sc["ds"])
     stream = torch.cuda.ExternalStream(lat.stream(), device=torch.device("cuda", local))
@@ -224,31 +255,35 @@ def run_ours(a):
     achieved = NX * NY * BYTES_PER_NODE / (ms_bulk * 1e-3) / 1e9
 
     # ---- end to end through the C ABI with host buffers --------------------
+    # The reference's driver (main.cpp:105-120) runs OneLBMStep every step
+    # and dumps the fluid fields every SaveStep steps.  Here: the initial
+    # fields uploaded from pinned host memory, the K steps in one ippi_step
+    # call, the per-step body forces read back (ippi_force_history) and the
+    # rho / ux / uy fields downloaded once (one field dump).
     n_e2e = a.steps
     rho0, ux0, uy0 = (np.ascontiguousarray(x) for x in sc["init"])
     pin = [torch.from_numpy(x).pin_memory().numpy() for x in (rho0, ux0, uy0)]
-    fxy = np.zeros(2)
-    nb = C.c_int(0)
     L = ip.lib()
-    out_u = torch.empty((NY, NX), dtype=torch.float64).pin_memory().numpy()
+    dump = [torch.empty((NY, NX), dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
+    hist = torch.zeros((n_e2e, 1, 2), dtype=torch.float64).pin_memory().numpy()
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
     lat.init_macros(*pin)
-    for s in range(n_e2e):
-        rc = L.ippi_step(lat.handle, 1, s + 1)
-        if rc:
-            ip._lib.check(rc, lat.handle)
-        L.ippi_forces(lat.handle, fxy.ctypes.data_as(C.POINTER(C.c_double)), C.byref(nb), None)
-    L.ippi_download(lat.handle, ip.FIELD_UX, out_u.ctypes.data_as(C.c_void_p), out_u.nbytes)
+    ip._lib.check(L.ippi_step(lat.handle, n_e2e, 1), lat.handle)
+    got = L.ippi_force_history(lat.handle, hist.ctypes.data_as(C.POINTER(C.c_double)), n_e2e)
+    for fld, buf in zip((ip.FIELD_RHO, ip.FIELD_UX, ip.FIELD_UY), dump):
+        ip._lib.check(L.ippi_download(lat.handle, fld, buf.ctypes.data_as(C.c_void_p), buf.nbytes),
+                      lat.handle)
     e2e_s = time.perf_counter() - t0
+    assert got == n_e2e, got
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e = NX * NY * n_e2e * world / e2e_s / 1e6
     h2d = (rho0.nbytes + ux0.nbytes + uy0.nbytes) / n_e2e
-    d2h = (16 * n_e2e + 4 * n_e2e + out_u.nbytes) / n_e2e
+    d2h = (hist.nbytes + sum(b.nbytes for b in dump)) / n_e2e
 
     if rank == 0:
         cpu = None
@@ -268,13 +303,14 @@ def run_ours(a):
                        "parallelism": f"replicas{world}"},
             "hbm_gbs": round(value * BYTES_PER_NODE / 1e3 / world, 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
-                         "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
-                         "peak_source": peak_kind, "kernel": "step_kernel<F32,MRT,CHANNEL>",
+                         "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": NCU_TRAFFIC_BYTES,
+                         "traffic_algorithmic": NX * NY * BYTES_PER_NODE,
+                         "peak_source": peak_kind, "kernel": kernel_name,
                          "kernel_ms": round(ms_bulk, 5), "band_ms": round(ms_band, 5),
                          "ib_ms": round(ms_ib, 5), "bytes_per_node": BYTES_PER_NODE},
             "e2e": {"value": round(e2e, 1), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d),
                     "d2h_bytes_per_step": round(d2h), "steps": n_e2e},
-            "gpu_launches": a.steps * 2,
+            "gpu_launches": a.steps * launches_per_step,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }

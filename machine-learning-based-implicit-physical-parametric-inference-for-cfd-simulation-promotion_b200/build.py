@@ -8,6 +8,10 @@ into csrc/_build/*.o (in parallel), then linked with the CUDA runtime
 (static) into ./libippi_lbm.so next to this file.  Incremental: a unit is
 rebuilt when it or any header under csrc/ or include/ is newer than its
 object.  nvcc cross-compiles, so this runs without a GPU.
+
+Then the C++ host layer (host/: the reference's Mesh / Lattice classes and
+its main.cpp driver over the C ABI) is compiled with the host compiler into
+./ippi_main, linked against ./libippi_lbm.so.
 """
 from __future__ import annotations
 
@@ -24,6 +28,8 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(CSRC, "_build")
 LIB = os.path.join(HERE, "libippi_lbm.so")
+HOST = os.path.join(HERE, "host")
+MAIN = os.path.join(HERE, "ippi_main")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "-I", os.path.join(REPO, "include")]
@@ -70,7 +76,29 @@ def build(force: bool = False, jobs: int | None = None) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
+    build_host(force)
     return LIB
+
+
+def cxx() -> str:
+    for cand in (os.environ.get("IPPI_CXX"), "/usr/bin/g++", shutil.which("g++")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("g++ not found")
+
+
+def build_host(force: bool = False) -> str:
+    """ippi_main: host/*.cpp (Mesh, Lattice, the driver) against libippi_lbm.so."""
+    srcs = sorted(glob.glob(os.path.join(HOST, "*.cpp")))
+    deps = srcs + glob.glob(os.path.join(HOST, "*.h")) + [LIB, os.path.join(REPO, "include", "ippi_lbm.h")]
+    if not force and os.path.exists(MAIN) and os.path.getmtime(MAIN) >= max(map(os.path.getmtime, deps)):
+        return MAIN
+    cmd = [cxx(), "-std=c++17", "-O2", "-Wall", "-I", os.path.join(REPO, "include"), "-I", HOST, *srcs,
+           "-o", MAIN, "-L", HERE, "-lippi_lbm", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host build failed:\n{r.stderr}")
+    return MAIN
 
 
 if __name__ == "__main__":

@@ -96,10 +96,27 @@ struct ippi_lbm {
     double* force_now = nullptr;
     double* force_hist = nullptr;
     long long hist_written = 0;
-    // graphs of two steps: [start buffer][step parity]
+    // graphs of two steps and of one step: [start buffer][step parity]
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    cudaGraphExec_t graph1[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     char err[512] = "";
 };
+
+// Initial moment table [3][nn]: fills the fields the caller did not give
+// (rho = 1, u = 0) and records the first node with rho <= 0 (or NaN) or a
+// non-finite velocity in *bad (all ones when there is none).
+__global__ void init_fields_kernel(double* m, long long nn, int has_rho, int has_ux, int has_uy,
+                                   unsigned long long* bad)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nn;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (!has_rho) m[i] = 1.0;
+        if (!has_ux) m[nn + i] = 0.0;
+        if (!has_uy) m[2 * nn + i] = 0.0;
+        if (!(m[i] > 0) || !isfinite(m[nn + i]) || !isfinite(m[2 * nn + i]))
+            atomicMin(bad, (unsigned long long)i);
+    }
+}
 
 namespace {
 
@@ -138,10 +155,11 @@ void drop_graphs(ippi_lbm* h)
 {
     for (int b = 0; b < 2; b++)
         for (int q = 0; q < 2; q++)
-            if (h->graph[b][q]) {
-                cudaGraphExecDestroy(h->graph[b][q]);
-                h->graph[b][q] = nullptr;
-            }
+            for (cudaGraphExec_t* g : {&h->graph[b][q], &h->graph1[b][q]})
+                if (*g) {
+                    cudaGraphExecDestroy(*g);
+                    *g = nullptr;
+                }
 }
 
 cudaError_t launch(const LaunchSet& L, int S)
@@ -622,20 +640,23 @@ int run_init(ippi_lbm* h)
     return IPPI_OK;
 }
 
-// two steps starting from buffer b with parity q, as one CUDA graph
-int build_graph(ippi_lbm* h, int b, int q)
+// n (1 or 2) steps starting from buffer b with parity q, as one CUDA graph
+int build_graph(ippi_lbm* h, int n, int b, int q)
 {
     cudaGraph_t g;
+    cudaGraphExec_t& slot = n == 2 ? h->graph[b][q] : h->graph1[b][q];
     CK(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
     LaunchSet L0 = make_launch(h, MODE_STEP, h->f[b], h->f[b ^ 1], q);
-    LaunchSet L1 = make_launch(h, MODE_STEP, h->f[b ^ 1], h->f[b], q ^ 1);
-    cudaError_t e0 = launch(L0, h->S);
-    cudaError_t e1 = launch(L1, h->S);
+    cudaError_t e0 = launch(L0, h->S), e1 = cudaSuccess;
+    if (n == 2) {
+        LaunchSet L1 = make_launch(h, MODE_STEP, h->f[b ^ 1], h->f[b], q ^ 1);
+        e1 = launch(L1, h->S);
+    }
     cudaError_t ec = cudaStreamEndCapture(h->st, &g);
     if (e0 != cudaSuccess || e1 != cudaSuccess || ec != cudaSuccess)
         return fail(h, IPPI_ERR_CUDA, "graph capture failed: %s",
                     cudaGetErrorString(e0 ? e0 : (e1 ? e1 : ec)));
-    cudaError_t ei = cudaGraphInstantiate(&h->graph[b][q], g, 0);
+    cudaError_t ei = cudaGraphInstantiate(&slot, g, 0);
     cudaGraphDestroy(g);
     CK(h, ei);
     return IPPI_OK;
@@ -797,22 +818,32 @@ int ippi_destroy(ippi_lbm* h)
 int ippi_init_macros(ippi_lbm* h, const double* rho, const double* ux, const double* uy)
 {
     if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    CK(h, cudaSetDevice(h->p.device));
     const size_t nn = (size_t)h->p.nx * h->p.ny;
-    std::vector<double> m(3 * nn);
-    for (size_t i = 0; i < nn; i++) {
-        m[i] = rho ? rho[i] : 1.0;
-        m[nn + i] = ux ? ux[i] : 0.0;
-        m[2 * nn + i] = uy ? uy[i] : 0.0;
-        if (!(m[i] > 0) || !std::isfinite(m[nn + i]) || !std::isfinite(m[2 * nn + i]))
-            return fail(h, IPPI_ERR_ARG, "initial rho must be positive and u finite (node %zu)", i);
-    }
     if (!h->init_m) CK(h, dalloc(&h->init_m, 3 * nn * sizeof(double)));
-    CK(h, cudaMemcpy(h->init_m, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(h, cudaMemset(h->avg, 0, 3 * nn * h->csize));
+    // host fields straight into the device table (fast from pinned memory),
+    // defaults and the validity check on the device
+    const double* src[3] = {rho, ux, uy};
+    for (int q = 0; q < 3; q++)
+        if (src[q])
+            CK(h, cudaMemcpyAsync(h->init_m + q * nn, src[q], nn * sizeof(double),
+                                  cudaMemcpyHostToDevice, h->st));
+    unsigned long long* bad = reinterpret_cast<unsigned long long*>(h->red);
+    CK(h, cudaMemsetAsync(bad, 0xff, sizeof *bad, h->st));
+    init_fields_kernel<<<std::min<size_t>((nn + 255) / 256, 4096), 256, 0, h->st>>>(
+        h->init_m, (long long)nn, rho != nullptr, ux != nullptr, uy != nullptr, bad);
+    CK(h, cudaGetLastError());
+    CK(h, cudaMemsetAsync(h->avg, 0, 3 * nn * h->csize, h->st));
+    unsigned long long first_bad = 0;
+    CK(h, cudaMemcpyAsync(&first_bad, bad, sizeof first_bad, cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    if (first_bad != ~0ull)
+        return fail(h, IPPI_ERR_ARG, "initial rho must be positive and u finite (node %llu)", first_bad);
+    // the step graphs read the initial fields only through MODE_INIT, which
+    // is launched outside them: they stay valid
     h->pending_init = true;
     h->dl_valid = false;
     h->hist_written = 0;
-    drop_graphs(h);
     return IPPI_OK;
 }
 
@@ -906,15 +937,20 @@ int ippi_step(ippi_lbm* h, int nsteps, int t0)
     const int q = h->kcount & 1;  // parity of the first step; graphs keep it
     while (left >= 2) {
         if (!h->graph[h->cur][q]) {
-            rc = build_graph(h, h->cur, q);
+            rc = build_graph(h, 2, h->cur, q);
             if (rc) return rc;
         }
         CK(h, cudaGraphLaunch(h->graph[h->cur][q], h->st));
         left -= 2;
     }
     if (left) {
-        LaunchSet L = make_launch(h, MODE_STEP, h->f[h->cur], h->f[h->cur ^ 1], q);
-        CK(h, launch(L, h->S));
+        // one step (a driver calling once per step): its own graph
+        const int q1 = q;  // an even number of steps came before in this call
+        if (!h->graph1[h->cur][q1]) {
+            rc = build_graph(h, 1, h->cur, q1);
+            if (rc) return rc;
+        }
+        CK(h, cudaGraphLaunch(h->graph1[h->cur][q1], h->st));
         h->cur ^= 1;
     }
     h->kcount += nsteps;
@@ -1068,12 +1104,16 @@ int ippi_force_history(ippi_lbm* h, double* out, int max_steps)
     const long long avail = std::min<long long>(h->hist_written + (h->pending_init ? 0 : 1), h->hist_cap);
     const int n = (int)std::min<long long>(avail, max_steps);
     const int nb = h->nbody;
-    std::vector<double> all((size_t)h->hist_cap * nb * 2);
-    CK(h, cudaMemcpy(all.data(), h->force_hist, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < n; i++) {
+    // the ring slots of steps last_t - n + 1 .. last_t: at most two runs
+    const size_t row = (size_t)nb * 2 * sizeof(double);
+    int i = 0;
+    while (i < n) {
         const long long t = (long long)h->last_t - (n - 1) + i;
         const long long slot = ((t % h->hist_cap) + h->hist_cap) % h->hist_cap;
-        std::memcpy(out + (size_t)i * nb * 2, all.data() + (size_t)slot * nb * 2, nb * 2 * sizeof(double));
+        const int run = (int)std::min<long long>(n - i, h->hist_cap - slot);
+        CK(h, cudaMemcpy(out + (size_t)i * nb * 2, h->force_hist + (size_t)slot * nb * 2, run * row,
+                         cudaMemcpyDeviceToHost));
+        i += run;
     }
     return n;
 }

@@ -1,0 +1,377 @@
+// mesh.cpp -- Mesh over the C ABI of include/ippi_lbm.h.  Method by method
+// the reference's IPPI-LBM/mesh.cpp entry points that its driver calls; the
+// time step itself (streaming, boundaries, LES, collision, IB, nets,
+// averages, error check) is one ippi_step call on the GPU.
+#include "mesh.h"
+
+#include <sys/stat.h>
+
+#include <cstdlib>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+
+namespace {
+
+const char* field_err(ippi_lbm* h)
+{
+    static char buf[512];
+    ippi_last_error(h, buf, sizeof buf);
+    return buf;
+}
+
+}  // namespace
+
+Mesh::Mesh() {}
+
+Mesh::~Mesh()
+{
+    if (h_) ippi_destroy(h_);
+}
+
+bool Mesh::check(int rc, const char* what)
+{
+    if (rc == IPPI_OK) return true;
+    if (rc == IPPI_ERR_DIVERGED) {
+        // Mesh::ErrorCatch (mesh.cpp:2101-2111)
+        cerr << "Simulation Error!" << endl;
+        errorflag = 1;
+    } else {
+        cerr << what << ": " << field_err(h_) << endl;
+    }
+    if (AbortOnError) std::exit(1);
+    return false;
+}
+
+// Mesh::InitialLatMesh (mesh.cpp:60-171): the whole lattice on one GPU, rho =
+// Rho, u = 0, populations at equilibrium.  Nx is LatmeshSizeNx when set,
+// else the slab width of the single rank.
+void Mesh::InitialLatMesh(int Nx_P, int Ny, double tau, Point2D StartVel, double Rho, int RankID,
+                          int CoreNum, int PartitionRemainderFlag)
+{
+    if (RankID != 0 || CoreNum != 1) {
+        cerr << "InitialLatMesh: one GPU holds the lattice; run one rank (RankID 0, CoreNum 1)" << endl;
+        if (AbortOnError) std::exit(1);
+        return;
+    }
+    const int nx = LatmeshSizeNx > 0 ? LatmeshSizeNx : (PartitionRemainderFlag ? PartitionRemainderFlag : Nx_P);
+    ippi_params p;
+    ippi_params_default(&p, nx, Ny);
+    p.collision = Collision;
+    p.storage = Storage;
+    p.bc_set = BoundarySet;
+    p.les_model = LesModel;
+    p.tau0 = tau;
+    p.cs = StartCs;
+    p.u_in = StartVel.x;
+    p.rho0 = Rho;
+    p.plate_x0 = PlateX0;
+    p.avg_start = startAvg;
+    p.delta_kernel = DeltaKernel;
+    p.mdf_iters = MdfIters;
+    p.device = Device;
+    if (h_) ippi_destroy(h_);
+    h_ = nullptr;
+    if (!check(ippi_create(&p, &h_), "ippi_create")) return;
+    nx_ = nx;
+    ny_ = Ny;
+    LatmeshSizeNx = nx;
+    LatmeshSizeNy = Ny;
+    ParallelSize = nx;
+    if (Rho != 1.0) {
+        std::vector<double> r((size_t)nx * Ny, Rho);
+        if (!check(ippi_init_macros(h_, r.data(), nullptr, nullptr), "ippi_init_macros")) return;
+    }
+    LatMesh.assign(nx + 2, vector<Lattice>(Ny));
+    for (int i = 0; i < nx + 2; i++)
+        for (int j = 0; j < Ny; j++) {
+            Lattice& L = LatMesh[i][j];
+            L.pos = {i - 1, j};
+            L.rho = (REAL)Rho;
+            L.tau = L.TauAtBeginning = (REAL)tau;
+            L.u = {0, 0};
+            L.InitialLatticeFeq();
+        }
+    synced_ = false;
+}
+
+void Mesh::SetInitialField(const double* rho, const double* ux, const double* uy)
+{
+    if (!h_) return;
+    check(ippi_init_macros(h_, rho, ux, uy), "ippi_init_macros");
+    synced_ = false;
+}
+
+bool Mesh::LoadBandNet(int type, const float* w, size_t n)
+{
+    return h_ && check(ippi_load_band_net(h_, type, w, n), "ippi_load_band_net");
+}
+
+// Mesh::InitialIBParticle (mesh.cpp:173-191): NumNodes markers on the circle,
+// marker i at (X + R sin(2 pi i / N), Y + R cos(2 pi i / N)), prescribed
+// velocity ParticleVel.  Each marker carries its arc length 2 pi R / N so
+// the body force is the boundary integral (the reference's marker force
+// leaves that factor out, mesh.cpp:527-528).
+void Mesh::InitialIBParticle(int NumNodes, double Radius, double ParticlePositionX,
+                             double ParticlePositionY, Point2D ParticleVel)
+{
+    IBParticle.assign(NumNodes, Particlenode());
+    std::vector<double> xy(2 * (size_t)NumNodes), ub(2 * (size_t)NumNodes), ds(NumNodes);
+    for (int i = 0; i < NumNodes; i++) {
+        Particlenode& P = IBParticle[i];
+        P.position.x = (REAL)(ParticlePositionX + Radius * std::sin(2. * M_PI * (double)i / NumNodes));
+        P.position.y = (REAL)(ParticlePositionY + Radius * std::cos(2. * M_PI * (double)i / NumNodes));
+        P.position_ref = P.position;
+        P.vel = ParticleVel;
+        P.center = {(REAL)ParticlePositionX, (REAL)ParticlePositionY};
+        xy[2 * i] = P.position.x;
+        xy[2 * i + 1] = P.position.y;
+        ub[2 * i] = ParticleVel.x;
+        ub[2 * i + 1] = ParticleVel.y;
+        ds[i] = 2. * M_PI * Radius / NumNodes;
+    }
+    center = {(REAL)ParticlePositionX, (REAL)ParticlePositionY};
+    radius = Radius;
+    if (h_) check(ippi_set_markers(h_, NumNodes, xy.data(), ub.data(), nullptr, ds.data()), "ippi_set_markers");
+}
+
+// Mesh::JudgeStyle (mesh.cpp:1391-1454): the node kinds follow from the
+// boundary set chosen at InitialLatMesh; this reads them into the mirror.
+void Mesh::JudgeStyle(Point2D CylinderCenter1, REAL Radius, int RankID, int CoreNum)
+{
+    (void)RankID;
+    (void)CoreNum;
+    center = CylinderCenter1;
+    radius = Radius;
+    if (!h_) return;
+    std::vector<unsigned char> fl((size_t)nx_ * ny_);
+    if (!check(ippi_download(h_, IPPI_FIELD_FLAGS, fl.data(), fl.size()), "ippi_download")) return;
+    for (int x = 0; x < nx_; x++)
+        for (int y = 0; y < ny_; y++) LatMesh[x + 1][y].style = (char)fl[(size_t)y * nx_ + x];
+}
+
+// Mesh::OneLBMStep (mesh.cpp:357-513): one step numbered t.  Cs and Pr are
+// fixed at InitialLatMesh (StartCs); RankID / CoreNum are 0 / 1.
+void Mesh::OneLBMStep(int RankID, int CoreNum, REAL Cs, REAL Pr, int t)
+{
+    (void)RankID;
+    (void)CoreNum;
+    (void)Cs;
+    (void)Pr;
+    RunSteps(t, 1);
+}
+
+void Mesh::RunSteps(int t0, int n)
+{
+    if (!h_ || n <= 0) return;
+    check(ippi_step(h_, n, t0), "ippi_step");
+    last_t_ = t0 + n - 1;
+    synced_ = false;
+}
+
+// Mesh::ComputeAvgVelocity (mesh.cpp:1954-1974): the running means of u, v
+// and rho from step startAvg on are updated inside every step on the GPU.
+void Mesh::ComputeAvgVelocity(int t) { (void)t; }
+
+void Mesh::Sync(bool with_f)
+{
+    if (!h_) return;
+    const size_t nn = (size_t)nx_ * ny_;
+    std::vector<double> buf(nn);
+    auto get = [&](int field, auto&& put) {
+        if (!check(ippi_download(h_, field, buf.data(), nn * sizeof(double)), "ippi_download")) return;
+        for (int y = 0; y < ny_; y++)
+            for (int x = 0; x < nx_; x++) put(LatMesh[x + 1][y], buf[(size_t)y * nx_ + x]);
+    };
+    get(IPPI_FIELD_RHO, [](Lattice& L, double v) { L.rho = (REAL)v; L.p = (REAL)(v / 3.0); });
+    get(IPPI_FIELD_UX, [](Lattice& L, double v) { L.u.x = (REAL)v; });
+    get(IPPI_FIELD_UY, [](Lattice& L, double v) { L.u.y = (REAL)v; });
+    get(IPPI_FIELD_TAU, [](Lattice& L, double v) { L.tau = (REAL)v; });
+    get(IPPI_FIELD_AVG_U, [](Lattice& L, double v) { L.avg_u = v; });
+    get(IPPI_FIELD_AVG_V, [](Lattice& L, double v) { L.avg_v = v; });
+    get(IPPI_FIELD_AVG_RHO, [](Lattice& L, double v) { L.avg_density = v; });
+    get(IPPI_FIELD_NNFLAG, [](Lattice& L, double v) { L.NNflag = v != 0; });
+    if (with_f) {
+        std::vector<double> f(9 * nn);
+        if (check(ippi_download(h_, IPPI_FIELD_F, f.data(), f.size() * sizeof(double)), "ippi_download"))
+            for (int k = 0; k < 9; k++)
+                for (int y = 0; y < ny_; y++)
+                    for (int x = 0; x < nx_; x++)
+                        LatMesh[x + 1][y].fnew[k] = (REAL)f[k * nn + (size_t)y * nx_ + x];
+    }
+    synced_ = true;
+}
+
+void Mesh::ensure_synced()
+{
+    if (!synced_) Sync(false);
+}
+
+// Mesh::ErrorCatch (mesh.cpp:2101-2111) on the mirror; the step checks every
+// node on the GPU already (ippi_step reports IPPI_ERR_DIVERGED).
+void Mesh::ErrorCatch(int i, int j)
+{
+    ensure_synced();
+    const double r = LatMesh[i][j].rho;
+    if (r > 10 || r < 0) {
+        cerr << "Simulation Error!" << endl;
+        errorflag = 1;
+        if (AbortOnError) std::exit(1);
+    }
+}
+
+// Mesh::InitialFile (mesh.cpp:1170-1179)
+void Mesh::InitialFile()
+{
+    ::mkdir("fluid", 0755);
+    ::mkdir("particle", 0755);
+    ::mkdir("cp", 0755);
+}
+
+// Mesh::WriteDatFluid (mesh.cpp:1180-1243): Tecplot point data, x-major, one
+// line per node: X Y Density U V avgu avgv tau avgRho
+void Mesh::WriteDatFluid(int t, int RankID, int NX, int CoreNum)
+{
+    (void)CoreNum;
+    ensure_synced();
+    std::ostringstream name;
+    name << "fluid/fluid_t" << t << "_" << RankID << ".dat";
+    std::ofstream out(name.str());
+    if (RankID == 0) {
+        out << "TITLE = \"Simulation of Fluid State at Time " << t << "\"\n";
+        out << "VARIABLES = \"X\" \"Y\" \"Density\" \"U\" \"V\" \"avgu\" \"avgv\" \"tau\" \"avgRho\" \n";
+        out << "ZONE T=\"Time " << t << "\", ";
+        out << "I=" << ny_ << ", J=" << NX << ", K=1, ";
+        out << "DATAPACKING=POINT, ZONETYPE=Ordered\n";
+    }
+    for (int X = 1; X < nx_ + 1; ++X)
+        for (int Y = 0; Y < ny_; ++Y) {
+            const Lattice& L = LatMesh[X][Y];
+            out << L.pos.x << " " << L.pos.y << " " << L.rho << " " << L.u.x << " " << L.u.y << " "
+                << L.avg_u << " " << L.avg_v << " " << L.tau << " " << L.avg_density << "\n";
+        }
+}
+
+namespace {
+// MergeDatFluid / MergeAvgu (mesh.cpp:1320-1353, 2069-2098): concatenate the
+// per-rank files and delete them
+void merge(const std::string& base, const std::string& merged, int CoreNum)
+{
+    std::ofstream out(merged);
+    for (int i = 0; i <= CoreNum; ++i) {
+        const std::string in_name = base + std::to_string(i) + ".dat";
+        std::ifstream in(in_name);
+        if (!in) continue;
+        out << in.rdbuf();
+        in.close();
+        std::remove(in_name.c_str());
+    }
+}
+}  // namespace
+
+void Mesh::MergeDatFluid(int t, int CoreNum)
+{
+    merge("fluid/fluid_t" + std::to_string(t) + "_", "fluid/fluid_Merged_" + std::to_string(t) + ".dat",
+          CoreNum);
+}
+
+// Mesh::WriteAvgu (mesh.cpp:2010-2068): inner rows, style code 0 fluid, 1
+// solid, 2 boundary, 3 other kinds
+void Mesh::WriteAvgu(int t, int RankID, int NX, int CoreNum)
+{
+    (void)CoreNum;
+    ensure_synced();
+    std::ostringstream name;
+    name << "fluid/Avgu_" << t << "_" << RankID << ".dat";
+    std::ofstream out(name.str());
+    if (RankID == 0) {
+        out << "TITLE = \"Simulation of Fluid State at Time " << t << "\"\n";
+        out << "VARIABLES = \"X\" \"Y\" \"AvgdDenstiy\" \"U\" \"V\" \"avgy\" \"avgv\" \"Style\" \n";
+        out << "ZONE T=\"Time " << t << "\", ";
+        out << "I=" << ny_ - 2 << ", J=" << NX << ", K=1, ";
+        out << "DATAPACKING=POINT, ZONETYPE=Ordered\n";
+    }
+    for (int X = 1; X < nx_ + 1; ++X)
+        for (int Y = 1; Y < ny_ - 1; ++Y) {
+            const Lattice& L = LatMesh[X][Y];
+            const int code = L.style == 'f' ? 0 : L.style == 's' ? 1 : L.style == 'b' ? 2 : 3;
+            out << L.pos.x << " " << L.pos.y << " " << L.rho << " " << L.u.x << " " << L.u.y << " "
+                << L.avg_u << " " << L.avg_v << " " << code << "\n";
+        }
+}
+
+void Mesh::MergeAvgu(int t, int CoreNum)
+{
+    merge("fluid/Avgu_" + std::to_string(t) + "_", "fluid/fluid_avg_" + std::to_string(t) + ".dat", CoreNum);
+}
+
+// Mesh::WriteDatParticle (mesh.cpp:1283-1317): the marker polyline
+void Mesh::WriteDatParticle(int t)
+{
+    std::ostringstream name;
+    name << "particle/particle_t" << t << ".dat";
+    std::ofstream out(name.str());
+    const size_t n = IBParticle.size();
+    out << "TITLE = \"Particle State at Time " << t << "\"\n";
+    out << "VARIABLES = \"X\" \"Y\" \"Z\"\n";
+    out << "ZONE T=\"Particle\", N=" << n << ", E=" << n;
+    out << ", DATAPACKING=POINT, ZONETYPE=FELINESEG\n";
+    out << "Nodes=" << n << ", Elements=" << n << "\n";
+    for (size_t i = 0; i < n; ++i) out << IBParticle[i].position.x << " " << IBParticle[i].position.y << " 0\n";
+    for (size_t i = 0; i + 1 < n; ++i) out << i + 1 << " " << i + 2 << "\n";
+    if (n) out << 1 << " " << n << "\n";
+}
+
+// Mesh::GetSt (mesh.cpp:1975-2009): velocity profiles at x = 9.33 stepH and
+// x = 12 stepH appended to particle/5.33H_<t>.dat and particle/8.0H_<t>.dat
+void Mesh::GetSt(int t)
+{
+    ensure_synced();
+    for (int i = 1; i < nx_ + 1; i++)
+        for (int j = 0; j < ny_; j++) {
+            const Lattice& L = LatMesh[i][j];
+            const char* which[2] = {"5.33H_", "8.0H_"};
+            const double at[2] = {9.33 * stepH, 12.0 * stepH};
+            for (int q = 0; q < 2; q++)
+                if (L.pos.x == at[q]) {
+                    std::ofstream out("particle/" + std::string(which[q]) + std::to_string(t) + ".dat",
+                                      std::ios::app);
+                    out << L.pos.y * 0.005 << " " << L.u.x << " " << L.u.y << " " << L.avg_u << " "
+                        << L.avg_v << std::endl;
+                }
+        }
+}
+
+int Mesh::BodyForces(double* fxy, int max_bodies)
+{
+    if (!h_) return 0;
+    int nb = 0;
+    if (!check(ippi_forces(h_, nullptr, &nb, nullptr), "ippi_forces")) return 0;
+    std::vector<double> f(2 * (size_t)std::max(nb, 1));
+    if (!check(ippi_forces(h_, f.data(), &nb, nullptr), "ippi_forces")) return 0;
+    for (int b = 0; b < nb && b < max_bodies; b++) {
+        fxy[2 * b] = f[2 * b];
+        fxy[2 * b + 1] = f[2 * b + 1];
+    }
+    for (size_t m = 0; m < IBParticle.size() && nb > 0; m++) IBParticle[m].force = {0, 0};
+    return nb;
+}
+
+void Mesh::DragLift(double U, double D, double* cd, double* cl)
+{
+    double f[2] = {0, 0};
+    BodyForces(f, 1);
+    const double q = 0.5 * U * U * D;
+    *cd = f[0] / q;
+    *cl = f[1] / q;
+}
+
+void Mesh::OutputForces(int t, double U, double D)
+{
+    double f[2] = {0, 0};
+    BodyForces(f, 1);
+    const double q = 0.5 * U * U * D;
+    std::ofstream out("particle/forces.dat", std::ios::app);
+    out.precision(12);
+    out << t << " " << f[0] << " " << f[1] << " " << f[0] / q << " " << f[1] / q << "\n";
+}

@@ -1,0 +1,108 @@
+// mesh.h -- the reference's Mesh class (IPPI-LBM/mesh.h:32-114) as a host
+// object over the B200 time step (include/ippi_lbm.h).
+//
+// Same public fields and the same call sequence as the reference's driver
+// (main.cpp): set the fields, InitialLatMesh, JudgeStyle, optionally
+// InitialIBParticle, then OneLBMStep / ComputeAvgVelocity every step and
+// WriteDatFluid + MergeDatFluid every SaveStep steps.  Differences:
+//   * one GPU holds the whole lattice: RankID / CoreNum are accepted and
+//     must be 0 / 1 (no MPI slabs, no halo exchange);
+//   * the node state lives on the GPU; LatMesh is its host mirror, refreshed
+//     by Sync() and by the methods that read it;
+//   * ComputeAvgVelocity is fused into the step (the averages start at
+//     startAvg) and only refreshes nothing on the host;
+//   * RunSteps(t0, n) advances n steps in one call (CUDA graphs, one
+//     synchronisation) for drivers that need no per-step host work;
+//   * a diverged run (ErrorCatch: rho outside [0, 10]) prints the reference's
+//     message and sets errorflag; with AbortOnError (default) it exits like
+//     the reference's MPI_Abort.
+#pragma once
+#ifndef MESH_H
+#define MESH_H
+#define _USE_MATH_DEFINES
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "NodeAndLattice.h"
+
+class Mesh {
+public:
+    Mesh();
+    ~Mesh();
+    Mesh(const Mesh&) = delete;
+    Mesh& operator=(const Mesh&) = delete;
+
+    vector<Particlenode> IBParticle;
+    vector<vector<Lattice>> LatMesh;  // [NX = Nx + 2][Ny], halo columns 0 and NX - 1
+    int LatmeshSizeNx = 0;
+    int LatmeshSizeNy = 0;
+    Point2D center{0, 0};
+    double radius = 0;
+    const double eps = 1.0e-9;
+    double startTau = 0;
+    Point2D startU{0, 0};
+    int MyrankID = 0;
+    int MyCoreNum = 1;
+    int stepH = 0, stepL = 0;
+    int startAvg = 0;
+    double StartCs = 0;
+    int errorflag = 0;
+    int ParallelSize = 0;
+
+    // settings with no field in the reference (Parameter.h gives the defaults)
+    int BoundarySet = IPPI_BC_REF_NEE;  // IPPI_BC_CHANNEL: Zou-He inlet, walls
+    int Collision = ippi_host::kCollision;
+    int Storage = ippi_host::kStorage;
+    int LesModel = ippi_host::kLes;
+    int DeltaKernel = ippi_host::kDelta;
+    int MdfIters = 1;
+    int PlateX0 = 400;  // flat plate: specular bottom for x < PlateX0 (mesh.cpp:1413)
+    int Device = 0;
+    bool AbortOnError = true;
+
+    // ---- the reference's API ------------------------------------------
+    void InitialLatMesh(int Nx_P, int Ny, double tau, Point2D StartVel, double Rho, int RankID,
+                        int CoreNum, int PartitionRemainderFlag);
+    void InitialIBParticle(int NumNodes, double Radius, double ParticlePositionX,
+                           double ParticlePositionY, Point2D ParticleVel);
+    void JudgeStyle(Point2D CylinderCenter1, REAL Radius, int RankID, int CoreNum);
+    void OneLBMStep(int RankID, int CoreNum, REAL Cs, REAL Pr, int t);
+    void ComputeAvgVelocity(int t);
+    void ErrorCatch(int i, int j);
+    void InitialFile();
+    void WriteDatFluid(int t, int RankID, int NX, int CoreNum);
+    void MergeDatFluid(int t, int CoreNum);
+    void WriteAvgu(int t, int RankID, int NX, int CoreNum);
+    void MergeAvgu(int t, int CoreNum);
+    void WriteDatParticle(int t);
+    void GetSt(int t);
+
+    // ---- additions ----------------------------------------------------
+    // initial macroscopic fields rho/ux/uy[Ny][Nx] (NULL: rho 1, u 0)
+    void SetInitialField(const double* rho, const double* ux, const double* uy);
+    // boundary net weights (NNmodel/AutoT0<type>.pt in TorchScript order)
+    bool LoadBandNet(int type, const float* w, size_t n);
+    // n steps numbered t0 .. t0 + n - 1
+    void RunSteps(int t0, int n);
+    // refresh LatMesh from the device (populations too when with_f)
+    void Sync(bool with_f = false);
+    // per-body force of the last step (FP64); returns the body count
+    int BodyForces(double* fxy, int max_bodies);
+    // drag / lift coefficients -sum(F) / (0.5 U^2 D) of body 0
+    void DragLift(double U, double D, double* cd, double* cl);
+    // one line "t Fx Fy Cd Cl" appended to particle/forces.dat
+    void OutputForces(int t, double U, double D);
+    ippi_lbm* Handle() { return h_; }
+
+private:
+    ippi_lbm* h_ = nullptr;
+    int nx_ = 0, ny_ = 0;
+    bool synced_ = false;
+    int last_t_ = 0;
+    std::vector<double> init_rho_, init_ux_, init_uy_;
+    bool check(int rc, const char* what);
+    void ensure_synced();
+};
+#endif

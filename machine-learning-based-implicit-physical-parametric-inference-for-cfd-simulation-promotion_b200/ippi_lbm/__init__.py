@@ -1,8 +1,8 @@
 """ippi_lbm -- Python host side of the B200 D2Q9 time step.
 
 ``Lattice`` wraps one lattice of the C ABI (libippi_lbm.so, include/ippi_lbm.h);
-``Mesh`` mirrors the reference's Mesh class (IPPI-LBM/mesh.h) method by method
-for drop-in use from Python; ``scenes`` builds the benchmark inputs.
+``scenes`` builds the benchmark inputs.  The reference's own C++ API (Mesh,
+Lattice, main.cpp) is mirrored in C++ by ../host/ over the same ABI.
 """
 from ._lib import (BC_CHANNEL, BC_REF_NEE, BF16, BGK, DELTA_BILINEAR, DELTA_PESKIN4, F16, F32,
                    F64, FIELD_AVG_RHO, FIELD_AVG_U, FIELD_AVG_V, FIELD_F, FIELD_FLAGS,

@@ -188,3 +188,13 @@ def test_bad_arguments_are_rejected():
         g.set_markers(cylinder_markers(3.0, 16.0, 2.0, 8))  # stencil leaves the interior
     with pytest.raises(ip.IppiError):
         g.load_band_net(1, np.zeros(10, np.float32))
+    rho = np.ones((32, 64))
+    rho[5, 7] = 0.0
+    with pytest.raises(ip.IppiError, match=r"node 327\b"):
+        g.init_macros(rho)
+    ux = np.zeros((32, 64))
+    ux[31, 63] = np.nan
+    with pytest.raises(ip.IppiError, match=r"node 2047\b"):
+        g.init_macros(None, ux)
+    g.init_macros()  # defaults are valid; the handle still steps
+    g.step(2, 1)
