@@ -44,7 +44,7 @@
 extern "C" {
 #endif
 
-#define IPPI_ABI_VERSION 1
+#define IPPI_ABI_VERSION 2
 
 /* status codes */
 #define IPPI_OK 0
@@ -70,6 +70,8 @@ extern "C" {
 /* subgrid model */
 #define IPPI_LES_NONE 0
 #define IPPI_LES_SMAGORINSKY 1 /* SmagorinskyByHybrid, mesh.cpp:852-911 */
+#define IPPI_LES_LEARNED 2     /* per-node network (ippi_load_tau_mlp), Smagorinsky
+                                  outside its training range; channel scene only */
 /* IB interpolation/spreading kernel */
 #define IPPI_DELTA_BILINEAR 0 /* mesh.cpp:606-644 (default of Parameter.h) */
 #define IPPI_DELTA_PESKIN4 1  /* Dirac_Delta, mesh.cpp:555-605, 1354-1389 */
@@ -168,6 +170,49 @@ int ippi_get_stream(ippi_lbm* h, void** stream);
  * ippi_step. */
 int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk,
                        double* ms_band, double* ms_ib);
+
+/* No counterpart in the reference: the learned relaxation time
+ * (IPPI_LES_LEARNED).  tau = tau0 + out_scale * softplus(MLP(x)) with
+ * x = (features - mean) / std and the MLP 6 -> 32 tanh -> 32 tanh -> 1.
+ * Features of a node, from its post-stream state (Pi_neq as in the
+ * Smagorinsky model, S = -3/(2 rho tau0) Pi_neq):
+ *   rho, |u|, Pi_xx/|Pi|, Pi_xy/|Pi|, Pi_yy/|Pi|, |S| = sqrt(2 S:S)
+ * with |Pi| = sqrt(Pi_xx^2 + 2 Pi_xy^2 + Pi_yy^2).  Nodes with any feature
+ * outside [lo, hi] take the Smagorinsky tau.
+ * w_bf16[1313]: BF16 bit patterns of W1[32][6] b1[32] W2[32][32] b2[32]
+ * w3[32] b3 (row-major, out x in).  stats[25]: mean[6] std[6] lo[6] hi[6]
+ * out_scale. */
+#define IPPI_MLP_PARAMS 1313
+#define IPPI_MLP_STATS 25
+int ippi_load_tau_mlp(ippi_lbm* h, const uint16_t* w_bf16, size_t n, const float* stats,
+                      size_t nstats);
+
+/* Filtered snapshot of the current state for training the learned tau:
+ * box filter over factor x factor blocks (nx, ny multiples of factor) into
+ * out[6][ny/factor][nx/factor] (host, FP64): rho_bar, ux_bar, uy_bar
+ * (density-weighted), Sxx, Sxy, Syy of the effective stress
+ *   Sigma = box(sigma) - (box(rho u u) - rho_bar u_bar u_bar),
+ *   sigma = -(1 - 1/(2 tau)) Pi_neq  (the lattice's deviatoric stress),
+ * i.e. the stress a coarse lattice must carry to reproduce the filtered
+ * fine-lattice momentum flux. */
+int ippi_filter_snapshot(ippi_lbm* h, int factor, double* out, size_t bytes);
+
+/* Training kernels of the learned tau (FP32, device pointers, enqueued on
+ * `stream`; deterministic for a given n).
+ * ippi_mlp_grad: x[n][6] standardised features, y[n] targets of
+ *   softplus(MLP(x)) (offset / out_scale), w[1313] FP32 parameters ->
+ *   grad[1313] of the mean squared error and *loss (may be NULL); scratch
+ *   holds ippi_mlp_scratch_floats() floats.
+ * ippi_mlp_adam: one Adam step (step >= 1) on w with moments m, v.
+ * ippi_mlp_forward: out[n] = softplus(MLP(x)). */
+#define IPPI_MLP_GRAD_BLOCKS 296
+int ippi_mlp_param_count(void);
+size_t ippi_mlp_scratch_floats(void);
+int ippi_mlp_grad(const float* x, const float* y, int n, const float* w, float* grad, float* loss,
+                  float* scratch, void* stream);
+int ippi_mlp_adam(float* w, const float* grad, float* m, float* v, int step, float lr, float beta1,
+                  float beta2, float eps, void* stream);
+int ippi_mlp_forward(const float* x, int n, const float* w, float* out, void* stream);
 
 /* Last error message of the handle (or of the library when h is NULL). */
 int ippi_last_error(ippi_lbm* h, char* buf, size_t n);

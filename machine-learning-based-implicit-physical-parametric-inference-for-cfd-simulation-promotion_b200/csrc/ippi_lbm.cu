@@ -96,6 +96,8 @@ struct ippi_lbm {
     double* force_now = nullptr;
     double* force_hist = nullptr;
     long long hist_written = 0;
+    // learned tau: parameters (FP32 values of the BF16 weights) + statistics
+    float* mlp_dev = nullptr;
     // graphs of two steps and of one step: [start buffer][step parity]
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     cudaGraphExec_t graph1[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -116,6 +118,47 @@ __global__ void init_fields_kernel(double* m, long long nn, int has_rho, int has
         if (!(m[i] > 0) || !isfinite(m[nn + i]) || !isfinite(m[2 * nn + i]))
             atomicMin(bad, (unsigned long long)i);
     }
+}
+
+// Box filter of the materialised post-stream state over fac x fac blocks
+// (ippi_filter_snapshot).  dl planes: f[0..8], rho 9, ux 10, uy 11, tau 13.
+__global__ void filter_snapshot_kernel(const double* dl, int nx, int ny, int fac, double* out)
+{
+    const int cx = blockIdx.x * blockDim.x + threadIdx.x, cy = blockIdx.y;
+    const int mx = nx / fac, my = ny / fac;
+    if (cx >= mx || cy >= my) return;
+    const long long nn = (long long)nx * ny;
+    double r = 0, jx = 0, jy = 0, txx = 0, txy = 0, tyy = 0, sxx = 0, sxy = 0, syy = 0;
+    for (int dy = 0; dy < fac; dy++)
+        for (int dx = 0; dx < fac; dx++) {
+            const long long n = (long long)(cy * fac + dy) * nx + (cx * fac + dx);
+            const double* f = dl + n;
+            const double rho = dl[9 * nn + n], ux = dl[10 * nn + n], uy = dl[11 * nn + n];
+            const double tau = dl[13 * nn + n];
+            const double d = f[5 * nn] + f[6 * nn] + f[7 * nn] + f[8 * nn];
+            const double pxx = f[1 * nn] + f[3 * nn] + d - rho / 3 - rho * ux * ux;
+            const double pyy = f[2 * nn] + f[4 * nn] + d - rho / 3 - rho * uy * uy;
+            const double pxy = f[5 * nn] - f[6 * nn] + f[7 * nn] - f[8 * nn] - rho * ux * uy;
+            const double c = -(1.0 - 0.5 / tau);
+            sxx += c * pxx;
+            sxy += c * pxy;
+            syy += c * pyy;
+            r += rho;
+            jx += rho * ux;
+            jy += rho * uy;
+            txx += rho * ux * ux;
+            txy += rho * ux * uy;
+            tyy += rho * uy * uy;
+        }
+    const double inv = 1.0 / ((double)fac * fac);
+    const double rb = r * inv, ub = jx / r, vb = jy / r;
+    const long long m = (long long)mx * my, o = (long long)cy * mx + cx;
+    out[o] = rb;
+    out[m + o] = ub;
+    out[2 * m + o] = vb;
+    out[3 * m + o] = sxx * inv - (txx * inv - rb * ub * ub);
+    out[4 * m + o] = sxy * inv - (txy * inv - rb * ub * vb);
+    out[5 * m + o] = syy * inv - (tyy * inv - rb * vb * vb);
 }
 
 namespace {
@@ -547,7 +590,8 @@ LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int pa
     a.plane = h->plane;
     a.nx = h->p.nx;
     a.ny = h->p.ny;
-    a.les = h->p.les_model == IPPI_LES_SMAGORINSKY;
+    a.les = h->p.les_model;
+    a.mlp = h->mlp_dev;
     a.plate_x0 = h->p.plate_x0;
     a.tau0 = h->p.tau0;
     a.cs = h->p.cs;
@@ -625,8 +669,17 @@ int set_time(ippi_lbm* h, int t)
 }
 
 // the first collision, from the equilibrium of the initial moments (k = 0)
+// every launch computes relaxation times: the learned model needs its network
+int tau_ready(ippi_lbm* h)
+{
+    if (h->p.les_model == IPPI_LES_LEARNED && !h->mlp_dev)
+        return fail(h, IPPI_ERR_STATE, "learned tau selected but no network loaded (ippi_load_tau_mlp)");
+    return IPPI_OK;
+}
+
 int run_init(ippi_lbm* h)
 {
+    if (int rc = tau_ready(h)) return rc;
     std::memset(h->ctr_h, 0, sizeof(Ctr));
     CK(h, cudaMemcpyAsync(h->ctr, h->ctr_h, sizeof(Ctr), cudaMemcpyHostToDevice, h->st));
     CK(h, cudaStreamSynchronize(h->st));
@@ -668,6 +721,7 @@ int build_graph(ippi_lbm* h, int n, int b, int q)
 int materialize(ippi_lbm* h)
 {
     if (h->dl_valid) return IPPI_OK;
+    if (int rc = tau_ready(h)) return rc;
     const size_t nn = (size_t)h->p.nx * h->p.ny;
     if (!h->dl) CK(h, dalloc(&h->dl, 14 * nn * sizeof(double)));
     CK(h, cudaMemsetAsync(h->dl + 12 * nn, 0, nn * sizeof(double), h->st));  // net-flag plane
@@ -723,7 +777,9 @@ int ippi_create(const ippi_params* p, ippi_lbm** out)
     if (p->collision < 0 || p->collision > 2) return fail(nullptr, IPPI_ERR_ARG, "bad collision");
     if (p->storage < 0 || p->storage > 3) return fail(nullptr, IPPI_ERR_ARG, "bad storage");
     if (p->bc_set < 0 || p->bc_set > 1) return fail(nullptr, IPPI_ERR_ARG, "bad bc_set");
-    if (p->les_model < 0 || p->les_model > 1) return fail(nullptr, IPPI_ERR_ARG, "bad les_model");
+    if (p->les_model < 0 || p->les_model > 2) return fail(nullptr, IPPI_ERR_ARG, "bad les_model");
+    if (p->les_model == IPPI_LES_LEARNED && p->bc_set != IPPI_BC_CHANNEL)
+        return fail(nullptr, IPPI_ERR_ARG, "the learned relaxation time is built for the channel scene");
     if (p->delta_kernel < 0 || p->delta_kernel > 1) return fail(nullptr, IPPI_ERR_ARG, "bad delta_kernel");
     if (!(p->tau0 > 0.5)) return fail(nullptr, IPPI_ERR_ARG, "tau0 must exceed 0.5");
     if (!(p->rho0 > 0)) return fail(nullptr, IPPI_ERR_ARG, "rho0 must be positive");
@@ -789,6 +845,7 @@ int ippi_destroy(ippi_lbm* h)
     if (h->st) cudaStreamSynchronize(h->st);
     drop_graphs(h);
     for (int b = 0; b < 2; b++) dfree(h->f[b]);
+    dfree(h->mlp_dev);
     dfree(h->ctr);
     if (h->ctr_h) cudaFreeHost(h->ctr_h);
     dfree(h->nflag);
@@ -924,6 +981,7 @@ int ippi_load_band_net(ippi_lbm* h, int type, const float* w, size_t n)
 int ippi_step(ippi_lbm* h, int nsteps, int t0)
 {
     if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (int rc = tau_ready(h)) return rc;
     if (nsteps < 0) return fail(h, IPPI_ERR_ARG, "negative step count");
     if (nsteps == 0) return IPPI_OK;
     CK(h, cudaSetDevice(h->p.device));
@@ -967,6 +1025,7 @@ int ippi_step(ippi_lbm* h, int nsteps, int t0)
 int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk, double* ms_band, double* ms_ib)
 {
     if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (int rc = tau_ready(h)) return rc;
     if (nsteps <= 0) return fail(h, IPPI_ERR_ARG, "nsteps must be positive");
     CK(h, cudaSetDevice(h->p.device));
     if (h->pending_init) {
@@ -1133,3 +1192,53 @@ int ippi_last_error(ippi_lbm* h, char* buf, size_t n)
 }
 
 }  // extern "C"
+
+int ippi_load_tau_mlp(ippi_lbm* h, const uint16_t* w_bf16, size_t n, const float* stats, size_t nstats)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (!w_bf16 || !stats || n != (size_t)IPPI_MLP_PARAMS || nstats != (size_t)IPPI_MLP_STATS)
+        return fail(h, IPPI_ERR_ARG, "tau network: %d BF16 weights and %d statistics expected", IPPI_MLP_PARAMS,
+                    IPPI_MLP_STATS);
+    std::vector<float> blob(IPPI_MLP_PARAMS + IPPI_MLP_STATS);
+    for (int i = 0; i < IPPI_MLP_PARAMS; i++) {
+        const uint32_t bits = (uint32_t)w_bf16[i] << 16;
+        std::memcpy(&blob[i], &bits, 4);
+        if (!std::isfinite(blob[i])) return fail(h, IPPI_ERR_ARG, "tau network weight %d is not finite", i);
+    }
+    for (int i = 0; i < IPPI_MLP_STATS; i++) blob[IPPI_MLP_PARAMS + i] = stats[i];
+    for (int i = 0; i < 6; i++)
+        if (!(stats[6 + i] > 0) || !(stats[12 + i] <= stats[18 + i]) || !std::isfinite(stats[i]))
+            return fail(h, IPPI_ERR_ARG, "tau network statistics of feature %d are invalid", i);
+    if (!(stats[24] > 0) || !std::isfinite(stats[24])) return fail(h, IPPI_ERR_ARG, "out_scale must be positive");
+    CK(h, cudaSetDevice(h->p.device));
+    CK(h, cudaStreamSynchronize(h->st));
+    if (!h->mlp_dev) CK(h, dalloc(&h->mlp_dev, blob.size() * sizeof(float)));
+    CK(h, cudaMemcpy(h->mlp_dev, blob.data(), blob.size() * sizeof(float), cudaMemcpyHostToDevice));
+    // the pointer is baked into the step graphs only through StepArgs, which
+    // were captured with the old (possibly null) pointer
+    drop_graphs(h);
+    h->dl_valid = false;
+    return IPPI_OK;
+}
+
+int ippi_filter_snapshot(ippi_lbm* h, int factor, double* out, size_t bytes)
+{
+    if (!h || !out) return fail(h, IPPI_ERR_ARG, "null argument");
+    const int nx = h->p.nx, ny = h->p.ny;
+    if (factor < 1 || nx % factor || ny % factor)
+        return fail(h, IPPI_ERR_ARG, "filter factor %d must divide %d and %d", factor, nx, ny);
+    const size_t m = (size_t)(nx / factor) * (ny / factor);
+    if (bytes != 6 * m * sizeof(double)) return fail(h, IPPI_ERR_ARG, "filtered snapshot needs %zu bytes", 6 * m * sizeof(double));
+    CK(h, cudaSetDevice(h->p.device));
+    if (int rc = materialize(h)) return rc;
+    double* d = nullptr;
+    CK(h, dalloc(&d, 6 * m * sizeof(double)));
+    const dim3 grid((nx / factor + 127) / 128, ny / factor);
+    filter_snapshot_kernel<<<grid, 128, 0, h->st>>>(h->dl, nx, ny, factor, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, 6 * m * sizeof(double), cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    dfree(d);
+    CK(h, e);
+    return IPPI_OK;
+}

@@ -26,7 +26,7 @@ static void launch_prio(void (*kernel)(KArgs...), unsigned grid, unsigned block,
     cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-template <int S, int CO, int SC>
+template <int S, int CO, int SC, bool LRN>
 static cudaError_t launch_tpl(const LaunchSet& L)
 {
     const bool side = L.nprep > 0 || L.band || L.ib;
@@ -52,13 +52,13 @@ static cudaError_t launch_tpl(const LaunchSet& L)
                     launch_prio(ib_markers<4>, gm, kIbThreads, L.side, L.side_prio, I, int(it == 0));
                 launch_prio(ib_spread, gn, kIbThreads, L.side, L.side_prio, I);
             }
-            launch_prio(ib_finish<S, CO>, (unsigned)I.nbody + gn, kIbThreads, L.side, L.side_prio, I);
+            launch_prio(ib_finish<S, CO, LRN>, (unsigned)I.nbody + gn, kIbThreads, L.side, L.side_prio, I);
         }
         if (L.events) cudaEventRecord(L.events[3], L.side);
         cudaEventRecord(L.join, L.side);
     }
     if (L.events) cudaEventRecord(L.events[0], L.stream);
-    step_kernel<S, CO, SC><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
+    step_kernel<S, CO, SC, LRN><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
     if (L.events) cudaEventRecord(L.events[1], L.stream);
     if (side) cudaStreamWaitEvent(L.stream, L.join, 0);
     return cudaGetLastError();
@@ -69,15 +69,23 @@ static cudaError_t launch_store(const LaunchSet& L)
 {
     if (L.scene == SC_REF) {
         switch (L.coll) {
-        case CO_MRT: return launch_tpl<S, CO_MRT, SC_REF>(L);
-        case CO_RR: return launch_tpl<S, CO_RR, SC_REF>(L);
-        default: return launch_tpl<S, CO_BGK, SC_REF>(L);
+        case CO_MRT: return launch_tpl<S, CO_MRT, SC_REF, false>(L);
+        case CO_RR: return launch_tpl<S, CO_RR, SC_REF, false>(L);
+        default: return launch_tpl<S, CO_BGK, SC_REF, false>(L);
+        }
+    }
+    // the learned relaxation time (les == 2) is built for the channel scene
+    if (L.step.les == 2) {
+        switch (L.coll) {
+        case CO_MRT: return launch_tpl<S, CO_MRT, SC_CHANNEL, true>(L);
+        case CO_RR: return launch_tpl<S, CO_RR, SC_CHANNEL, true>(L);
+        default: return launch_tpl<S, CO_BGK, SC_CHANNEL, true>(L);
         }
     }
     switch (L.coll) {
-    case CO_MRT: return launch_tpl<S, CO_MRT, SC_CHANNEL>(L);
-    case CO_RR: return launch_tpl<S, CO_RR, SC_CHANNEL>(L);
-    default: return launch_tpl<S, CO_BGK, SC_CHANNEL>(L);
+    case CO_MRT: return launch_tpl<S, CO_MRT, SC_CHANNEL, false>(L);
+    case CO_RR: return launch_tpl<S, CO_RR, SC_CHANNEL, false>(L);
+    default: return launch_tpl<S, CO_BGK, SC_CHANNEL, false>(L);
     }
 }
 

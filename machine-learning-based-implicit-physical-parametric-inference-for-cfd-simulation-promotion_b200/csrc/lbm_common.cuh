@@ -254,12 +254,101 @@ __device__ __forceinline__ void collide_node(C* f, C rho, C ux, C uy, C rb, C ta
     }
 }
 
+// ---------------------------------------------------------------------------
+// learned relaxation time: tau = tau0 + out_scale * softplus(MLP(features)),
+// MLP 6 -> 32 tanh -> 32 tanh -> 1 with weights rounded to BF16 (held here
+// as their exact FP32 values) and arithmetic in the compute type.
+// Features of a node (post-stream state, Pi_neq as for the Smagorinsky model):
+//   rho, |u|, Pi_neq_xx / |Pi|, Pi_neq_xy / |Pi|, Pi_neq_yy / |Pi|, |S|
+// with |Pi| = sqrt(Pxx^2 + 2 Pxy^2 + Pyy^2), S = -3/(2 rho tau0) Pi_neq,
+// |S| = sqrt(2 S:S).  Outside the training range [lo, hi] of any feature
+// the node falls back to the Smagorinsky tau.
+// Parameter block (floats): W1[32][6] b1[32] W2[32][32] b2[32] w3[32] b3,
+// then mean[6] std[6] lo[6] hi[6] out_scale.
+// ---------------------------------------------------------------------------
+constexpr int kMlpIn = 6, kMlpHid = 32;
+constexpr int kMlpW1 = 0, kMlpB1 = kMlpW1 + kMlpHid * kMlpIn, kMlpW2 = kMlpB1 + kMlpHid,
+              kMlpB2 = kMlpW2 + kMlpHid * kMlpHid, kMlpW3 = kMlpB2 + kMlpHid, kMlpB3 = kMlpW3 + kMlpHid;
+constexpr int kMlpParams = kMlpB3 + 1;  // 1313
+constexpr int kMlpStats = 4 * kMlpIn + 1;
+static_assert(kMlpParams == 1313, "MLP size");
+
+__device__ __forceinline__ double mlp_tanh(double v) { return tanh(v); }
+__device__ __forceinline__ float mlp_tanh(float v) { return tanhf(v); }
+// softplus(z) = max(z, 0) + log(1 + exp(-|z|))
+__device__ __forceinline__ double softplus(double z) { return fmax(z, 0.0) + log1p(exp(-fabs(z))); }
+__device__ __forceinline__ float softplus(float z) { return fmaxf(z, 0.f) + log1pf(expf(-fabsf(z))); }
+
 template <typename C>
-__device__ __forceinline__ C node_tau(const C* f, C rho, C ux, C uy, C rb, int les, C tau0, C cs)
+__device__ __forceinline__ void mlp_features(C pxx, C pxy, C pyy, C rho, C ux, C uy, C tau0, C* x)
 {
-    if (!les) return tau0;
+    const C c = C(-1.5) / (rho * tau0);
+    const C sxx = pxx * c, sxy = pxy * c, syy = pyy * c;
+    const C pn = sqrt(pxx * pxx + C(2) * pxy * pxy + pyy * pyy);
+    const C inv = pn > C(0) ? C(1) / pn : C(0);
+    x[0] = rho;
+    x[1] = sqrt(ux * ux + uy * uy);
+    x[2] = pxx * inv;
+    x[3] = pxy * inv;
+    x[4] = pyy * inv;
+    x[5] = sqrt(C(2) * (sxx * sxx + C(2) * sxy * sxy + syy * syy));
+}
+
+// network output softplus(z) for standardised inputs x
+template <typename C>
+__device__ __forceinline__ C mlp_forward(const float* __restrict__ w, const C* x)
+{
+    C h1[kMlpHid];
+#pragma unroll
+    for (int j = 0; j < kMlpHid; j++) {
+        C a = C(__ldg(w + kMlpB1 + j));
+#pragma unroll
+        for (int i = 0; i < kMlpIn; i++) a += C(__ldg(w + kMlpW1 + j * kMlpIn + i)) * x[i];
+        h1[j] = mlp_tanh(a);
+    }
+    C z = C(__ldg(w + kMlpB3));
+#pragma unroll 4
+    for (int j = 0; j < kMlpHid; j++) {
+        C a = C(__ldg(w + kMlpB2 + j));
+        const float4* row = reinterpret_cast<const float4*>(w + kMlpW2 + j * kMlpHid);
+#pragma unroll
+        for (int i = 0; i < kMlpHid / 4; i++) {
+            const float4 q = __ldg(row + i);
+            a += C(q.x) * h1[4 * i] + C(q.y) * h1[4 * i + 1] + C(q.z) * h1[4 * i + 2] +
+                 C(q.w) * h1[4 * i + 3];
+        }
+        z += C(__ldg(w + kMlpW3 + j)) * mlp_tanh(a);
+    }
+    return softplus(z);
+}
+
+template <typename C>
+__device__ __forceinline__ C learned_tau(C pxx, C pxy, C pyy, C rho, C ux, C uy, C tau0, C cs,
+                                         const float* __restrict__ w)
+{
+    const float* st = w + kMlpParams;
+    C x[kMlpIn];
+    mlp_features<C>(pxx, pxy, pyy, rho, ux, uy, tau0, x);
+    bool in = true;
+#pragma unroll
+    for (int i = 0; i < kMlpIn; i++) {
+        in = in && x[i] >= C(__ldg(st + 2 * kMlpIn + i)) && x[i] <= C(__ldg(st + 3 * kMlpIn + i));
+        x[i] = (x[i] - C(__ldg(st + i))) / C(__ldg(st + kMlpIn + i));
+    }
+    if (!in) return les_tau<C>(pxx, pxy, pyy, rho, tau0, cs);
+    return tau0 + C(__ldg(st + 4 * kMlpIn)) * mlp_forward<C>(w, x);
+}
+
+// relaxation time of a node's next collision: tau0, Smagorinsky, or (LRN)
+// the learned model with its Smagorinsky fallback
+template <typename C, bool LRN = false>
+__device__ __forceinline__ C node_tau(const C* f, C rho, C ux, C uy, C rb, int les, C tau0, C cs,
+                                      const float* mlp = nullptr)
+{
+    if (!LRN && !les) return tau0;
     C pxx, pxy, pyy;
     pi_neq<C>(f, rho, ux, uy, rb, pxx, pxy, pyy);
+    if (LRN) return learned_tau<C>(pxx, pxy, pyy, rho, ux, uy, tau0, cs, mlp);
     return les_tau<C>(pxx, pxy, pyy, rho, tau0, cs);
 }
 

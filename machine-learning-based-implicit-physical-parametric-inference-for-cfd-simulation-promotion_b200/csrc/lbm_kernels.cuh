@@ -55,6 +55,7 @@ struct StepArgs {
     int par;              // step parity: side-buffer half and ctr->t entry
     int fixed_t;          // step number for the MAT modes
     const double* init_m; // [3][ny][nx] initial rho, ux, uy (INIT modes)
+    const float* mlp;     // learned tau: parameters + feature statistics (LRN kernels)
     double* dl_f;         // MAT: fnew [9][ny][nx]
     double* dl_m;         // MAT: rho, ux, uy, boundary-net flag [4][ny][nx]
     double* dl_tau;       // MAT: tau of the next collision [ny][nx]
@@ -400,8 +401,10 @@ __device__ __forceinline__ void node_epilogue(const StepArgs& a, long long node,
 // ---------------------------------------------------------------------------
 // the fused stream + boundary + collide kernel (every node not deferred)
 // ---------------------------------------------------------------------------
-template <int S, int CO, int SC>
-__global__ void __launch_bounds__(kBlockX, 8) step_kernel(const StepArgs a)
+// (the learned-tau variant keeps the network's hidden layer in registers:
+// fewer resident blocks)
+template <int S, int CO, int SC, bool LRN>
+__global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step_kernel(const StepArgs a)
 {
     using C = typename Store<S>::C;
     const int x = blockIdx.x * kBlockX + threadIdx.x;
@@ -418,7 +421,8 @@ __global__ void __launch_bounds__(kBlockX, 8) step_kernel(const StepArgs a)
             node_state<S, SC>(a, x, y, f, rho, ux, uy);
             if (!deferred) {
                 node_epilogue<S>(a, node, t, f, rho, ux, uy);
-                const C tau = node_tau<C>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0), prm<C>(a.cs, a.f_cs));
+                const C tau = node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
+                                               prm<C>(a.cs, a.f_cs), a.mlp);
                 if (a.mode >= MODE_MAT) {
                     a.dl_tau[node] = double(tau);
                 } else {
@@ -714,8 +718,8 @@ static __global__ void __launch_bounds__(kIbThreads, 8) ib_spread(const IbArgs i
     ia.fy[n] += dfy;
 }
 
-template <int S, int CO>
-__global__ void __launch_bounds__(kIbThreads, 8) ib_finish(const IbArgs ia)
+template <int S, int CO, bool LRN>
+__global__ void __launch_bounds__(kIbThreads, LRN ? 4 : 8) ib_finish(const IbArgs ia)
 {
     using C = typename Store<S>::C;
     const StepArgs& a = ia.s;
@@ -761,7 +765,8 @@ __global__ void __launch_bounds__(kIbThreads, 8) ib_finish(const IbArgs ia)
     const C rho = C(ia.rho[n]);
     const C ux = C(ia.ucx[n]), uy = C(ia.ucy[n]);
     const C rbs = rbase<S>(a);
-    const C tau = node_tau<C>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0), prm<C>(a.cs, a.f_cs));
+    const C tau = node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
+                                   prm<C>(a.cs, a.f_cs), a.mlp);
     const int2 xy = ia.fn_xy[n];
     if (a.mode >= MODE_MAT) {
         a.dl_tau[(long long)xy.y * a.nx + xy.x] = double(tau);

@@ -1,0 +1,260 @@
+// tau_train.cu -- training and batch inference kernels of the learned
+// relaxation-time network (the MLP of lbm_common.cuh: 6 -> 32 tanh -> 32 tanh
+// -> softplus), FP32, deterministic.
+//
+//   mlp_grad_kernel   each warp takes 32 samples at a time: one thread per
+//                     sample runs the forward and backward pass and stages
+//                     its activations and deltas in shared memory; then lane
+//                     j accumulates row j of every weight gradient over the 32
+//                     samples (dW2[j][:] += d2[s][j] h1[s][:], ...).  Warp
+//                     sums are added in a fixed order into one partial per
+//                     block.
+//   mlp_reduce_kernel the block partials summed in block order: gradient of
+//                     the mean squared error and the loss
+//   mlp_adam_kernel   Adam update, one thread per parameter
+//   mlp_forward_kernel softplus outputs for a batch (evaluation)
+#include <cuda_runtime.h>
+
+#include "../../include/ippi_lbm.h"
+#include "lbm_common.cuh"
+
+namespace {
+
+using namespace ippi;
+
+constexpr int kThreads = 128;                  // 4 warps
+constexpr int kWarps = kThreads / 32;
+constexpr int kRow = kMlpHid + 1;               // padded row of a 32-vector
+constexpr int kXRow = kMlpIn + 1;
+// per warp: x[32][7], h1/h2/d2/d1 [32][33], dout[32]
+constexpr int kWarpFloats = 32 * kXRow + 4 * 32 * kRow + 32;
+constexpr int kPartial = kMlpParams + 1;        // gradient + loss
+constexpr size_t kGradSmem = (size_t)(kWarps * kWarpFloats + kMlpParams + 3) * sizeof(float);
+static_assert(kWarps * kWarpFloats >= kWarps * kPartial, "reduction buffer fits the staging area");
+
+__device__ __forceinline__ float sigmoidf(float z) { return 1.f / (1.f + expf(-z)); }
+
+__global__ void __launch_bounds__(kThreads) mlp_grad_kernel(const float* __restrict__ X,
+                                                             const float* __restrict__ Y, int n,
+                                                             const float* __restrict__ W,
+                                                             float* __restrict__ part)
+{
+    extern __shared__ float sm[];
+    float* ws = sm + kWarps * kWarpFloats;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int p = tid; p < kMlpParams; p += kThreads) ws[p] = W[p];
+    __syncthreads();
+    float* base = sm + warp * kWarpFloats;
+    float* xs = base;
+    float* h1s = xs + 32 * kXRow;
+    float* h2s = h1s + 32 * kRow;
+    float* d2s = h2s + 32 * kRow;
+    float* d1s = d2s + 32 * kRow;
+    float* dos = d1s + 32 * kRow;
+
+    const float inv_n = 1.f / (float)n;
+    float gW2[kMlpHid], gW1[kMlpIn];
+#pragma unroll
+    for (int i = 0; i < kMlpHid; i++) gW2[i] = 0.f;
+#pragma unroll
+    for (int i = 0; i < kMlpIn; i++) gW1[i] = 0.f;
+    float gb2 = 0.f, gb1 = 0.f, gw3 = 0.f, gb3 = 0.f, loss = 0.f;
+
+    const int nchunks = (n + 31) / 32;
+    for (int c = blockIdx.x * kWarps + warp; c < nchunks; c += gridDim.x * kWarps) {
+        // ---- phase A: one sample per lane ----------------------------------
+        const int s = c * 32 + lane;
+        float x[kMlpIn], h1[kMlpHid], h2[kMlpHid];
+        float dout = 0.f;
+        if (s < n) {
+#pragma unroll
+            for (int i = 0; i < kMlpIn; i++) x[i] = X[(size_t)s * kMlpIn + i];
+        } else {
+#pragma unroll
+            for (int i = 0; i < kMlpIn; i++) x[i] = 0.f;
+        }
+#pragma unroll
+        for (int j = 0; j < kMlpHid; j++) {
+            float a = ws[kMlpB1 + j];
+#pragma unroll
+            for (int i = 0; i < kMlpIn; i++) a += ws[kMlpW1 + j * kMlpIn + i] * x[i];
+            h1[j] = tanhf(a);
+        }
+        float z = ws[kMlpB3];
+#pragma unroll
+        for (int j = 0; j < kMlpHid; j++) {
+            float a = ws[kMlpB2 + j];
+#pragma unroll
+            for (int i = 0; i < kMlpHid; i++) a += ws[kMlpW2 + j * kMlpHid + i] * h1[i];
+            h2[j] = tanhf(a);
+            z += ws[kMlpW3 + j] * h2[j];
+        }
+        if (s < n) {
+            const float r = softplus(z) - Y[s];
+            loss += r * r;
+            dout = 2.f * r * sigmoidf(z) * inv_n;
+        }
+        // deltas: d2 = dout w3 (1 - h2^2); d1 = (W2^T d2) (1 - h1^2)
+        float d2[kMlpHid];
+#pragma unroll
+        for (int j = 0; j < kMlpHid; j++) d2[j] = dout * ws[kMlpW3 + j] * (1.f - h2[j] * h2[j]);
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < kMlpIn; i++) xs[lane * kXRow + i] = x[i];
+#pragma unroll
+        for (int i = 0; i < kMlpHid; i++) {
+            float g = 0.f;
+#pragma unroll
+            for (int j = 0; j < kMlpHid; j++) g += ws[kMlpW2 + j * kMlpHid + i] * d2[j];
+            d1s[lane * kRow + i] = g * (1.f - h1[i] * h1[i]);
+            h1s[lane * kRow + i] = h1[i];
+            h2s[lane * kRow + i] = h2[i];
+            d2s[lane * kRow + i] = d2[i];
+        }
+        dos[lane] = dout;
+        __syncwarp();
+        // ---- phase B: lane j accumulates row j over the 32 samples --------
+        const int j = lane;
+        for (int q = 0; q < 32; q++) {
+            const float dj2 = d2s[q * kRow + j], dj1 = d1s[q * kRow + j], dq = dos[q];
+#pragma unroll
+            for (int i = 0; i < kMlpHid; i++) gW2[i] += dj2 * h1s[q * kRow + i];
+            gb2 += dj2;
+#pragma unroll
+            for (int i = 0; i < kMlpIn; i++) gW1[i] += dj1 * xs[q * kXRow + i];
+            gb1 += dj1;
+            gw3 += dq * h2s[q * kRow + j];
+            gb3 += dq;
+        }
+        __syncwarp();
+    }
+    // ---- warp partials -> block partial (fixed order) -----------------------
+    // the staging area is reused: warp w's gradient at sm[w * kPartial ...]
+    float lsum = loss;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+    __syncthreads();
+    float* g = sm + warp * kPartial;
+    {
+        const int j = lane;
+#pragma unroll
+        for (int i = 0; i < kMlpHid; i++) g[kMlpW2 + j * kMlpHid + i] = gW2[i];
+        g[kMlpB2 + j] = gb2;
+#pragma unroll
+        for (int i = 0; i < kMlpIn; i++) g[kMlpW1 + j * kMlpIn + i] = gW1[i];
+        g[kMlpB1 + j] = gb1;
+        g[kMlpW3 + j] = gw3;
+        if (j == 0) {
+            g[kMlpB3] = gb3;
+            g[kMlpParams] = lsum * inv_n;
+        }
+    }
+    __syncthreads();
+    for (int p = tid; p < kPartial; p += kThreads) {
+        float v = 0.f;
+        for (int w = 0; w < kWarps; w++) v += sm[w * kPartial + p];
+        part[(size_t)blockIdx.x * kPartial + p] = v;
+    }
+}
+
+__global__ void mlp_reduce_kernel(const float* __restrict__ part, int nblocks, float* __restrict__ grad,
+                                  float* __restrict__ loss)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kPartial) return;
+    float v = 0.f;
+    for (int b = 0; b < nblocks; b++) v += part[(size_t)b * kPartial + p];
+    if (p < kMlpParams) grad[p] = v;
+    else if (loss) *loss = v;
+}
+
+__global__ void mlp_adam_kernel(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                                float* __restrict__ v, float lr, float b1, float b2, float eps, float c1,
+                                float c2)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kMlpParams) return;
+    const float gp = g[p];
+    const float mp = b1 * m[p] + (1.f - b1) * gp;
+    const float vp = b2 * v[p] + (1.f - b2) * gp * gp;
+    m[p] = mp;
+    v[p] = vp;
+    w[p] -= lr * (mp / c1) / (sqrtf(vp / c2) + eps);
+}
+
+__global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restrict__ X, int n,
+                                                          const float* __restrict__ W,
+                                                          float* __restrict__ out)
+{
+    __shared__ __align__(16) float ws[kMlpParams + 3];
+    for (int p = threadIdx.x; p < kMlpParams; p += blockDim.x) ws[p] = W[p];
+    __syncthreads();
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    float x[kMlpIn];
+#pragma unroll
+    for (int i = 0; i < kMlpIn; i++) x[i] = X[(size_t)s * kMlpIn + i];
+    float h1[kMlpHid];
+#pragma unroll
+    for (int j = 0; j < kMlpHid; j++) {
+        float a = ws[kMlpB1 + j];
+#pragma unroll
+        for (int i = 0; i < kMlpIn; i++) a += ws[kMlpW1 + j * kMlpIn + i] * x[i];
+        h1[j] = tanhf(a);
+    }
+    float z = ws[kMlpB3];
+#pragma unroll 4
+    for (int j = 0; j < kMlpHid; j++) {
+        float a = ws[kMlpB2 + j];
+#pragma unroll
+        for (int i = 0; i < kMlpHid; i++) a += ws[kMlpW2 + j * kMlpHid + i] * h1[i];
+        z += ws[kMlpW3 + j] * tanhf(a);
+    }
+    out[s] = softplus(z);
+}
+
+bool g_grad_attr = false;
+
+}  // namespace
+
+extern "C" {
+
+int ippi_mlp_param_count(void) { return kMlpParams; }
+
+size_t ippi_mlp_scratch_floats(void) { return (size_t)IPPI_MLP_GRAD_BLOCKS * kPartial; }
+
+int ippi_mlp_grad(const float* x, const float* y, int n, const float* w, float* grad, float* loss,
+                  float* scratch, void* stream)
+{
+    if (!x || !y || !w || !grad || !scratch || n <= 0) return IPPI_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!g_grad_attr) {
+        if (cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kGradSmem) != cudaSuccess)
+            return IPPI_ERR_CUDA;
+        g_grad_attr = true;
+    }
+    mlp_grad_kernel<<<IPPI_MLP_GRAD_BLOCKS, kThreads, kGradSmem, st>>>(x, y, n, w, scratch);
+    mlp_reduce_kernel<<<(kPartial + 255) / 256, 256, 0, st>>>(scratch, IPPI_MLP_GRAD_BLOCKS, grad, loss);
+    return cudaGetLastError() == cudaSuccess ? IPPI_OK : IPPI_ERR_CUDA;
+}
+
+int ippi_mlp_adam(float* w, const float* grad, float* m, float* v, int step, float lr, float beta1,
+                  float beta2, float eps, void* stream)
+{
+    if (!w || !grad || !m || !v || step < 1 || !(lr > 0)) return IPPI_ERR_ARG;
+    const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+    mlp_adam_kernel<<<(kMlpParams + 255) / 256, 256, 0, (cudaStream_t)stream>>>(w, grad, m, v, lr, beta1,
+                                                                               beta2, eps, c1, c2);
+    return cudaGetLastError() == cudaSuccess ? IPPI_OK : IPPI_ERR_CUDA;
+}
+
+int ippi_mlp_forward(const float* x, int n, const float* w, float* out, void* stream)
+{
+    if (!x || !w || !out || n < 0) return IPPI_ERR_ARG;
+    if (n == 0) return IPPI_OK;
+    mlp_forward_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(x, n, w, out);
+    return cudaGetLastError() == cudaSuccess ? IPPI_OK : IPPI_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -16,7 +16,9 @@ IPPI_OK, IPPI_ERR_ARG, IPPI_ERR_CUDA, IPPI_ERR_DIVERGED, IPPI_ERR_STATE, IPPI_ER
 BGK, MRT, RR = 0, 1, 2
 F64, F32, F16, BF16 = 0, 1, 2, 3
 BC_REF_NEE, BC_CHANNEL = 0, 1
-LES_NONE, LES_SMAGORINSKY = 0, 1
+LES_NONE, LES_SMAGORINSKY, LES_LEARNED = 0, 1, 2
+MLP_PARAMS, MLP_STATS, MLP_GRAD_BLOCKS = 1313, 25, 296
+ABI_VERSION = 2
 DELTA_BILINEAR, DELTA_PESKIN4 = 0, 1
 (FIELD_F, FIELD_RHO, FIELD_UX, FIELD_UY, FIELD_TAU, FIELD_AVG_U, FIELD_AVG_V, FIELD_AVG_RHO,
  FIELD_FLAGS, FIELD_NNFLAG) = range(10)
@@ -24,7 +26,9 @@ DELTA_BILINEAR, DELTA_PESKIN4 = 0, 1
 EXPORTS = ("ippi_abi_version", "ippi_params_default", "ippi_create", "ippi_destroy",
            "ippi_init_macros", "ippi_set_markers", "ippi_load_band_net", "ippi_step",
            "ippi_download", "ippi_forces", "ippi_force_history", "ippi_get_stream",
-           "ippi_profile_steps", "ippi_last_error")
+           "ippi_profile_steps", "ippi_last_error", "ippi_mass_noalloc", "ippi_load_tau_mlp",
+           "ippi_filter_snapshot", "ippi_mlp_param_count", "ippi_mlp_scratch_floats", "ippi_mlp_grad",
+           "ippi_mlp_adam", "ippi_mlp_forward")
 
 
 class Params(C.Structure):
@@ -59,6 +63,9 @@ def lib() -> C.CDLL:
             raise ImportError(f"{LIB_PATH} is missing; run build.py (no CPU fallback exists)")
         L = C.CDLL(LIB_PATH)
         L.ippi_abi_version.restype = C.c_int
+        if L.ippi_abi_version() != ABI_VERSION:
+            raise ImportError(f"{LIB_PATH} has ABI {L.ippi_abi_version()}, expected {ABI_VERSION}; "
+                              "rebuild it with build.py")
         L.ippi_params_default.argtypes = [C.POINTER(Params), C.c_int, C.c_int]
         L.ippi_params_default.restype = None
         L.ippi_create.argtypes = [C.POINTER(Params), C.POINTER(C.c_void_p)]
@@ -73,6 +80,16 @@ def lib() -> C.CDLL:
         L.ippi_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
         L.ippi_profile_steps.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp, _dp]
         L.ippi_last_error.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
+        L.ippi_mass_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        L.ippi_load_tau_mlp.argtypes = [C.c_void_p, C.POINTER(C.c_uint16), C.c_size_t,
+                                        C.POINTER(C.c_float), C.c_size_t]
+        L.ippi_filter_snapshot.argtypes = [C.c_void_p, C.c_int, _dp, C.c_size_t]
+        L.ippi_mlp_scratch_floats.restype = C.c_size_t
+        _vp = C.c_void_p
+        L.ippi_mlp_grad.argtypes = [_vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp]
+        L.ippi_mlp_adam.argtypes = [_vp, _vp, _vp, _vp, C.c_int, C.c_float, C.c_float, C.c_float,
+                                    C.c_float, _vp]
+        L.ippi_mlp_forward.argtypes = [_vp, C.c_int, _vp, _vp, _vp]
         _lib = L
     return _lib
 

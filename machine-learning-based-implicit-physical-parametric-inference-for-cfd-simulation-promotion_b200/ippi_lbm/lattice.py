@@ -117,6 +117,21 @@ class Lattice:
             L.check(n, self._h)
         return out[:n, : nb.value]
 
+    def load_tau_mlp(self, w_bf16, stats):
+        """Learned relaxation time: w_bf16[1313] BF16 bit patterns (uint16),
+        stats[25] (mean, std, lo, hi of the 6 features, out_scale)."""
+        w = np.ascontiguousarray(w_bf16, dtype=np.uint16)
+        st = np.ascontiguousarray(stats, dtype=np.float32)
+        L.check(L.lib().ippi_load_tau_mlp(self._h, w.ctypes.data_as(C.POINTER(C.c_uint16)), w.size,
+                                          st.ctypes.data_as(C.POINTER(C.c_float)), st.size), self._h)
+
+    def filter_snapshot(self, factor):
+        """Box-filtered state [6][ny/f][nx/f]: rho, ux, uy (density-weighted),
+        effective stress Sxx, Sxy, Syy (include/ippi_lbm.h)."""
+        out = np.zeros((6, self.ny // factor, self.nx // factor))
+        L.check(L.lib().ippi_filter_snapshot(self._h, factor, _p(out), out.nbytes), self._h)
+        return out
+
     def stream(self) -> int:
         s = C.c_void_p()
         L.check(L.lib().ippi_get_stream(self._h, C.byref(s)), self._h)

@@ -1,0 +1,251 @@
+"""Learned relaxation time: training data made by the solver itself, training
+on the GPU with the library's own kernels (ippi_mlp_grad / ippi_mlp_adam),
+and the trained network fused into the collision (IPPI_LES_LEARNED).
+
+Data.  A fine lattice runs the cylinder flow (MRT + Smagorinsky).  Snapshots
+of its state are box-filtered by `factor` on the GPU (ippi_filter_snapshot):
+filtered density and velocity and the effective stress Sigma that a coarse
+lattice would have to carry (filtered viscous + Smagorinsky stress minus the
+subgrid momentum flux).  On the coarse grid the resolved strain rate S_bar
+comes from central differences of the filtered velocity; the eddy viscosity
+that best carries Sigma is the least-squares fit
+    nu = (Sigma : S_bar) / (2 rho_bar S_bar : S_bar),
+and the target relaxation time tau = 3 nu + 1/2 (coarse lattice units: the
+velocity scale is shared, lengths and times grow by `factor`), clamped below
+at the coarse tau0.  The network learns the offset tau - tau0.
+
+Features are the ones the collision sees at run time (lbm_common.cuh
+mlp_features): rho, |u|, the direction of Pi_neq (which is that of -S) and
+|S| as estimated from Pi_neq with tau0 -- at a node relaxed with tau that
+estimate is (tau / tau0) |S_bar|, which is what the training set holds.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+
+from . import _lib as L
+
+NIN, NHID = 6, 32
+NPARAM = L.MLP_PARAMS
+FEATURES = ("rho", "|u|", "Pxx/|P|", "Pxy/|P|", "Pyy/|P|", "|S|")
+
+
+# ---------------------------------------------------------------------------
+# parameters
+# ---------------------------------------------------------------------------
+def xavier(seed=0):
+    """Xavier-uniform weights (limit sqrt(6 / (fan_in + fan_out))), zero
+    biases; layout W1[32][6] b1[32] W2[32][32] b2[32] w3[32] b3."""
+    rng = np.random.default_rng(seed)
+    w = np.zeros(NPARAM)
+    for lo, fi, fo in ((0, NIN, NHID), (224, NHID, NHID), (1280, NHID, 1)):
+        lim = math.sqrt(6.0 / (fi + fo))
+        w[lo:lo + fi * fo] = rng.uniform(-lim, lim, fi * fo)
+    return w
+
+
+def bf16_bits(w):
+    """Round FP32 values to BF16 (nearest, ties to even): the bit patterns
+    (uint16) and their exact FP32 values."""
+    f = np.ascontiguousarray(w, dtype=np.float32)
+    u = f.view(np.uint32).astype(np.uint64)
+    rounded = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+    bits = rounded.astype(np.uint16)
+    vals = (bits.astype(np.uint32) << 16).view(np.float32)
+    return bits, vals
+
+
+class TauNet:
+    """Parameters (FP32 master copy) + feature statistics of a trained net."""
+
+    def __init__(self, w, mean, std, lo, hi, out_scale):
+        self.w = np.asarray(w, dtype=np.float32)
+        self.mean, self.std = np.asarray(mean, np.float32), np.asarray(std, np.float32)
+        self.lo, self.hi = np.asarray(lo, np.float32), np.asarray(hi, np.float32)
+        self.out_scale = float(out_scale)
+
+    def stats(self):
+        return np.concatenate([self.mean, self.std, self.lo, self.hi,
+                               [self.out_scale]]).astype(np.float32)
+
+    def export(self):
+        """(BF16 bit patterns, stats) for Lattice.load_tau_mlp."""
+        bits, _ = bf16_bits(self.w)
+        return bits, self.stats()
+
+    def standardise(self, x):
+        return ((x - self.mean) / self.std).astype(np.float32)
+
+    def save(self, path):
+        np.savez(path, w=self.w, mean=self.mean, std=self.std, lo=self.lo, hi=self.hi,
+                 out_scale=self.out_scale)
+
+    @classmethod
+    def load(cls, path):
+        d = np.load(path)
+        return cls(d["w"], d["mean"], d["std"], d["lo"], d["hi"], float(d["out_scale"]))
+
+
+# ---------------------------------------------------------------------------
+# data
+# ---------------------------------------------------------------------------
+def strain(ux, uy):
+    """Resolved strain rate of a [ny][nx] field by central differences."""
+    dudy, dudx = np.gradient(ux)
+    dvdy, dvdx = np.gradient(uy)
+    return dudx, 0.5 * (dudy + dvdx), dvdy
+
+
+def samples_from_snapshot(snap, tau0, mask, min_strain=1e-7):
+    """Features and target offsets of the masked cells of one filtered
+    snapshot [6][ny][nx] (rho, ux, uy, Sxx, Sxy, Syy)."""
+    rho, ux, uy, sgx, sgy_xy, sgy = snap
+    sxx, sxy, syy = strain(ux, uy)
+    ss = sxx * sxx + 2 * sxy * sxy + syy * syy
+    keep = mask & (np.sqrt(2 * ss) > min_strain)
+    nu = (sgx * sxx + 2 * sgy_xy * sxy + sgy * syy) / (2 * rho * np.where(ss > 0, ss, 1.0))
+    tau_t = np.maximum(3 * nu + 0.5, tau0)
+    fn = np.sqrt(ss)  # |S|_F with the off-diagonal counted twice
+    inv = 1.0 / np.where(fn > 0, fn, 1.0)
+    smag = (tau_t / tau0) * np.sqrt(2 * ss)
+    x = np.stack([rho, np.sqrt(ux * ux + uy * uy), -sxx * inv, -sxy * inv, -syy * inv, smag], -1)
+    return x[keep], (tau_t - tau0)[keep]
+
+
+def cylinder_mask(nx, ny, cx, cy, d, margin=3):
+    """Cells away from the lattice edges and outside the cylinder's IB band."""
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    r = np.hypot(xx + 0.5 - cx, yy + 0.5 - cy)
+    m = (xx >= margin) & (xx < nx - margin) & (yy >= margin) & (yy < ny - margin)
+    return m & (r > 0.5 * d + margin)
+
+
+# ---------------------------------------------------------------------------
+# training on the GPU (the library's kernels; torch only holds the buffers)
+# ---------------------------------------------------------------------------
+def train(x_raw, y, epochs=40, batch=8192, lr=3e-3, seed=0, device=0, clip_pct=99.5,
+          log=None):
+    """Fit softplus(MLP((x - mean) / std)) * out_scale to y.  Returns
+    (TauNet, per-epoch mean loss)."""
+    import torch
+
+    x_raw = np.asarray(x_raw, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    y = np.minimum(y, np.percentile(y, clip_pct))
+    mean, std = x_raw.mean(0), x_raw.std(0)
+    std = np.where(std > 0, std, 1.0)
+    lo, hi = x_raw.min(0), x_raw.max(0)
+    out_scale = max(float(np.mean(y)), 1e-7)
+    net = TauNet(xavier(seed), mean, std, lo, hi, out_scale)
+    xs = net.standardise(x_raw)
+    ys = (y / out_scale).astype(np.float32)
+    n = xs.shape[0]
+    dev = torch.device("cuda", device)
+    lib = L.lib()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    w = torch.from_numpy(net.w.copy()).to(dev)
+    m = torch.zeros_like(w)
+    v = torch.zeros_like(w)
+    g = torch.zeros_like(w)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    scratch = torch.zeros(int(lib.ippi_mlp_scratch_floats()), dtype=torch.float32, device=dev)
+    xb = torch.empty((batch, NIN), dtype=torch.float32, device=dev)
+    yb = torch.empty(batch, dtype=torch.float32, device=dev)
+    rng = np.random.default_rng(seed + 1)
+    hist = []
+    step = 0
+    for ep in range(epochs):
+        perm = rng.permutation(n)
+        xp = torch.from_numpy(xs[perm]).pin_memory()
+        yp = torch.from_numpy(ys[perm]).pin_memory()
+        tot, cnt = 0.0, 0
+        for b0 in range(0, n - batch + 1, batch):
+            xb.copy_(xp[b0:b0 + batch], non_blocking=True)
+            yb.copy_(yp[b0:b0 + batch], non_blocking=True)
+            step += 1
+            L.check(lib.ippi_mlp_grad(xb.data_ptr(), yb.data_ptr(), batch, w.data_ptr(), g.data_ptr(),
+                                      loss.data_ptr(), scratch.data_ptr(), stream))
+            L.check(lib.ippi_mlp_adam(w.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(), step,
+                                      lr, 0.9, 0.999, 1e-8, stream))
+            tot += float(loss.item()) if (b0 // batch) % 16 == 0 else 0.0
+            cnt += 1 if (b0 // batch) % 16 == 0 else 0
+        hist.append(tot / max(cnt, 1))
+        if log:
+            log(f"epoch {ep}: loss {hist[-1]:.4g}")
+    net.w = w.cpu().numpy()
+    return net, hist
+
+
+def predict(net, x_raw, device=0, bf16=True):
+    """tau offsets (out_scale * softplus) of raw features through the
+    library's batch kernel (BF16-rounded weights when bf16)."""
+    import torch
+
+    dev = torch.device("cuda", device)
+    w = bf16_bits(net.w)[1] if bf16 else net.w
+    wd = torch.from_numpy(np.ascontiguousarray(w, dtype=np.float32)).to(dev)
+    xd = torch.from_numpy(net.standardise(np.asarray(x_raw))).to(dev)
+    out = torch.empty(xd.shape[0], dtype=torch.float32, device=dev)
+    L.check(L.lib().ippi_mlp_forward(xd.data_ptr(), xd.shape[0], wd.data_ptr(), out.data_ptr(),
+                                     torch.cuda.current_stream(dev).cuda_stream))
+    return out.cpu().numpy().astype(np.float64) * net.out_scale
+
+
+# ---------------------------------------------------------------------------
+# runs
+# ---------------------------------------------------------------------------
+def run_cylinder(sc, steps, avg_from, net=None, snapshot=None, device=0, chunk=2000):
+    """Run a cylinder scene (scenes.cylinder_channel dict) for `steps` steps;
+    returns mean Cd / Cl over steps >= avg_from, the Strouhal number of Cl in
+    that window, the device wall time of the stepping, and the snapshots
+    taken by snapshot = (factor, first_step, stride, count)."""
+    from .lattice import Lattice
+
+    params = dict(sc["params"])
+    if net is not None:
+        params["les_model"] = L.LES_LEARNED
+    lat = Lattice(sc["nx"], sc["ny"], device=device, **params)
+    lat.init_macros(*sc["init"])
+    lat.set_markers(sc["markers"], ds=sc["ds"])
+    if net is not None:
+        lat.load_tau_mlp(*net.export())
+    forces = np.zeros((steps, 2))
+    snaps = []
+    marks = []
+    if snapshot is not None:
+        factor, first, stride, count = snapshot
+        marks = [first + i * stride for i in range(count) if first + i * stride <= steps]
+    t = 1
+    wall = 0.0
+    while t <= steps:
+        end = min(t + chunk - 1, steps)
+        pending = [m for m in marks if m >= t]
+        if pending:
+            end = min(end, pending[0])
+        t0 = time.perf_counter()
+        lat.step(end - t + 1, t)
+        wall += time.perf_counter() - t0
+        forces[t - 1:end] = lat.force_history(end - t + 1)[:, 0, :]
+        if end in marks:
+            snaps.append(lat.filter_snapshot(snapshot[0]))
+        t = end + 1
+    lat.close()
+    q = 0.5 * sc["u_ref"] ** 2 * sc["d"]
+    cd, cl = forces[:, 0] / q, forces[:, 1] / q
+    win = slice(avg_from - 1, steps)
+    return dict(cd=float(cd[win].mean()), cl=float(cl[win].mean()),
+                st=strouhal(cl[win], sc["d"], sc["u_ref"]), wall_s=wall,
+                cd_series=cd, cl_series=cl, snapshots=snaps)
+
+
+def strouhal(cl, d, u):
+    """St = f D / U from the dominant frequency of the lift signal."""
+    c = np.asarray(cl) - np.mean(cl)
+    if c.size < 16 or not np.any(c):
+        return float("nan")
+    spec = np.abs(np.fft.rfft(c * np.hanning(c.size)))
+    k = int(np.argmax(spec[1:]) + 1)
+    return float(k / c.size * d / u)

@@ -50,6 +50,8 @@ struct orc {
     double* body_force;         /* [2*nbody] */
     double mass;
     double mrt_tm[9][9], mrt_tminv[9][9];
+    double mlp[1313 + 25];      /* learned tau network (les_model 2) */
+    int mlp_loaded;
 };
 
 #define ID(s, i, j) ((size_t)(i) * (size_t)(s)->NY + (size_t)(j))
@@ -142,6 +144,64 @@ double orc_les_tau(const double* fnew, double rho, double ux, double uy,
     double Q = sqrt(2.0 * S2);
     double g1 = tau0 * tau0 + 18.0 * cs * cs * Q / (rhoTemp);
     return (sqrt(g1) + tau0) / 2.0;
+}
+
+/* Learned relaxation time (no reference code).  Features from the node's
+ * post-stream state: rho, |u|, the direction Pi/|Pi| of
+ * Pi = sum_k e e (fnew - feq) (|Pi| = sqrt(Pxx^2 + 2 Pxy^2 + Pyy^2)) and
+ * |S| = sqrt(2 S:S) with S = -3/(2 rho tau0) Pi, as in orc_les_tau.  Outside
+ * the training range of any feature the Smagorinsky tau is used. */
+double orc_learned_tau(const double* fnew, double rho, double ux, double uy,
+                       double tau0, double cs, const double* p)
+{
+    const double* W1 = p;
+    const double* b1 = p + 192;
+    const double* W2 = p + 224;
+    const double* b2 = p + 1248;
+    const double* w3 = p + 1280;
+    const double b3 = p[1312];
+    const double* st = p + 1313;
+    double feq[9];
+    compute_feq(rho, ux, uy, feq);
+    double pxx = 0.0, pxy = 0.0, pyy = 0.0;
+    for (int k = 0; k < 9; k++) {
+        pxx += E[k][0] * E[k][0] * (fnew[k] - feq[k]);
+        pxy += E[k][0] * E[k][1] * (fnew[k] - feq[k]);
+        pyy += E[k][1] * E[k][1] * (fnew[k] - feq[k]);
+    }
+    double c = -1.5 / (rho * tau0);
+    double sxx = pxx * c, sxy = pxy * c, syy = pyy * c;
+    double pn = sqrt(pxx * pxx + 2.0 * pxy * pxy + pyy * pyy);
+    double inv = pn > 0 ? 1.0 / pn : 0.0;
+    double x[6] = {rho, sqrt(ux * ux + uy * uy), pxx * inv, pxy * inv, pyy * inv,
+                   sqrt(2.0 * (sxx * sxx + 2.0 * sxy * sxy + syy * syy))};
+    for (int i = 0; i < 6; i++) {
+        if (!(x[i] >= st[12 + i] && x[i] <= st[18 + i])) return orc_les_tau(fnew, rho, ux, uy, tau0, cs);
+        x[i] = (x[i] - st[i]) / st[6 + i];
+    }
+    double h1[32];
+    for (int j = 0; j < 32; j++) {
+        double a = b1[j];
+        for (int i = 0; i < 6; i++) a += W1[j * 6 + i] * x[i];
+        h1[j] = tanh(a);
+    }
+    double z = b3;
+    for (int j = 0; j < 32; j++) {
+        double a = b2[j];
+        for (int i = 0; i < 32; i++) a += W2[j * 32 + i] * h1[i];
+        z += w3[j] * tanh(a);
+    }
+    double sp = (z > 0 ? z : 0.0) + log1p(exp(-fabs(z)));
+    return tau0 + st[24] * sp;
+}
+
+int orc_load_tau_mlp(orc* s, const float* w, size_t n, const float* stats, size_t nstats)
+{
+    if (!s || !w || !stats || n != 1313 || nstats != 25) return -1;
+    for (size_t i = 0; i < n; i++) s->mlp[i] = w[i];
+    for (size_t i = 0; i < nstats; i++) s->mlp[1313 + i] = stats[i];
+    s->mlp_loaded = 1;
+    return 0;
 }
 
 /* D2Q9 MRT transformation matrix in the reference velocity order, built from
@@ -679,7 +739,9 @@ static int collide_all(orc* s)
             double fn[9], fc[9];
             for (int k = 0; k < 9; k++) fn[k] = FN(s, k, i, j);
             int use_les = s->p.les_model == 1 && !(coll == COLL_BGK && s->nnflag[id]);
-            if (use_les)
+            if (s->p.les_model == 2)
+                s->tau[id] = orc_learned_tau(fn, r, s->ux[id], s->uy[id], s->p.tau0, s->p.cs, s->mlp);
+            else if (use_les)
                 s->tau[id] = orc_les_tau(fn, r, s->ux[id], s->uy[id], s->p.tau0, s->p.cs);
             else if (!(coll == COLL_BGK && s->nnflag[id]))
                 s->tau[id] = s->p.tau0;
@@ -860,6 +922,7 @@ static void update_mass(orc* s)
 int orc_step(orc* s, int nsteps, int t0)
 {
     int status = 0;
+    if (s->p.les_model == 2 && !s->mlp_loaded) return -1;
     for (int t = t0; t < t0 + nsteps; t++) {
         ib_substep(s);
         if (s->p.collision == COLL_BGK) nn_band(s);
@@ -910,6 +973,8 @@ static void next_tau(orc* s, double* tau_out, unsigned char* flag_out)
             int nnf = (s->p.collision == COLL_BGK) && s->nnflag[id];
             if (nnf)
                 t = s->tau[id];
+            else if (s->p.les_model == 2)
+                t = orc_learned_tau(fn, s->rho[id], s->ux[id], s->uy[id], s->p.tau0, s->p.cs, s->mlp);
             else if (s->p.les_model == 1)
                 t = orc_les_tau(fn, s->rho[id], s->ux[id], s->uy[id], s->p.tau0, s->p.cs);
             else

@@ -73,6 +73,11 @@ def lib() -> C.CDLL:
                                        C.c_double, _dp]
         L.orc_les_tau.restype = C.c_double
         L.orc_les_tau.argtypes = [_dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.orc_load_tau_mlp.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_size_t,
+                                       C.POINTER(C.c_float), C.c_size_t]
+        L.orc_learned_tau.argtypes = [_dp, C.c_double, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, _dp]
+        L.orc_learned_tau.restype = C.c_double
         _lib = L
     return _lib
 
@@ -124,6 +129,14 @@ class Oracle:
         rc = lib().orc_load_band_net(self._h, t, _ptr(w, C.c_float), w.size)
         if rc != 0:
             raise ValueError("bad net")
+
+    def load_tau_mlp(self, w, stats):
+        """Learned-tau network: w[1313] (FP32 values of the BF16 weights),
+        stats[25]."""
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        st = np.ascontiguousarray(stats, dtype=np.float32)
+        if lib().orc_load_tau_mlp(self._h, _ptr(w, C.c_float), w.size, _ptr(st, C.c_float), st.size):
+            raise ValueError("bad tau network")
 
     def step(self, n, t0=1):
         return lib().orc_step(self._h, n, t0)
