@@ -336,6 +336,43 @@ def run_ncu_case(a):
     print(json.dumps({"ncu_case": WORKLOAD, "steps": a.steps}))
 
 
+def run_learned(a):
+    """The learned-tau comparison: a fine 4096 x 1024 plain-Smagorinsky run
+    (the Cd reference and the data source), training on its filtered
+    snapshots, then the 1024 x 256 lattice with plain Smagorinsky and with the
+    learned tau over the same physical time.  value = wall time of the fine
+    run / wall time of the coarse learned run (same GPU); the Cd errors say
+    whether the coarse learned run reached the fine run's answer."""
+    import torch
+
+    from ippi_lbm import learned_tau as lt
+
+    rank, local, world = env_rank()
+    torch.cuda.set_device(local)
+    r = lt.experiment(fine_steps=a.learned_steps, avg_steps=a.learned_steps * 2 // 5, device=local)
+    r.pop("net")
+    if rank != 0:
+        return
+    line = {
+        "metric": "learned_tau_time_to_solution", "value": round(r["speedup_vs_fine"], 3),
+        "unit": "x (fine plain wall / coarse learned wall)", "higher_is_better": True,
+        "n_gpus": 1, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "channel_cylinder_re3900_fine_4096x1024_coarse_1024x256_mrt_fp32",
+                   "fine_steps": r["fine"]["steps"], "coarse_steps": r["coarse_learned"]["steps"],
+                   "snapshots": 200, "filter": 4},
+        "cd": {"fine": r["fine"]["cd"], "coarse_plain": r["coarse_plain"]["cd"],
+               "coarse_learned": r["coarse_learned"]["cd"],
+               "rel_err_plain": r["coarse_plain"]["cd_rel_err"],
+               "rel_err_learned": r["coarse_learned"]["cd_rel_err"]},
+        "st": {"fine": r["fine"]["st"], "coarse_plain": r["coarse_plain"]["st"],
+               "coarse_learned": r["coarse_learned"]["st"]},
+        "wall_s": {"fine": r["fine"]["wall_s"], "coarse_plain": r["coarse_plain"]["wall_s"],
+                   "coarse_learned": r["coarse_learned"]["wall_s"]},
+        "training": r["training"],
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -344,11 +381,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--learned", action="store_true",
+                    help="learned-tau time-to-solution comparison instead of the MLUPS line")
+    ap.add_argument("--learned-steps", type=int, default=160000)
     ap.add_argument("--ncu-case", action="store_true",
                     help="short run of single launches for an ncu capture")
     a = ap.parse_args()
     if a.ncu_case:
         run_ncu_case(a)
+    elif a.learned:
+        run_learned(a)
     elif a.impl == "reference":
         run_reference_arm(a)
     else:

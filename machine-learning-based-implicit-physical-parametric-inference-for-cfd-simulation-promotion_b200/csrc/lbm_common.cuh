@@ -235,6 +235,51 @@ __device__ __forceinline__ void add_guo(C* f, C ux, C uy, C fx, C fy, C tau0)
     }
 }
 
+// Forcing term of the IB force for the operator in use, added after the
+// collision of a forced node (equilibrium at the corrected velocity
+// u = u* + F / (2 rho)); each form adds exactly F to the node's momentum:
+//   BGK  the Guo term above (omega from tau0, as Compute_Disforce)
+//   MRT  the Guo source G in moment space, M^-1 (I - S/2) M G, written out
+//        in the moment basis of collide_mrt: conserved jx, jy whole, e, eps,
+//        qx, qy with 1 - s/2 = 0.4, 0.45, 0.4, 0.4, pxx, pxy with 1 - 1/(2 tau)
+//   RR   first-order part of G halved, second-order part (1 - 1/(2 tau))
+template <typename C, int CO>
+__device__ __forceinline__ void add_force(C* f, C ux, C uy, C fx, C fy, C tau0, C tau)
+{
+    if (CO == CO_BGK) {
+        add_guo<C>(f, ux, uy, fx, fy, tau0);
+        return;
+    }
+    const C uF = ux * fx + uy * fy;
+    const C om2 = C(1) - C(0.5) / tau;
+    if (CO == CO_RR) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            const C eu = C(EX(k)) * ux + C(EY(k)) * uy;
+            const C eF = C(EX(k)) * fx + C(EY(k)) * fy;
+            f[k] += WK<C>(k) * (C(1.5) * eF + om2 * (C(9) * eu * eF - C(3) * uF));
+        }
+        return;
+    }
+    // moments of G: e 6 uF, eps -6 uF, jx Fx, qx -Fx, jy Fy, qy -Fy,
+    // pxx 2 (ux Fx - uy Fy), pxy ux Fy + uy Fx; a_m = (1 - s_m/2) G_m / |M_m|^2
+    const C a1 = C(0.4 * 6.0 / 36.0) * uF;
+    const C a2 = C(-0.45 * 6.0 / 36.0) * uF;
+    const C a3 = fx * C(1.0 / 6.0), a5 = fy * C(1.0 / 6.0);
+    const C a4 = fx * C(-0.4 / 12.0), a6 = fy * C(-0.4 / 12.0);
+    const C a7 = om2 * C(0.5) * (ux * fx - uy * fy);
+    const C a8 = om2 * C(0.25) * (ux * fy + uy * fx);
+    f[0] += C(-4) * a1 + C(4) * a2;
+    f[1] += -a1 - C(2) * a2 + a3 - C(2) * a4 + a7;
+    f[2] += -a1 - C(2) * a2 + a5 - C(2) * a6 - a7;
+    f[3] += -a1 - C(2) * a2 - a3 + C(2) * a4 + a7;
+    f[4] += -a1 - C(2) * a2 - a5 + C(2) * a6 - a7;
+    f[5] += C(2) * a1 + a2 + a3 + a4 + a5 + a6 + a8;
+    f[6] += C(2) * a1 + a2 - a3 - a4 + a5 + a6 - a8;
+    f[7] += C(2) * a1 + a2 - a3 - a4 - a5 - a6 + a8;
+    f[8] += C(2) * a1 + a2 + a3 + a4 - a5 - a6 - a8;
+}
+
 // Relax one node's populations in place with the chosen operator.
 template <typename C, int CO>
 __device__ __forceinline__ void collide_node(C* f, C rho, C ux, C uy, C rb, C tau)
@@ -273,8 +318,16 @@ constexpr int kMlpParams = kMlpB3 + 1;  // 1313
 constexpr int kMlpStats = 4 * kMlpIn + 1;
 static_assert(kMlpParams == 1313, "MLP size");
 
+// FP64 (parity path): libm-accurate tanh.  FP32: the hardware tanh
+// (tanh.approx.f32, one MUFU op, max relative error about 2^-11): with BF16
+// weights the network's own rounding is larger than that.
 __device__ __forceinline__ double mlp_tanh(double v) { return tanh(v); }
-__device__ __forceinline__ float mlp_tanh(float v) { return tanhf(v); }
+__device__ __forceinline__ float mlp_tanh(float v)
+{
+    float r;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(v));
+    return r;
+}
 // softplus(z) = max(z, 0) + log(1 + exp(-|z|))
 __device__ __forceinline__ double softplus(double z) { return fmax(z, 0.0) + log1p(exp(-fabs(z))); }
 __device__ __forceinline__ float softplus(float z) { return fmaxf(z, 0.f) + log1pf(expf(-fabsf(z))); }

@@ -772,7 +772,7 @@ __global__ void __launch_bounds__(kIbThreads, LRN ? 4 : 8) ib_finish(const IbArg
         a.dl_tau[(long long)xy.y * a.nx + xy.x] = double(tau);
     } else {
         collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
-        add_guo<C>(f, ux, uy, C(ia.fx[n]), C(ia.fy[n]), prm<C>(a.tau0, a.f_tau0));
+        add_force<C, CO>(f, ux, uy, C(ia.fx[n]), C(ia.fy[n]), prm<C>(a.tau0, a.f_tau0), tau);
 #pragma unroll
         for (int q = 0; q < 9; q++) stf<S>(a, q, xy.x, xy.y, f[q]);
     }

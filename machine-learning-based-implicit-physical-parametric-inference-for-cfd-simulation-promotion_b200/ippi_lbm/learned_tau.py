@@ -249,3 +249,60 @@ def strouhal(cl, d, u):
     spec = np.abs(np.fft.rfft(c * np.hanning(c.size)))
     k = int(np.argmax(spec[1:]) + 1)
     return float(k / c.size * d / u)
+
+
+# ---------------------------------------------------------------------------
+# the learned-tau experiment: fine plain run -> data -> training -> coarse runs
+# ---------------------------------------------------------------------------
+def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=160000,
+               avg_steps=64000, n_snap=200, max_samples=2_000_000, epochs=30, seed=0, device=0,
+               log=None):
+    """Fine lattice (plain Smagorinsky MRT, FP32) -> `n_snap` filtered
+    snapshots over its averaging window -> training -> the coarse lattice
+    (nx/factor x ny/factor, same Re and Mach) with plain Smagorinsky and with
+    the learned tau.  Mean Cd / Cl and St over the same physical window, and
+    the device wall time of each run."""
+    from . import scenes
+
+    say = log or (lambda s: None)
+    cx, cy = nx / 4, ny / 2
+    fine = scenes.cylinder_channel(nx, ny, d, cx, cy, u, re, seed=seed)
+    first = fine_steps - avg_steps + 1
+    stride = max(avg_steps // n_snap, 1)
+    say(f"fine {nx}x{ny}: {fine_steps} steps, snapshots every {stride} from {first}")
+    rf = run_cylinder(fine, fine_steps, first, snapshot=(factor, first + stride - 1, stride, n_snap),
+                      device=device)
+    say(f"fine: Cd {rf['cd']:.5f} St {rf['st']:.4f} wall {rf['wall_s']:.2f} s")
+    mx, my, dc = nx // factor, ny // factor, d / factor
+    coarse = scenes.cylinder_channel(mx, my, dc, cx / factor, cy / factor, u, re, seed=seed)
+    tau0c = coarse["params"]["tau0"]
+    mask = cylinder_mask(mx, my, cx / factor, cy / factor, dc)
+    xs, ys = zip(*(samples_from_snapshot(s, tau0c, mask) for s in rf["snapshots"]))
+    x, y = np.concatenate(xs), np.concatenate(ys)
+    rng = np.random.default_rng(seed)
+    if x.shape[0] > max_samples:
+        sel = rng.choice(x.shape[0], max_samples, replace=False)
+        x, y = x[sel], y[sel]
+    t0 = time.perf_counter()
+    net, hist = train(x, y, epochs=epochs, seed=seed, device=device, log=log)
+    train_s = time.perf_counter() - t0
+    say(f"trained on {x.shape[0]} samples in {train_s:.1f} s, loss {hist[0]:.4g} -> {hist[-1]:.4g}")
+    csteps, cfirst = fine_steps // factor, (fine_steps - avg_steps) // factor + 1
+    rp = run_cylinder(coarse, csteps, cfirst, device=device)
+    rl = run_cylinder(coarse, csteps, cfirst, net=net, device=device)
+    say(f"coarse plain: Cd {rp['cd']:.5f}; learned: Cd {rl['cd']:.5f}")
+
+    def err(r):
+        return abs(r["cd"] - rf["cd"]) / abs(rf["cd"])
+
+    return dict(
+        fine=dict(nx=nx, ny=ny, steps=fine_steps, cd=rf["cd"], cl=rf["cl"], st=rf["st"],
+                  wall_s=rf["wall_s"]),
+        coarse_plain=dict(nx=mx, ny=my, steps=csteps, cd=rp["cd"], st=rp["st"], wall_s=rp["wall_s"],
+                          cd_rel_err=err(rp)),
+        coarse_learned=dict(nx=mx, ny=my, steps=csteps, cd=rl["cd"], st=rl["st"], wall_s=rl["wall_s"],
+                            cd_rel_err=err(rl)),
+        training=dict(samples=int(x.shape[0]), epochs=epochs, loss_first=hist[0], loss_last=hist[-1],
+                      seconds=train_s),
+        speedup_vs_fine=rf["wall_s"] / rl["wall_s"],
+        net=net)

@@ -329,6 +329,59 @@ static void guo_force(double ux, double uy, double Fx, double Fy, double tau0, d
     }
 }
 
+/* Forcing term of the IB force (Fx, Fy) for the collision operator in use
+ * (no reference code: the reference's IB path is not active).  Each form
+ * adds exactly F to a forced node's momentum in one collision, the
+ * equilibrium being taken at the corrected velocity u = u* + F / (2 rho):
+ *   BGK  Lattice::Compute_Disforce (Guo, omega from tau0), as the reference
+ *   MRT  the Guo source G in moment space, M^-1 (I - S/2) M G: conserved
+ *        moments take it whole, the others (1 - s_m / 2), s_7 = s_8 = 1/tau
+ *   RR   first-order part of G halved (the shifted equilibrium carries the
+ *        other half), second-order part (1 - 1/(2 tau)) */
+static void force_term(int coll, double ux, double uy, double Fx, double Fy, double tau0,
+                       double tau, double* lf)
+{
+    if (coll == COLL_BGK) {
+        guo_force(ux, uy, Fx, Fy, tau0, lf);
+        return;
+    }
+    double g[9];
+    for (int k = 0; k < 9; k++) {
+        double eu = E[k][0] * ux + E[k][1] * uy;
+        double eF = E[k][0] * Fx + E[k][1] * Fy;
+        double uF = ux * Fx + uy * Fy;
+        if (coll == COLL_RR)
+            lf[k] = W[k] * (0.5 * 3.0 * eF + (1.0 - 0.5 / tau) * (9.0 * eu * eF - 3.0 * uF));
+        g[k] = W[k] * (3.0 * eF - 3.0 * uF + 9.0 * eu * eF);
+    }
+    if (coll == COLL_RR) return;
+    if (!g_mrt_ready) {
+        build_mrt(g_tm, g_tminv);
+        g_mrt_ready = 1;
+    }
+    double sm[9] = {0, 1.2, 1.1, 0, 1.2, 0, 1.2, 1. / tau, 1. / tau};
+    double a[9];
+    for (int m = 0; m < 9; m++) {
+        double gm = 0.0, norm = 0.0;
+        for (int k = 0; k < 9; k++) {
+            gm += g_tm[m][k] * g[k];
+            norm += g_tm[m][k] * g_tm[m][k];
+        }
+        a[m] = (1.0 - 0.5 * sm[m]) * gm / norm;
+    }
+    for (int k = 0; k < 9; k++) {
+        double v = 0.0;
+        for (int m = 0; m < 9; m++) v += g_tm[m][k] * a[m];
+        lf[k] = v;
+    }
+}
+
+void orc_force_node(int collision, double ux, double uy, double fx, double fy, double tau0,
+                    double tau, double* lf)
+{
+    force_term(collision, ux, uy, fx, fy, tau0, tau, lf);
+}
+
 /* Mesh::DiracDelta, mesh.cpp:1354-1385 */
 double orc_peskin_phi(double x)
 {
@@ -748,7 +801,7 @@ static int collide_all(orc* s)
             orc_collide_node(coll, fn, r, s->ux[id], s->uy[id], s->tau[id], fc);
             if (s->nmark > 0) {
                 double lf[9];
-                guo_force(s->ux[id], s->uy[id], s->fxn[id], s->fyn[id], s->p.tau0, lf);
+                force_term(coll, s->ux[id], s->uy[id], s->fxn[id], s->fyn[id], s->p.tau0, s->tau[id], lf);
                 for (int k = 0; k < 9; k++) fc[k] += lf[k];
             }
             for (int k = 0; k < 9; k++) FC(s, k, i, j) = fc[k];

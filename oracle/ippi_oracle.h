@@ -100,6 +100,10 @@ void orc_collide_node(int collision, const double* fnew, double rho, double ux,
                       double uy, double tau, double* fcol);
 double orc_les_tau(const double* fnew, double rho, double ux, double uy,
                    double tau0, double cs);
+/* IB forcing term added after one collision of a forced node (per operator,
+ * see force_term in ippi_oracle.c) -> lf[9]. */
+void orc_force_node(int collision, double ux, double uy, double fx, double fy, double tau0,
+                    double tau, double* lf);
 
 /* Learned relaxation time (no reference code; les_model 2): network
  * parameters w[1313] (the FP32 values of the BF16 weights: W1[32][6] b1[32]

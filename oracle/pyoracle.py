@@ -73,6 +73,8 @@ def lib() -> C.CDLL:
                                        C.c_double, _dp]
         L.orc_les_tau.restype = C.c_double
         L.orc_les_tau.argtypes = [_dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.orc_force_node.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                     C.c_double, C.c_double, _dp]
         L.orc_load_tau_mlp.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_size_t,
                                        C.POINTER(C.c_float), C.c_size_t]
         L.orc_learned_tau.argtypes = [_dp, C.c_double, C.c_double, C.c_double, C.c_double,
