@@ -72,6 +72,7 @@ extern "C" {
 #define IPPI_LES_SMAGORINSKY 1 /* SmagorinskyByHybrid, mesh.cpp:852-911 */
 #define IPPI_LES_LEARNED 2     /* per-node network (ippi_load_tau_mlp), Smagorinsky
                                   outside its training range; channel scene only */
+#define IPPI_LES_FIELD 3       /* a given relaxation time per node (ippi_set_tau_field) */
 /* IB interpolation/spreading kernel */
 #define IPPI_DELTA_BILINEAR 0 /* mesh.cpp:606-644 (default of Parameter.h) */
 #define IPPI_DELTA_PESKIN4 1  /* Dirac_Delta, mesh.cpp:555-605, 1354-1389 */
@@ -187,6 +188,11 @@ int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk,
 int ippi_load_tau_mlp(ippi_lbm* h, const uint16_t* w_bf16, size_t n, const float* stats,
                       size_t nstats);
 
+/* No counterpart in the reference: the relaxation time of every node for
+ * IPPI_LES_FIELD, tau[ny][nx] (host, each > 0.5) -- the parameter field of
+ * the adjoint's tau gradient. */
+int ippi_set_tau_field(ippi_lbm* h, const double* tau);
+
 /* Filtered snapshot of the current state for training the learned tau:
  * box filter over factor x factor blocks (nx, ny multiples of factor) into
  * out[6][ny/factor][nx/factor] (host, FP64): rho_bar, ux_bar, uy_bar
@@ -213,6 +219,31 @@ int ippi_mlp_grad(const float* x, const float* y, int n, const float* w, float* 
 int ippi_mlp_adam(float* w, const float* grad, float* m, float* v, int step, float lr, float beta1,
                   float beta2, float eps, void* stream);
 int ippi_mlp_forward(const float* x, int n, const float* w, float* out, void* stream);
+
+/* ippi_load_tau_mlp with FP32 weights used as given (no BF16 rounding):
+ * for gradient checks and end-to-end training through the solver. */
+int ippi_load_tau_mlp_f32(ippi_lbm* h, const float* w, size_t n, const float* stats, size_t nstats);
+
+/* No counterpart in the reference: reverse-mode gradients through the step
+ * (channel scene; BGK / MRT / RR; tau constant, Smagorinsky, learned or a
+ * field; immersed boundary with one direct-forcing pass).
+ * ippi_adjoint_forward advances nsteps steps numbered t0.. like ippi_step,
+ * keeping the state before every ckpt_every-th step on the device.
+ * ippi_adjoint_backward then returns, for the loss L whose partial
+ * derivatives are
+ *   dl_dforce[nsteps][nbody][2]  dL / d(body force of each step) (may be NULL)
+ *   dl_dmacro[3][ny][nx]        dL / d(rho, ux, uy) of the last step's
+ *                               post-stream state, i.e. the fields
+ *                               ippi_download gives after the rollout (may be NULL),
+ * the gradients (host arrays, FP64, each may be NULL):
+ *   grad_tau[ny][nx]   with respect to the tau field (IPPI_LES_FIELD)
+ *   grad_mlp[1313]     with respect to the network weights (IPPI_LES_LEARNED)
+ *   grad_f0[9][ny][nx] with respect to the populations before the first step
+ * Each segment of ckpt_every steps is recomputed from its checkpoint with the
+ * forward kernels; the reverse sweep is FP64. */
+int ippi_adjoint_forward(ippi_lbm* h, int nsteps, int t0, int ckpt_every);
+int ippi_adjoint_backward(ippi_lbm* h, const double* dl_dforce, const double* dl_dmacro,
+                          double* grad_tau, double* grad_mlp, double* grad_f0);
 
 /* Last error message of the handle (or of the library when h is NULL). */
 int ippi_last_error(ippi_lbm* h, char* buf, size_t n);

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "../../include/ippi_lbm.h"
+#include "adjoint.h"
 #include "launch.h"
 
 using namespace ippi;
@@ -98,6 +99,16 @@ struct ippi_lbm {
     long long hist_written = 0;
     // learned tau: parameters (FP32 values of the BF16 weights) + statistics
     float* mlp_dev = nullptr;
+    double* tau_field = nullptr;  // IPPI_LES_FIELD: [ny][nx]
+    // adjoint: the recorded rollout (checkpoints every K steps) and work buffers
+    struct Adjoint {
+        bool ready = false;
+        int nsteps = 0, t0 = 0, K = 0;
+        std::vector<void*> ck;   // state before steps 0, K, 2K, ...
+        std::vector<void*> seg;  // recomputed inputs of one segment
+        std::vector<void*> work; // everything else, freed together
+    } adj;
+    bool no_avg = false;         // forward recomputes must not touch the averages
     // graphs of two steps and of one step: [start buffer][step parity]
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     cudaGraphExec_t graph1[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -203,6 +214,15 @@ void drop_graphs(ippi_lbm* h)
                     cudaGraphExecDestroy(*g);
                     *g = nullptr;
                 }
+}
+
+void adjoint_free(ippi_lbm* h)
+{
+    for (auto* v : {&h->adj.ck, &h->adj.seg, &h->adj.work}) {
+        for (void* p : *v) dfree(p);
+        v->clear();
+    }
+    h->adj.ready = false;
 }
 
 cudaError_t launch(const LaunchSet& L, int S)
@@ -592,6 +612,7 @@ LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int pa
     a.ny = h->p.ny;
     a.les = h->p.les_model;
     a.mlp = h->mlp_dev;
+    a.tau_field = h->tau_field;
     a.plate_x0 = h->p.plate_x0;
     a.tau0 = h->p.tau0;
     a.cs = h->p.cs;
@@ -609,7 +630,7 @@ LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int pa
     a.nslots = h->nslots;
     a.corner = h->corner;
     a.avg = h->avg;
-    a.avg_start = h->p.avg_start;
+    a.avg_start = h->no_avg ? 0x7fffffff : h->p.avg_start;
     a.ctr = h->ctr;
     a.mode = mode;
     a.par = par;
@@ -668,15 +689,17 @@ int set_time(ippi_lbm* h, int t)
     return IPPI_OK;
 }
 
-// the first collision, from the equilibrium of the initial moments (k = 0)
 // every launch computes relaxation times: the learned model needs its network
 int tau_ready(ippi_lbm* h)
 {
     if (h->p.les_model == IPPI_LES_LEARNED && !h->mlp_dev)
         return fail(h, IPPI_ERR_STATE, "learned tau selected but no network loaded (ippi_load_tau_mlp)");
+    if (h->p.les_model == IPPI_LES_FIELD && !h->tau_field)
+        return fail(h, IPPI_ERR_STATE, "tau field selected but none set (ippi_set_tau_field)");
     return IPPI_OK;
 }
 
+// the first collision, from the equilibrium of the initial moments (k = 0)
 int run_init(ippi_lbm* h)
 {
     if (int rc = tau_ready(h)) return rc;
@@ -777,7 +800,7 @@ int ippi_create(const ippi_params* p, ippi_lbm** out)
     if (p->collision < 0 || p->collision > 2) return fail(nullptr, IPPI_ERR_ARG, "bad collision");
     if (p->storage < 0 || p->storage > 3) return fail(nullptr, IPPI_ERR_ARG, "bad storage");
     if (p->bc_set < 0 || p->bc_set > 1) return fail(nullptr, IPPI_ERR_ARG, "bad bc_set");
-    if (p->les_model < 0 || p->les_model > 2) return fail(nullptr, IPPI_ERR_ARG, "bad les_model");
+    if (p->les_model < 0 || p->les_model > 3) return fail(nullptr, IPPI_ERR_ARG, "bad les_model");
     if (p->les_model == IPPI_LES_LEARNED && p->bc_set != IPPI_BC_CHANNEL)
         return fail(nullptr, IPPI_ERR_ARG, "the learned relaxation time is built for the channel scene");
     if (p->delta_kernel < 0 || p->delta_kernel > 1) return fail(nullptr, IPPI_ERR_ARG, "bad delta_kernel");
@@ -844,8 +867,10 @@ int ippi_destroy(ippi_lbm* h)
     if (!h) return IPPI_OK;
     if (h->st) cudaStreamSynchronize(h->st);
     drop_graphs(h);
+    adjoint_free(h);
     for (int b = 0; b < 2; b++) dfree(h->f[b]);
     dfree(h->mlp_dev);
+    dfree(h->tau_field);
     dfree(h->ctr);
     if (h->ctr_h) cudaFreeHost(h->ctr_h);
     dfree(h->nflag);
@@ -1214,8 +1239,7 @@ int ippi_load_tau_mlp(ippi_lbm* h, const uint16_t* w_bf16, size_t n, const float
     CK(h, cudaStreamSynchronize(h->st));
     if (!h->mlp_dev) CK(h, dalloc(&h->mlp_dev, blob.size() * sizeof(float)));
     CK(h, cudaMemcpy(h->mlp_dev, blob.data(), blob.size() * sizeof(float), cudaMemcpyHostToDevice));
-    // the pointer is baked into the step graphs only through StepArgs, which
-    // were captured with the old (possibly null) pointer
+    // step graphs captured before the first load hold a null network pointer
     drop_graphs(h);
     h->dl_valid = false;
     return IPPI_OK;
@@ -1240,5 +1264,207 @@ int ippi_filter_snapshot(ippi_lbm* h, int factor, double* out, size_t bytes)
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
     dfree(d);
     CK(h, e);
+    return IPPI_OK;
+}
+
+int ippi_set_tau_field(ippi_lbm* h, const double* tau)
+{
+    if (!h || !tau) return fail(h, IPPI_ERR_ARG, "null argument");
+    const size_t nn = (size_t)h->p.nx * h->p.ny;
+    for (size_t i = 0; i < nn; i++)
+        if (!(tau[i] > 0.5) || !std::isfinite(tau[i]))
+            return fail(h, IPPI_ERR_ARG, "tau field must exceed 0.5 (node %zu)", i);
+    CK(h, cudaSetDevice(h->p.device));
+    CK(h, cudaStreamSynchronize(h->st));
+    if (!h->tau_field) CK(h, dalloc(&h->tau_field, nn * sizeof(double)));
+    CK(h, cudaMemcpy(h->tau_field, tau, nn * sizeof(double), cudaMemcpyHostToDevice));
+    drop_graphs(h);
+    h->dl_valid = false;
+    return IPPI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// adjoint
+// ---------------------------------------------------------------------------
+int ippi_load_tau_mlp_f32(ippi_lbm* h, const float* w, size_t n, const float* stats, size_t nstats)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (!w || n != (size_t)IPPI_MLP_PARAMS) return fail(h, IPPI_ERR_ARG, "tau network: %d weights expected", IPPI_MLP_PARAMS);
+    std::vector<uint16_t> dummy(IPPI_MLP_PARAMS, 0);
+    int rc = ippi_load_tau_mlp(h, dummy.data(), n, stats, nstats);  // validates and allocates
+    if (rc) return rc;
+    for (size_t i = 0; i < n; i++)
+        if (!std::isfinite(w[i])) return fail(h, IPPI_ERR_ARG, "tau network weight %zu is not finite", i);
+    CK(h, cudaMemcpy(h->mlp_dev, w, n * sizeof(float), cudaMemcpyHostToDevice));
+    return IPPI_OK;
+}
+
+int ippi_adjoint_forward(ippi_lbm* h, int nsteps, int t0, int ckpt_every)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (nsteps < 1 || ckpt_every < 1) return fail(h, IPPI_ERR_ARG, "nsteps and ckpt_every must be positive");
+    if (h->p.bc_set != IPPI_BC_CHANNEL) return fail(h, IPPI_ERR_STATE, "the adjoint is built for the channel scene");
+    if (h->ib_active && h->p.mdf_iters != 1)
+        return fail(h, IPPI_ERR_STATE, "the adjoint supports one direct-forcing pass (mdf_iters = 1)");
+    if (h->ib_active && (long long)nsteps > h->hist_cap)
+        return fail(h, IPPI_ERR_ARG, "rollout longer than the force history (%d steps)", h->hist_cap);
+    if (int rc = tau_ready(h)) return rc;
+    CK(h, cudaSetDevice(h->p.device));
+    adjoint_free(h);
+    if (h->pending_init) {
+        int rc = run_init(h);
+        if (rc) return rc;
+    }
+    const size_t fbytes = (size_t)9 * h->plane * h->tsize;
+    const int nck = (nsteps + ckpt_every - 1) / ckpt_every;
+    for (int i = 0; i < nck; i++) {
+        void* p = nullptr;
+        if (dalloc(&p, fbytes) != cudaSuccess) {
+            adjoint_free(h);
+            return fail(h, IPPI_ERR_NOMEM, "adjoint checkpoints (%d x %zu bytes)", nck, fbytes);
+        }
+        h->adj.ck.push_back(p);
+        CK(h, cudaMemcpyAsync(p, h->f[h->cur], fbytes, cudaMemcpyDeviceToDevice, h->st));
+        const int n = std::min(ckpt_every, nsteps - i * ckpt_every);
+        int rc = ippi_step(h, n, t0 + i * ckpt_every);
+        if (rc) {
+            adjoint_free(h);
+            return rc;
+        }
+    }
+    h->adj.nsteps = nsteps;
+    h->adj.t0 = t0;
+    h->adj.K = ckpt_every;
+    h->adj.ready = true;
+    return IPPI_OK;
+}
+
+int ippi_adjoint_backward(ippi_lbm* h, const double* dl_dforce, const double* dl_dmacro, double* grad_tau,
+                          double* grad_mlp, double* grad_f0)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (!h->adj.ready) return fail(h, IPPI_ERR_STATE, "no recorded rollout (ippi_adjoint_forward)");
+    if (grad_tau && h->p.les_model != IPPI_LES_FIELD)
+        return fail(h, IPPI_ERR_STATE, "grad_tau needs the tau-field model (IPPI_LES_FIELD)");
+    if (grad_mlp && h->p.les_model != IPPI_LES_LEARNED)
+        return fail(h, IPPI_ERR_STATE, "grad_mlp needs the learned model (IPPI_LES_LEARNED)");
+    CK(h, cudaSetDevice(h->p.device));
+    const int nx = h->p.nx, ny = h->p.ny, nsteps = h->adj.nsteps, K = h->adj.K;
+    const size_t nn = (size_t)nx * ny;
+    const size_t fbytes = (size_t)9 * h->plane * h->tsize;
+    auto& W = h->adj.work;
+    auto get = [&](size_t bytes) -> void* {
+        void* p = nullptr;
+        if (dalloc(&p, bytes) != cudaSuccess) p = nullptr;
+        W.push_back(p);  // a failed allocation stays as a null entry
+        if (p) cudaMemsetAsync(p, 0, bytes, h->st);
+        return p;
+    };
+    // work buffers (freed with the record)
+    for (void* p : W) dfree(p);
+    W.clear();
+    for (void* p : h->adj.seg) dfree(p);
+    h->adj.seg.clear();
+    for (int i = 1; i < K && i < nsteps; i++) {
+        void* p = nullptr;
+        if (dalloc(&p, fbytes) != cudaSuccess) return fail(h, IPPI_ERR_NOMEM, "adjoint segment buffers");
+        h->adj.seg.push_back(p);
+    }
+    AdjArgs A{};
+    A.storage = h->S;
+    A.collision = h->p.collision;
+    A.learned = h->p.les_model == IPPI_LES_LEARNED;
+    A.ft = (double*)get(9 * nn * sizeof(double));
+    A.m = (double*)get(3 * nn * sizeof(double));
+    double* la = (double*)get(9 * nn * sizeof(double));
+    double* lb = (double*)get(9 * nn * sizeof(double));
+    A.lam_ft = (double*)get(9 * nn * sizeof(double));
+    A.grad_tau = grad_tau ? (double*)get(nn * sizeof(double)) : nullptr;
+    double* gmlp = nullptr;
+    double* part = nullptr;
+    if (grad_mlp) {
+        A.xs = (double*)get(nn * 6 * sizeof(double));
+        A.up = (double*)get(nn * sizeof(double));
+        gmlp = (double*)get(IPPI_MLP_PARAMS * sizeof(double));
+        part = (double*)get(mlp_grad_f64_partial_doubles() * sizeof(double));
+    }
+    double* dldm = nullptr;
+    if (dl_dmacro) {
+        dldm = (double*)get(3 * nn * sizeof(double));
+        if (dldm) CK(h, cudaMemcpyAsync(dldm, dl_dmacro, 3 * nn * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    }
+    double* dldF = nullptr;
+    IbArgs I = h->ib;
+    if (h->ib_active) {
+        const int nf = h->nforced, nm = h->nmark;
+        A.ib = &I;
+        A.nst = h->ib_nst;
+        A.fidx = (int*)get(nn * sizeof(int));
+        A.mbody = (int*)get(std::max(nm, 1) * sizeof(int));
+        A.ib_rho = (double*)get(nf * sizeof(double));
+        A.lam_rho = (double*)get(nf * sizeof(double));
+        A.ib_us = (double2*)get(nf * sizeof(double2));
+        A.ib_fn = (double2*)get(nf * sizeof(double2));
+        A.ib_uc = (double2*)get(nf * sizeof(double2));
+        A.lam_uc = (double2*)get(nf * sizeof(double2));
+        A.lam_fn = (double2*)get(nf * sizeof(double2));
+        A.lam_ftot = (double2*)get(nf * sizeof(double2));
+        A.ib_F = (double2*)get(nm * sizeof(double2));
+        A.lam_F = (double2*)get(nm * sizeof(double2));
+        if (dl_dforce) {
+            const size_t nb = (size_t)nsteps * h->nbody * 2;
+            dldF = (double*)get(nb * sizeof(double));
+            if (dldF) CK(h, cudaMemcpyAsync(dldF, dl_dforce, nb * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        }
+    }
+    for (void* p : W)
+        if (!p) return fail(h, IPPI_ERR_NOMEM, "adjoint work buffers");
+    if (h->ib_active) CK(h, adj_ib_tables(I, nx, ny, const_cast<int*>(A.fidx), const_cast<int*>(A.mbody), h->st));
+
+    h->no_avg = true;
+    int rc = IPPI_OK;
+    const int nck = (int)h->adj.ck.size();
+    for (int seg = nck - 1; seg >= 0 && rc == IPPI_OK; seg--) {
+        const int s0 = seg * K, s1 = std::min(s0 + K, nsteps);
+        std::vector<const void*> in(s1 - s0);
+        in[0] = h->adj.ck[seg];
+        // recompute the segment's step inputs with the forward kernels
+        h->ctr_h->t[0] = h->adj.t0 + s0;
+        cudaMemcpyAsync(&h->ctr->t[0], &h->ctr_h->t[0], sizeof(int), cudaMemcpyHostToDevice, h->st);
+        for (int s = s0; s < s1 - 1; s++) {
+            void* out = h->adj.seg[s - s0];
+            LaunchSet L = make_launch(h, MODE_STEP, in[s - s0], out, (s - s0) & 1);
+            cudaError_t e = launch(L, h->S);
+            if (e != cudaSuccess) {
+                rc = fail(h, IPPI_ERR_CUDA, "adjoint recompute: %s", cudaGetErrorString(e));
+                break;
+            }
+            in[s - s0 + 1] = out;
+        }
+        for (int s = s1 - 1; s >= s0 && rc == IPPI_OK; s--) {
+            A.s = make_launch(h, MODE_STEP, in[s - s0], nullptr, 0).step;
+            A.lam_out = la;
+            A.lam_in = lb;
+            A.dldm = dldm;
+            A.dldF = dldF ? dldF + (size_t)s * h->nbody * 2 : nullptr;
+            cudaError_t e = adj_state(A, h->st);
+            if (e == cudaSuccess && h->ib_active) e = adj_ib_fwd(A, h->st);
+            if (e == cudaSuccess) e = adj_collide(A, h->st);
+            if (e == cudaSuccess && dldm && s == nsteps - 1) e = adj_inject_moments(A, h->st);
+            if (e == cudaSuccess && gmlp) e = mlp_grad_upstream_f64(A.xs, A.up, (int)nn, h->mlp_dev, part, gmlp, h->st);
+            if (e == cudaSuccess && h->ib_active) e = adj_ib_back(A, h->st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(lb, 0, 9 * nn * sizeof(double), h->st);
+            if (e == cudaSuccess) e = adj_stream(A, h->st);
+            if (e != cudaSuccess) rc = fail(h, IPPI_ERR_CUDA, "adjoint step %d: %s", s, cudaGetErrorString(e));
+            std::swap(la, lb);
+        }
+    }
+    h->no_avg = false;
+    if (rc) return rc;
+    if (grad_f0) CK(h, cudaMemcpyAsync(grad_f0, la, 9 * nn * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    if (grad_tau) CK(h, cudaMemcpyAsync(grad_tau, A.grad_tau, nn * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    if (grad_mlp) CK(h, cudaMemcpyAsync(grad_mlp, gmlp, IPPI_MLP_PARAMS * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    CK(h, cudaGetLastError());
     return IPPI_OK;
 }

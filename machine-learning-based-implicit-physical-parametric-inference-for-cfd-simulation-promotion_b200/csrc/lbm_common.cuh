@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "dual.cuh"
+
 namespace ippi {
 
 enum { ST_F64 = 0, ST_F32 = 1, ST_F16 = 2, ST_BF16 = 3 };
@@ -392,6 +394,53 @@ __device__ __forceinline__ C learned_tau(C pxx, C pxy, C pyy, C rho, C ux, C uy,
     return tau0 + C(__ldg(st + 4 * kMlpIn)) * mlp_forward<C>(w, x);
 }
 
+// The learned tau on dual numbers (adjoint): features carry their partial
+// derivatives; the network runs in FP64 with a backward pass for dz/dx, and
+// the chain rule gives the partial derivatives of tau.
+template <int N>
+__device__ Dual<N> learned_tau(Dual<N> pxx, Dual<N> pxy, Dual<N> pyy, Dual<N> rho, Dual<N> ux,
+                               Dual<N> uy, Dual<N> tau0, Dual<N> cs, const float* __restrict__ w)
+{
+    using D = Dual<N>;
+    const float* st = w + kMlpParams;
+    D x[kMlpIn];
+    mlp_features<D>(pxx, pxy, pyy, rho, ux, uy, tau0, x);
+    bool in = true;
+    for (int i = 0; i < kMlpIn; i++) {
+        in = in && x[i].v >= double(st[2 * kMlpIn + i]) && x[i].v <= double(st[3 * kMlpIn + i]);
+        x[i] = (x[i] - D(double(st[i]))) / D(double(st[kMlpIn + i]));
+    }
+    if (!in) return les_tau<D>(pxx, pxy, pyy, rho, tau0, cs);
+    double h1[kMlpHid], g2[kMlpHid];
+    for (int j = 0; j < kMlpHid; j++) {
+        double a = w[kMlpB1 + j];
+        for (int i = 0; i < kMlpIn; i++) a += double(w[kMlpW1 + j * kMlpIn + i]) * x[i].v;
+        h1[j] = tanh(a);
+    }
+    double z = w[kMlpB3];
+    for (int j = 0; j < kMlpHid; j++) {
+        double a = w[kMlpB2 + j];
+        for (int i = 0; i < kMlpHid; i++) a += double(w[kMlpW2 + j * kMlpHid + i]) * h1[i];
+        const double h2 = tanh(a);
+        z += double(w[kMlpW3 + j]) * h2;
+        g2[j] = double(w[kMlpW3 + j]) * (1.0 - h2 * h2);  // dz / d(pre-activation 2)
+    }
+    double gx[kMlpIn] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < kMlpHid; i++) {
+        double g1 = 0.0;
+        for (int j = 0; j < kMlpHid; j++) g1 += double(w[kMlpW2 + j * kMlpHid + i]) * g2[j];
+        g1 *= 1.0 - h1[i] * h1[i];
+        for (int k = 0; k < kMlpIn; k++) gx[k] += double(w[kMlpW1 + i * kMlpIn + k]) * g1;
+    }
+    const double os = st[4 * kMlpIn];
+    const double sig = 1.0 / (1.0 + exp(-z));
+    D t = tau0;
+    t.v += os * (fmax(z, 0.0) + log1p(exp(-fabs(z))));
+    for (int k = 0; k < kMlpIn; k++)
+        for (int i = 0; i < N; i++) t.d[i] += os * sig * gx[k] * x[k].d[i];
+    return t;
+}
+
 // relaxation time of a node's next collision: tau0, Smagorinsky, or (LRN)
 // the learned model with its Smagorinsky fallback
 template <typename C, bool LRN = false>
@@ -401,7 +450,7 @@ __device__ __forceinline__ C node_tau(const C* f, C rho, C ux, C uy, C rb, int l
     if (!LRN && !les) return tau0;
     C pxx, pxy, pyy;
     pi_neq<C>(f, rho, ux, uy, rb, pxx, pxy, pyy);
-    if (LRN) return learned_tau<C>(pxx, pxy, pyy, rho, ux, uy, tau0, cs, mlp);
+    if (LRN) return learned_tau(pxx, pxy, pyy, rho, ux, uy, tau0, cs, mlp);
     return les_tau<C>(pxx, pxy, pyy, rho, tau0, cs);
 }
 

@@ -56,6 +56,7 @@ struct StepArgs {
     int fixed_t;          // step number for the MAT modes
     const double* init_m; // [3][ny][nx] initial rho, ux, uy (INIT modes)
     const float* mlp;     // learned tau: parameters + feature statistics (LRN kernels)
+    const double* tau_field; // les == 3: relaxation time per node [ny][nx]
     double* dl_f;         // MAT: fnew [9][ny][nx]
     double* dl_m;         // MAT: rho, ux, uy, boundary-net flag [4][ny][nx]
     double* dl_tau;       // MAT: tau of the next collision [ny][nx]
@@ -421,8 +422,9 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
             node_state<S, SC>(a, x, y, f, rho, ux, uy);
             if (!deferred) {
                 node_epilogue<S>(a, node, t, f, rho, ux, uy);
-                const C tau = node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
-                                               prm<C>(a.cs, a.f_cs), a.mlp);
+                const C tau = a.les == 3 ? C(a.tau_field[node])
+                                         : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
+                                                            prm<C>(a.cs, a.f_cs), a.mlp);
                 if (a.mode >= MODE_MAT) {
                     a.dl_tau[node] = double(tau);
                 } else {
@@ -595,8 +597,11 @@ __global__ void __launch_bounds__(kBandThreads) band_kernel(const BandArgs ba)
         const C rho = mm[0], ux = mm[1], uy = mm[2];
         const C rbs = rbase<S>(a);
         const bool use_nn = nn_tau >= 0.501;
-        const C tau = use_nn ? C(nn_tau) : node_tau<C>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0), prm<C>(a.cs, a.f_cs));
         const long long node = (long long)bn.y * a.nx + bn.x;
+        const C tau = use_nn       ? C(nn_tau)
+                      : a.les == 3 ? C(a.tau_field[node])
+                                   : node_tau<C>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
+                                                 prm<C>(a.cs, a.f_cs));
         if (a.mode >= MODE_MAT) {
             a.dl_tau[node] = double(tau);
             a.dl_m[3ll * a.nx * a.ny + node] = use_nn ? 1.0 : 0.0;
@@ -765,9 +770,10 @@ __global__ void __launch_bounds__(kIbThreads, LRN ? 4 : 8) ib_finish(const IbArg
     const C rho = C(ia.rho[n]);
     const C ux = C(ia.ucx[n]), uy = C(ia.ucy[n]);
     const C rbs = rbase<S>(a);
-    const C tau = node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
-                                   prm<C>(a.cs, a.f_cs), a.mlp);
     const int2 xy = ia.fn_xy[n];
+    const C tau = a.les == 3 ? C(a.tau_field[(long long)xy.y * a.nx + xy.x])
+                             : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
+                                                prm<C>(a.cs, a.f_cs), a.mlp);
     if (a.mode >= MODE_MAT) {
         a.dl_tau[(long long)xy.y * a.nx + xy.x] = double(tau);
     } else {

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/ippi_lbm.h"
+#include "adjoint.h"
 #include "lbm_common.cuh"
 
 namespace {
@@ -29,84 +30,99 @@ constexpr int kXRow = kMlpIn + 1;
 // per warp: x[32][7], h1/h2/d2/d1 [32][33], dout[32]
 constexpr int kWarpFloats = 32 * kXRow + 4 * 32 * kRow + 32;
 constexpr int kPartial = kMlpParams + 1;        // gradient + loss
-constexpr size_t kGradSmem = (size_t)(kWarps * kWarpFloats + kMlpParams + 3) * sizeof(float);
+template <typename R>
+constexpr size_t grad_smem()
+{
+    return (size_t)(kWarps * kWarpFloats + kMlpParams + 3) * sizeof(R);
+}
 static_assert(kWarps * kWarpFloats >= kWarps * kPartial, "reduction buffer fits the staging area");
 
-__device__ __forceinline__ float sigmoidf(float z) { return 1.f / (1.f + expf(-z)); }
+__device__ __forceinline__ float sigm(float z) { return 1.f / (1.f + expf(-z)); }
+__device__ __forceinline__ double sigm(double z) { return 1.0 / (1.0 + exp(-z)); }
+__device__ __forceinline__ float acc_tanh(float v) { return tanhf(v); }
+__device__ __forceinline__ double acc_tanh(double v) { return tanh(v); }
 
-__global__ void __launch_bounds__(kThreads) mlp_grad_kernel(const float* __restrict__ X,
-                                                             const float* __restrict__ Y, int n,
-                                                             const float* __restrict__ W,
-                                                             float* __restrict__ part)
+// R: arithmetic type.  UP = false: Y holds targets, the loss is the mean
+// squared error of softplus(z).  UP = true: Y holds upstream gradients
+// dL/dsoftplus per sample (the loss is sum Y * softplus; no mean).
+template <typename R, bool UP>
+__global__ void __launch_bounds__(kThreads) mlp_grad_kernel(const R* __restrict__ X, const R* __restrict__ Y,
+                                                             int n, const float* __restrict__ W,
+                                                             R* __restrict__ part)
 {
-    extern __shared__ float sm[];
-    float* ws = sm + kWarps * kWarpFloats;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    R* sm = reinterpret_cast<R*>(sm_raw);
+    R* ws = sm + kWarps * kWarpFloats;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int p = tid; p < kMlpParams; p += kThreads) ws[p] = W[p];
+    for (int p = tid; p < kMlpParams; p += kThreads) ws[p] = R(W[p]);
     __syncthreads();
-    float* base = sm + warp * kWarpFloats;
-    float* xs = base;
-    float* h1s = xs + 32 * kXRow;
-    float* h2s = h1s + 32 * kRow;
-    float* d2s = h2s + 32 * kRow;
-    float* d1s = d2s + 32 * kRow;
-    float* dos = d1s + 32 * kRow;
+    R* base = sm + warp * kWarpFloats;
+    R* xs = base;
+    R* h1s = xs + 32 * kXRow;
+    R* h2s = h1s + 32 * kRow;
+    R* d2s = h2s + 32 * kRow;
+    R* d1s = d2s + 32 * kRow;
+    R* dos = d1s + 32 * kRow;
 
-    const float inv_n = 1.f / (float)n;
-    float gW2[kMlpHid], gW1[kMlpIn];
+    const R inv_n = R(1) / (R)n;
+    R gW2[kMlpHid], gW1[kMlpIn];
 #pragma unroll
-    for (int i = 0; i < kMlpHid; i++) gW2[i] = 0.f;
+    for (int i = 0; i < kMlpHid; i++) gW2[i] = R(0);
 #pragma unroll
-    for (int i = 0; i < kMlpIn; i++) gW1[i] = 0.f;
-    float gb2 = 0.f, gb1 = 0.f, gw3 = 0.f, gb3 = 0.f, loss = 0.f;
+    for (int i = 0; i < kMlpIn; i++) gW1[i] = R(0);
+    R gb2 = 0, gb1 = 0, gw3 = 0, gb3 = 0, loss = 0;
 
     const int nchunks = (n + 31) / 32;
     for (int c = blockIdx.x * kWarps + warp; c < nchunks; c += gridDim.x * kWarps) {
         // ---- phase A: one sample per lane ----------------------------------
         const int s = c * 32 + lane;
-        float x[kMlpIn], h1[kMlpHid], h2[kMlpHid];
-        float dout = 0.f;
+        R x[kMlpIn], h1[kMlpHid], h2[kMlpHid];
+        R dout = 0;
         if (s < n) {
 #pragma unroll
             for (int i = 0; i < kMlpIn; i++) x[i] = X[(size_t)s * kMlpIn + i];
         } else {
 #pragma unroll
-            for (int i = 0; i < kMlpIn; i++) x[i] = 0.f;
+            for (int i = 0; i < kMlpIn; i++) x[i] = 0;
         }
 #pragma unroll
         for (int j = 0; j < kMlpHid; j++) {
-            float a = ws[kMlpB1 + j];
+            R a = ws[kMlpB1 + j];
 #pragma unroll
             for (int i = 0; i < kMlpIn; i++) a += ws[kMlpW1 + j * kMlpIn + i] * x[i];
-            h1[j] = tanhf(a);
+            h1[j] = acc_tanh(a);
         }
-        float z = ws[kMlpB3];
+        R z = ws[kMlpB3];
 #pragma unroll
         for (int j = 0; j < kMlpHid; j++) {
-            float a = ws[kMlpB2 + j];
+            R a = ws[kMlpB2 + j];
 #pragma unroll
             for (int i = 0; i < kMlpHid; i++) a += ws[kMlpW2 + j * kMlpHid + i] * h1[i];
-            h2[j] = tanhf(a);
+            h2[j] = acc_tanh(a);
             z += ws[kMlpW3 + j] * h2[j];
         }
         if (s < n) {
-            const float r = softplus(z) - Y[s];
-            loss += r * r;
-            dout = 2.f * r * sigmoidf(z) * inv_n;
+            if (UP) {
+                dout = Y[s] * sigm(z);
+            } else {
+                const R r = softplus(z) - Y[s];
+                loss += r * r;
+                dout = R(2) * r * sigm(z) * inv_n;
+            }
         }
         // deltas: d2 = dout w3 (1 - h2^2); d1 = (W2^T d2) (1 - h1^2)
-        float d2[kMlpHid];
+        R d2[kMlpHid];
 #pragma unroll
-        for (int j = 0; j < kMlpHid; j++) d2[j] = dout * ws[kMlpW3 + j] * (1.f - h2[j] * h2[j]);
+        for (int j = 0; j < kMlpHid; j++) d2[j] = dout * ws[kMlpW3 + j] * (R(1) - h2[j] * h2[j]);
         __syncwarp();
 #pragma unroll
         for (int i = 0; i < kMlpIn; i++) xs[lane * kXRow + i] = x[i];
 #pragma unroll
         for (int i = 0; i < kMlpHid; i++) {
-            float g = 0.f;
+            R g = 0;
 #pragma unroll
             for (int j = 0; j < kMlpHid; j++) g += ws[kMlpW2 + j * kMlpHid + i] * d2[j];
-            d1s[lane * kRow + i] = g * (1.f - h1[i] * h1[i]);
+            d1s[lane * kRow + i] = g * (R(1) - h1[i] * h1[i]);
             h1s[lane * kRow + i] = h1[i];
             h2s[lane * kRow + i] = h2[i];
             d2s[lane * kRow + i] = d2[i];
@@ -116,7 +132,7 @@ __global__ void __launch_bounds__(kThreads) mlp_grad_kernel(const float* __restr
         // ---- phase B: lane j accumulates row j over the 32 samples --------
         const int j = lane;
         for (int q = 0; q < 32; q++) {
-            const float dj2 = d2s[q * kRow + j], dj1 = d1s[q * kRow + j], dq = dos[q];
+            const R dj2 = d2s[q * kRow + j], dj1 = d1s[q * kRow + j], dq = dos[q];
 #pragma unroll
             for (int i = 0; i < kMlpHid; i++) gW2[i] += dj2 * h1s[q * kRow + i];
             gb2 += dj2;
@@ -130,11 +146,11 @@ __global__ void __launch_bounds__(kThreads) mlp_grad_kernel(const float* __restr
     }
     // ---- warp partials -> block partial (fixed order) -----------------------
     // the staging area is reused: warp w's gradient at sm[w * kPartial ...]
-    float lsum = loss;
+    R lsum = loss;
 #pragma unroll
     for (int o = 16; o; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
     __syncthreads();
-    float* g = sm + warp * kPartial;
+    R* g = sm + warp * kPartial;
     {
         const int j = lane;
 #pragma unroll
@@ -151,20 +167,23 @@ __global__ void __launch_bounds__(kThreads) mlp_grad_kernel(const float* __restr
     }
     __syncthreads();
     for (int p = tid; p < kPartial; p += kThreads) {
-        float v = 0.f;
+        R v = 0;
         for (int w = 0; w < kWarps; w++) v += sm[w * kPartial + p];
         part[(size_t)blockIdx.x * kPartial + p] = v;
     }
 }
 
-__global__ void mlp_reduce_kernel(const float* __restrict__ part, int nblocks, float* __restrict__ grad,
-                                  float* __restrict__ loss)
+// block partials summed in block order; ACC adds into grad instead of
+// overwriting it
+template <typename R, bool ACC>
+__global__ void mlp_reduce_kernel(const R* __restrict__ part, int nblocks, R* __restrict__ grad,
+                                  R* __restrict__ loss)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= kPartial) return;
-    float v = 0.f;
+    R v = 0;
     for (int b = 0; b < nblocks; b++) v += part[(size_t)b * kPartial + p];
-    if (p < kMlpParams) grad[p] = v;
+    if (p < kMlpParams) grad[p] = ACC ? grad[p] + v : v;
     else if (loss) *loss = v;
 }
 
@@ -214,8 +233,30 @@ __global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restric
 }
 
 bool g_grad_attr = false;
+bool g_grad_attr64 = false;
 
 }  // namespace
+
+namespace ippi {
+
+size_t mlp_grad_f64_partial_doubles() { return (size_t)IPPI_MLP_GRAD_BLOCKS * kPartial; }
+
+cudaError_t mlp_grad_upstream_f64(const double* xs, const double* up, int n, const float* w, double* part,
+                                  double* grad, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    if (!g_grad_attr64) {
+        cudaError_t e = cudaFuncSetAttribute(mlp_grad_kernel<double, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_smem<double>());
+        if (e != cudaSuccess) return e;
+        g_grad_attr64 = true;
+    }
+    mlp_grad_kernel<double, true><<<IPPI_MLP_GRAD_BLOCKS, kThreads, grad_smem<double>(), st>>>(xs, up, n, w, part);
+    mlp_reduce_kernel<double, true><<<(kPartial + 255) / 256, 256, 0, st>>>(part, IPPI_MLP_GRAD_BLOCKS, grad, nullptr);
+    return cudaGetLastError();
+}
+
+}  // namespace ippi
 
 extern "C" {
 
@@ -229,13 +270,14 @@ int ippi_mlp_grad(const float* x, const float* y, int n, const float* w, float* 
     if (!x || !y || !w || !grad || !scratch || n <= 0) return IPPI_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     if (!g_grad_attr) {
-        if (cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kGradSmem) != cudaSuccess)
+        if (cudaFuncSetAttribute(mlp_grad_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)grad_smem<float>()) != cudaSuccess)
             return IPPI_ERR_CUDA;
         g_grad_attr = true;
     }
-    mlp_grad_kernel<<<IPPI_MLP_GRAD_BLOCKS, kThreads, kGradSmem, st>>>(x, y, n, w, scratch);
-    mlp_reduce_kernel<<<(kPartial + 255) / 256, 256, 0, st>>>(scratch, IPPI_MLP_GRAD_BLOCKS, grad, loss);
+    mlp_grad_kernel<float, false><<<IPPI_MLP_GRAD_BLOCKS, kThreads, grad_smem<float>(), st>>>(x, y, n, w, scratch);
+    mlp_reduce_kernel<float, false><<<(kPartial + 255) / 256, 256, 0, st>>>(scratch, IPPI_MLP_GRAD_BLOCKS, grad,
+                                                                           loss);
     return cudaGetLastError() == cudaSuccess ? IPPI_OK : IPPI_ERR_CUDA;
 }
 

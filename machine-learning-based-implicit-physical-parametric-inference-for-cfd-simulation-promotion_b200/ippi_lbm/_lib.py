@@ -16,7 +16,7 @@ IPPI_OK, IPPI_ERR_ARG, IPPI_ERR_CUDA, IPPI_ERR_DIVERGED, IPPI_ERR_STATE, IPPI_ER
 BGK, MRT, RR = 0, 1, 2
 F64, F32, F16, BF16 = 0, 1, 2, 3
 BC_REF_NEE, BC_CHANNEL = 0, 1
-LES_NONE, LES_SMAGORINSKY, LES_LEARNED = 0, 1, 2
+LES_NONE, LES_SMAGORINSKY, LES_LEARNED, LES_FIELD = 0, 1, 2, 3
 MLP_PARAMS, MLP_STATS, MLP_GRAD_BLOCKS = 1313, 25, 296
 ABI_VERSION = 2
 DELTA_BILINEAR, DELTA_PESKIN4 = 0, 1
@@ -28,7 +28,8 @@ EXPORTS = ("ippi_abi_version", "ippi_params_default", "ippi_create", "ippi_destr
            "ippi_download", "ippi_forces", "ippi_force_history", "ippi_get_stream",
            "ippi_profile_steps", "ippi_last_error", "ippi_mass_noalloc", "ippi_load_tau_mlp",
            "ippi_filter_snapshot", "ippi_mlp_param_count", "ippi_mlp_scratch_floats", "ippi_mlp_grad",
-           "ippi_mlp_adam", "ippi_mlp_forward")
+           "ippi_mlp_adam", "ippi_mlp_forward", "ippi_set_tau_field", "ippi_load_tau_mlp_f32",
+           "ippi_adjoint_forward", "ippi_adjoint_backward")
 
 
 class Params(C.Structure):
@@ -90,6 +91,11 @@ def lib() -> C.CDLL:
         L.ippi_mlp_adam.argtypes = [_vp, _vp, _vp, _vp, C.c_int, C.c_float, C.c_float, C.c_float,
                                     C.c_float, _vp]
         L.ippi_mlp_forward.argtypes = [_vp, C.c_int, _vp, _vp, _vp]
+        L.ippi_set_tau_field.argtypes = [C.c_void_p, _dp]
+        L.ippi_load_tau_mlp_f32.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_size_t,
+                                            C.POINTER(C.c_float), C.c_size_t]
+        L.ippi_adjoint_forward.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.ippi_adjoint_backward.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
         _lib = L
     return _lib
 

@@ -125,6 +125,42 @@ class Lattice:
         L.check(L.lib().ippi_load_tau_mlp(self._h, w.ctypes.data_as(C.POINTER(C.c_uint16)), w.size,
                                           st.ctypes.data_as(C.POINTER(C.c_float)), st.size), self._h)
 
+    def load_tau_mlp_f32(self, w, stats):
+        """Learned tau with FP32 weights used as given (no BF16 rounding)."""
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        st = np.ascontiguousarray(stats, dtype=np.float32)
+        L.check(L.lib().ippi_load_tau_mlp_f32(self._h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size,
+                                              st.ctypes.data_as(C.POINTER(C.c_float)), st.size), self._h)
+
+    def set_tau_field(self, tau):
+        """Relaxation time per node [ny][nx] for les_model = LES_FIELD."""
+        tau = _f64(tau, self.nx * self.ny)
+        L.check(L.lib().ippi_set_tau_field(self._h, _p(tau)), self._h)
+
+    def adjoint_forward(self, nsteps, t0=1, ckpt_every=64):
+        """Advance nsteps steps, recording checkpoints for adjoint_backward."""
+        L.check(L.lib().ippi_adjoint_forward(self._h, nsteps, t0, ckpt_every), self._h)
+
+    def adjoint_backward(self, dl_dforce=None, dl_dmacro=None, tau=False, mlp=False, f0=False):
+        """Gradients of the loss with partial derivatives dl_dforce
+        [nsteps][nbody][2] and dl_dmacro [3][ny][nx] (final post-stream rho,
+        ux, uy): dict with 'tau' [ny][nx], 'mlp' [1313], 'f0' [9][ny][nx]."""
+        nn = self.nx * self.ny
+        dF = None if dl_dforce is None else _f64(dl_dforce)
+        dM = None if dl_dmacro is None else _f64(dl_dmacro, 3 * nn)
+        out = {}
+        gt = np.zeros((self.ny, self.nx)) if tau else None
+        gm = np.zeros(L.MLP_PARAMS) if mlp else None
+        gf = np.zeros((9, self.ny, self.nx)) if f0 else None
+        L.check(L.lib().ippi_adjoint_backward(self._h, _p(dF), _p(dM), _p(gt), _p(gm), _p(gf)), self._h)
+        if tau:
+            out["tau"] = gt
+        if mlp:
+            out["mlp"] = gm
+        if f0:
+            out["f0"] = gf
+        return out
+
     def filter_snapshot(self, factor):
         """Box-filtered state [6][ny/f][nx/f]: rho, ux, uy (density-weighted),
         effective stress Sxx, Sxy, Syy (include/ippi_lbm.h)."""

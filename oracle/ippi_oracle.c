@@ -51,6 +51,7 @@ struct orc {
     double mass;
     double mrt_tm[9][9], mrt_tminv[9][9];
     double mlp[1313 + 25];      /* learned tau network (les_model 2) */
+    double* tau_field;          /* les_model 3: tau per node, [ny][nx] global */
     int mlp_loaded;
 };
 
@@ -193,6 +194,14 @@ double orc_learned_tau(const double* fnew, double rho, double ux, double uy,
     }
     double sp = (z > 0 ? z : 0.0) + log1p(exp(-fabs(z)));
     return tau0 + st[24] * sp;
+}
+
+int orc_set_tau_field(orc* s, const double* tau)
+{
+    size_t n = (size_t)s->p.nx * s->p.ny;
+    if (!s->tau_field) s->tau_field = (double*)malloc(n * sizeof(double));
+    memcpy(s->tau_field, tau, n * sizeof(double));
+    return 0;
 }
 
 int orc_load_tau_mlp(orc* s, const float* w, size_t n, const float* stats, size_t nstats)
@@ -539,6 +548,7 @@ void orc_destroy(orc* s)
     free(s->tau); free(s->fxn); free(s->fyn); free(s->avg_u); free(s->avg_v);
     free(s->avg_rho); free(s->nnflag); free(s->style); free(s->mk);
     free(s->body_force);
+    free(s->tau_field);
     for (int t = 0; t < 8; t++) free(s->nets[t].w);
     free(s);
 }
@@ -792,7 +802,9 @@ static int collide_all(orc* s)
             double fn[9], fc[9];
             for (int k = 0; k < 9; k++) fn[k] = FN(s, k, i, j);
             int use_les = s->p.les_model == 1 && !(coll == COLL_BGK && s->nnflag[id]);
-            if (s->p.les_model == 2)
+            if (s->p.les_model == 3 && !(coll == COLL_BGK && s->nnflag[id]))
+                s->tau[id] = s->tau_field[(size_t)j * s->p.nx + (i - 1)];
+            else if (s->p.les_model == 2)
                 s->tau[id] = orc_learned_tau(fn, r, s->ux[id], s->uy[id], s->p.tau0, s->p.cs, s->mlp);
             else if (use_les)
                 s->tau[id] = orc_les_tau(fn, r, s->ux[id], s->uy[id], s->p.tau0, s->p.cs);
@@ -976,6 +988,7 @@ int orc_step(orc* s, int nsteps, int t0)
 {
     int status = 0;
     if (s->p.les_model == 2 && !s->mlp_loaded) return -1;
+    if (s->p.les_model == 3 && !s->tau_field) return -1;
     for (int t = t0; t < t0 + nsteps; t++) {
         ib_substep(s);
         if (s->p.collision == COLL_BGK) nn_band(s);
@@ -1026,6 +1039,8 @@ static void next_tau(orc* s, double* tau_out, unsigned char* flag_out)
             int nnf = (s->p.collision == COLL_BGK) && s->nnflag[id];
             if (nnf)
                 t = s->tau[id];
+            else if (s->p.les_model == 3)
+                t = s->tau_field[(size_t)j * s->p.nx + (i - 1)];
             else if (s->p.les_model == 2)
                 t = orc_learned_tau(fn, s->rho[id], s->ux[id], s->uy[id], s->p.tau0, s->p.cs, s->mlp);
             else if (s->p.les_model == 1)

@@ -47,7 +47,8 @@ typedef struct {
     int nx, ny;          /* global lattice (reference Nx, Ny)                    */
     int collision;       /* 0 BGK, 1 MRT, 2 RR                                   */
     int bc_set;          /* 0 reference flat plate (NEE), 1 channel (ZH/ZG/BB)   */
-    int les_model;       /* 0 constant tau0, 1 Smagorinsky "hybrid", 2 learned    */
+    int les_model;       /* 0 constant tau0, 1 Smagorinsky "hybrid", 2 learned,
+                            3 given tau per node (orc_set_tau_field)            */
     double tau0;         /* startTau                                              */
     double cs;           /* Smagorinsky constant                                 */
     double u_in;         /* inlet velocity (flat plate) / u_max (channel)         */
@@ -110,6 +111,8 @@ void orc_force_node(int collision, double ux, double uy, double fx, double fy, d
  * W2[32][32] b2[32] w3[32] b3) and stats[25] (mean[6] std[6] lo[6] hi[6]
  * out_scale).  Returns 0, or -1 on a bad size. */
 int orc_load_tau_mlp(orc* s, const float* w, size_t n, const float* stats, size_t nstats);
+/* tau per node for les_model 3: [ny][nx] global. */
+int orc_set_tau_field(orc* s, const double* tau);
 /* tau0 + out_scale * softplus(MLP(features)), Smagorinsky outside [lo, hi];
  * p = the 1338 parameters + statistics as doubles */
 double orc_learned_tau(const double* fnew, double rho, double ux, double uy,

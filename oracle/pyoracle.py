@@ -73,6 +73,7 @@ def lib() -> C.CDLL:
                                        C.c_double, _dp]
         L.orc_les_tau.restype = C.c_double
         L.orc_les_tau.argtypes = [_dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.orc_set_tau_field.argtypes = [C.c_void_p, _dp]
         L.orc_force_node.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                      C.c_double, C.c_double, _dp]
         L.orc_load_tau_mlp.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_size_t,
@@ -139,6 +140,10 @@ class Oracle:
         st = np.ascontiguousarray(stats, dtype=np.float32)
         if lib().orc_load_tau_mlp(self._h, _ptr(w, C.c_float), w.size, _ptr(st, C.c_float), st.size):
             raise ValueError("bad tau network")
+
+    def set_tau_field(self, tau):
+        tau = np.ascontiguousarray(tau, dtype=np.float64)
+        lib().orc_set_tau_field(self._h, _ptr(tau))
 
     def step(self, n, t0=1):
         return lib().orc_step(self._h, n, t0)
