@@ -349,7 +349,8 @@ def run_learned(a):
 
     rank, local, world = env_rank()
     torch.cuda.set_device(local)
-    r = lt.experiment(fine_steps=a.learned_steps, avg_steps=a.learned_steps * 2 // 5, device=local)
+    r = lt.experiment(fine_steps=a.learned_steps, avg_steps=a.learned_steps * 2 // 5, device=local,
+                      finetune_iters=a.learned_finetune)
     r.pop("net")
     if rank != 0:
         return
@@ -369,6 +370,84 @@ def run_learned(a):
         "wall_s": {"fine": r["fine"]["wall_s"], "coarse_plain": r["coarse_plain"]["wall_s"],
                    "coarse_learned": r["coarse_learned"]["wall_s"]},
         "training": r["training"],
+        "through_solver": None if r["coarse_learned_through_solver"] is None else {
+            k: v for k, v in r["coarse_learned_through_solver"].items() if k != "history"},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_adjoint(a):
+    """Forward + backward throughput of the adjoint on the 1024 x 256 MRT
+    lattice with the per-node learned tau (a seeded Xavier network), a
+    4,000-step rollout checkpointed every 64 steps, FP32 forward; gradient
+    with respect to the network weights.  The gradient is checked in FP64
+    (FP64 forward on the same lattice) by central differences (eps 1e-3,
+    Richardson-combined with eps 5e-4) along seeded random directions, over
+    --adjoint-check-steps steps: the Re 3900 wake is chaotic, so over
+    thousands of steps finite differences and the tangent gradient part ways
+    (the reported errors at two horizons show it)."""
+    import numpy as np
+    import torch
+
+    import ippi_lbm as ip
+    from ippi_lbm import learned_tau as lt
+    from ippi_lbm import scenes
+
+    rank, local, world = env_rank()
+    torch.cuda.set_device(local)
+    nsteps, K = a.adjoint_steps, 64
+    sc = scenes.cylinder_channel(1024, 256, 32, 256, 128, 0.04, 3900, collision=ip.MRT)
+    params = dict(sc["params"], les_model=ip.LES_LEARNED)
+    w = lt.xavier(0).astype(np.float32)
+    stats = np.concatenate([[1.0, 0.04, 0, 0, 0, 1e-3], [2e-3, 0.02, 0.5, 0.5, 0.5, 1e-3],
+                            [0.9, 0.0, -1, -1, -1, 0.0], [1.1, 0.2, 1, 1, 1, 0.1],
+                            [1e-3]]).astype(np.float32)
+    rng = np.random.default_rng(0)
+    wF = rng.normal(0, 1, (nsteps, 1, 2))
+
+    def run(wv, n, weights, grads=False, storage=ip.F32):
+        lat = ip.Lattice(1024, 256, device=local, **dict(params, storage=storage))
+        lat.init_macros(*sc["init"])
+        lat.set_markers(sc["markers"], ds=sc["ds"])
+        lat.load_tau_mlp_f32(wv, stats)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lat.adjoint_forward(n, 1, K)
+        t1 = time.perf_counter()
+        F = lat.force_history(n)
+        g = lat.adjoint_backward(dl_dforce=weights, mlp=True) if grads else None
+        t2 = time.perf_counter()
+        lat.close()
+        return float(np.sum(weights * F)), g, t1 - t0, t2 - t1
+
+    run(w, nsteps, wF, grads=True)  # warm-up (allocations, graphs)
+    _, g, tf, tb = run(w, nsteps, wF, grads=True)
+    checks = {}
+    for hn in sorted({a.adjoint_check_steps, nsteps}):
+        wc = rng.normal(0, 1, (hn, 1, 2))
+        _, gc, _, _ = run(w, hn, wc, grads=True, storage=ip.F64)
+        errs = []
+        for _ in range(a.adjoint_dirs):
+            d = rng.normal(0, 1, w.size)
+            dl, ad = [], []
+            for eps in (1e-3, 5e-4):
+                wp, wm = (w + eps * d).astype(np.float32), (w - eps * d).astype(np.float32)
+                dl.append(run(wp, hn, wc, storage=ip.F64)[0] - run(wm, hn, wc, storage=ip.F64)[0])
+                ad.append(float(gc["mlp"] @ (wp.astype(np.float64) - wm.astype(np.float64))))
+            fd, want = 8 * dl[1] - dl[0], 8 * ad[1] - ad[0]
+            errs.append(float(f"{abs(fd - want) / max(abs(fd), 1e-30):.3g}"))
+        checks[str(hn)] = errs
+    if rank != 0:
+        return
+    line = {
+        "metric": "adjoint_forward_backward_steps_per_s", "value": round(nsteps / (tf + tb), 1),
+        "unit": "steps/s", "higher_is_better": True, "n_gpus": 1, "dtype": "f32 forward, f64 adjoint",
+        "data": "synthetic",
+        "config": {"workload": "channel_cylinder_1024x256_mrt_learned_tau_adjoint", "nx": 1024, "ny": 256,
+                   "rollout_steps": nsteps, "checkpoint_every": K, "gradient": "network weights (1313)"},
+        "forward_s": round(tf, 3), "backward_s": round(tb, 3),
+        "mlups_forward_backward": round(1024 * 256 * nsteps / (tf + tb) / 1e6, 1),
+        "fd_check_fp64_rel_err_by_steps": checks,
     }
     print(json.dumps(line), flush=True)
 
@@ -384,6 +463,13 @@ def main():
     ap.add_argument("--learned", action="store_true",
                     help="learned-tau time-to-solution comparison instead of the MLUPS line")
     ap.add_argument("--learned-steps", type=int, default=160000)
+    ap.add_argument("--learned-finetune", type=int, default=0,
+                    help="iterations of training through the solver (adjoint) after the a-priori fit")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="adjoint forward+backward throughput and gradient check instead of the MLUPS line")
+    ap.add_argument("--adjoint-steps", type=int, default=4000)
+    ap.add_argument("--adjoint-dirs", type=int, default=2)
+    ap.add_argument("--adjoint-check-steps", type=int, default=400)
     ap.add_argument("--ncu-case", action="store_true",
                     help="short run of single launches for an ncu capture")
     a = ap.parse_args()
@@ -391,6 +477,8 @@ def main():
         run_ncu_case(a)
     elif a.learned:
         run_learned(a)
+    elif a.adjoint:
+        run_adjoint(a)
     elif a.impl == "reference":
         run_reference_arm(a)
     else:

@@ -256,7 +256,7 @@ def strouhal(cl, d, u):
 # ---------------------------------------------------------------------------
 def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=160000,
                avg_steps=64000, n_snap=200, max_samples=2_000_000, epochs=30, seed=0, device=0,
-               log=None):
+               finetune_iters=0, finetune_lr=2e-3, log=None):
     """Fine lattice (plain Smagorinsky MRT, FP32) -> `n_snap` filtered
     snapshots over its averaging window -> training -> the coarse lattice
     (nx/factor x ny/factor, same Re and Mach) with plain Smagorinsky and with
@@ -291,6 +291,18 @@ def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=
     rp = run_cylinder(coarse, csteps, cfirst, device=device)
     rl = run_cylinder(coarse, csteps, cfirst, net=net, device=device)
     say(f"coarse plain: Cd {rp['cd']:.5f}; learned: Cd {rl['cd']:.5f}")
+    tuned = None
+    if finetune_iters:
+        t1 = time.perf_counter()
+        net_ft, ft_hist = train_through_solver(net, coarse, rf["cd"], iters=finetune_iters,
+                                               spinup=cfirst - 1, lr=finetune_lr, device=device, log=log)
+        ft_s = time.perf_counter() - t1
+        rt = run_cylinder(coarse, csteps, cfirst, net=net_ft, device=device)
+        say(f"coarse learned + through-solver training: Cd {rt['cd']:.5f}")
+        tuned = dict(cd=rt["cd"], st=rt["st"], wall_s=rt["wall_s"],
+                     cd_rel_err=abs(rt["cd"] - rf["cd"]) / abs(rf["cd"]), iters=finetune_iters,
+                     train_seconds=ft_s, history=ft_hist)
+        net = net_ft
 
     def err(r):
         return abs(r["cd"] - rf["cd"]) / abs(rf["cd"])
@@ -304,5 +316,59 @@ def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=
                             cd_rel_err=err(rl)),
         training=dict(samples=int(x.shape[0]), epochs=epochs, loss_first=hist[0], loss_last=hist[-1],
                       seconds=train_s),
+        coarse_learned_through_solver=tuned,
         speedup_vs_fine=rf["wall_s"] / rl["wall_s"],
         net=net)
+
+
+# ---------------------------------------------------------------------------
+# end-to-end training through the solver (adjoint)
+# ---------------------------------------------------------------------------
+def train_through_solver(net, sc, cd_ref, iters=8, nsteps=4000, ckpt=64, spinup=12000, lr=2e-3,
+                         device=0, log=None):
+    """Fine-tune the network so that the coarse lattice's mean drag over an
+    nsteps window (after `spinup` steps) matches cd_ref.  Loss
+    ((<Cd> - cd_ref) / cd_ref)^2; its gradient with respect to the FP32
+    weights comes from the adjoint (NetworkRollout), the update from the
+    library's Adam kernel.  Returns (net with new weights, history)."""
+    import torch
+
+    from .autograd import NetworkRollout, Rollout
+    from .lattice import Lattice
+
+    params = dict(sc["params"], les_model=L.LES_LEARNED)
+    lat = Lattice(sc["nx"], sc["ny"], device=device, **params)
+    lat.set_markers(sc["markers"], ds=sc["ds"])
+    stats = net.stats()
+    dev = torch.device("cuda", device)
+    wd = torch.from_numpy(net.w.astype(np.float32)).to(dev)
+    md, vd, gd = torch.zeros_like(wd), torch.zeros_like(wd), torch.zeros_like(wd)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    lib = L.lib()
+
+    def reset(lt_):
+        lt_.init_macros(*sc["init"])
+        lt_.load_tau_mlp_f32(wd.cpu().numpy(), stats)
+        lt_.step(spinup, 1)
+
+    roll = Rollout(lat, reset, nsteps, spinup + 1, ckpt, stats)
+    q = 0.5 * sc["u_ref"] ** 2 * sc["d"]
+    hist = []
+    for it in range(iters):
+        w = wd.cpu().clone().requires_grad_(True)
+        t0 = time.perf_counter()
+        forces, _ = NetworkRollout.apply(w, roll)
+        cd = forces[:, 0, 0].mean() / q
+        loss = ((cd - cd_ref) / cd_ref) ** 2
+        loss.backward()
+        gd.copy_(w.grad.float())
+        L.check(lib.ippi_mlp_adam(wd.data_ptr(), gd.data_ptr(), md.data_ptr(), vd.data_ptr(), it + 1, lr,
+                                  0.9, 0.999, 1e-8, stream))
+        torch.cuda.synchronize(dev)
+        hist.append(dict(cd=float(cd.detach()), loss=float(loss.detach()), seconds=time.perf_counter() - t0))
+        if log:
+            log(f"through-solver {it}: Cd {hist[-1]['cd']:.5f} loss {hist[-1]['loss']:.4g} "
+                f"({hist[-1]['seconds']:.1f} s)")
+    lat.close()
+    out = TauNet(wd.cpu().numpy(), net.mean, net.std, net.lo, net.hi, net.out_scale)
+    return out, hist
