@@ -452,6 +452,24 @@ def run_adjoint(a):
     print(json.dumps(line), flush=True)
 
 
+def run_validate(a):
+    """Precision studies: config 2 (FP32 vs FP64, MRT and RR, 4096 x 1024,
+    Cd / St / mean-velocity L2) and config 3 (16384 x 4096, 64 cylinders,
+    FP32 / FP16 / BF16 vs FP64: per-cylinder Cd, mean-velocity L2, mass
+    drift)."""
+    import torch
+
+    from ippi_lbm import validation as val
+
+    rank, local, world = env_rank()
+    torch.cuda.set_device(local)
+    log = (lambda s_: print(s_, file=sys.stderr, flush=True))
+    c2 = val.config2_precision(steps=a.validate_steps2, avg=a.validate_steps2 * 2 // 5, log=log)
+    c3 = val.config3_precision(steps=a.validate_steps3, avg=a.validate_steps3 // 2, log=log)
+    if rank == 0:
+        print(json.dumps({"metric": "precision_study", "config2": c2, "config3": c3}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -470,6 +488,10 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=4000)
     ap.add_argument("--adjoint-dirs", type=int, default=2)
     ap.add_argument("--adjoint-check-steps", type=int, default=400)
+    ap.add_argument("--validate", action="store_true",
+                    help="precision studies of configs 2 and 3 instead of the MLUPS line")
+    ap.add_argument("--validate-steps2", type=int, default=160000)
+    ap.add_argument("--validate-steps3", type=int, default=20000)
     ap.add_argument("--ncu-case", action="store_true",
                     help="short run of single launches for an ncu capture")
     a = ap.parse_args()
@@ -479,6 +501,8 @@ def main():
         run_learned(a)
     elif a.adjoint:
         run_adjoint(a)
+    elif a.validate:
+        run_validate(a)
     elif a.impl == "reference":
         run_reference_arm(a)
     else:

@@ -229,23 +229,23 @@ __device__ __forceinline__ void fluid_back(const AdjArgs& A, int x, int y, doubl
 {
     const StepArgs& a = A.s;
     if (x == 0) {
-        const double u = inlet_profile<double>(y, a.ny, a.u_in);
-        // f1 = f3 + 2/3 r u; f5 = f7 - (f2 - f4)/2 + r u / 6; f8 = f6 + (f2 - f4)/2 + r u / 6
-        // r = sk / (1 - u), sk = f0 + f2 + f4 + 2 (f3 + f6 + f7)
-        const double lr = (2.0 / 3.0) * u * lam[1] + (1.0 / 6.0) * u * (lam[5] + lam[8]);
-        lam[3] += lam[1];
-        lam[7] += lam[5];
-        lam[6] += lam[8];
-        lam[2] += 0.5 * (lam[8] - lam[5]);
-        lam[4] += 0.5 * (lam[5] - lam[8]);
-        const double ls = lr / (1.0 - u);
-        lam[0] += ls;
-        lam[2] += ls;
-        lam[4] += ls;
-        lam[3] += 2.0 * ls;
-        lam[6] += 2.0 * ls;
-        lam[7] += 2.0 * ls;
-        lam[1] = lam[5] = lam[8] = 0.0;
+        // the regularised Zou-He inlet is linear in the pulled populations:
+        // its Jacobian from one dual evaluation, transposed onto lam
+        using D9 = Dual<9>;
+        D9 g[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) g[k] = D9::seed(0.0, k);
+        zh_inlet<D9>(g, D9(inlet_profile<double>(y, a.ny, a.u_in)), D9(0.0));
+        double lp[9];
+#pragma unroll
+        for (int j = 0; j < 9; j++) {
+            double v = 0.0;
+#pragma unroll
+            for (int k = 0; k < 9; k++) v += lam[k] * g[k].d[j];
+            lp[j] = v;
+        }
+#pragma unroll
+        for (int k = 0; k < 9; k++) lam[k] = lp[k];
     }
     scatter_pull(A, x, y, lam);
 }

@@ -1,0 +1,136 @@
+"""Precision studies of the benchmark configurations on the GPU.
+
+config2_precision  4096 x 1024, D = 128, Re 3900, MRT and RR + Smagorinsky:
+                   FP32 against an FP64 run of the same (mean Cd / Cl, St,
+                   L2 of the time-averaged velocity field).
+config3_precision  16384 x 4096 (67 M nodes), 64 seeded cylinders D = 48
+                   (non-overlapping, gap >= 2 D), Re 1000, MRT + Smagorinsky:
+                   FP32 / FP16 / BF16 storage against FP64 (per-cylinder mean
+                   Cd, time-averaged velocity L2, mass drift).
+The FP64 GPU path is the reference here: it is pinned to the FP64 CPU oracle
+bit-for-bit-close (1e-11) by the parity tests, and unlike the CPU oracle it
+runs the full lattices.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+
+from . import _lib as L
+from . import scenes
+from .lattice import Lattice
+from .learned_tau import strouhal
+
+
+def _run(nx, ny, params, init, markers, ds, bodies, steps, avg_from, chunk=4000):
+    lat = Lattice(nx, ny, **dict(params, avg_start=avg_from))
+    lat.init_macros(*init)
+    lat.set_markers(markers, ds=ds, body=bodies)
+    _, m0 = lat.forces(with_mass=True)
+    nb = int(bodies.max()) + 1 if bodies is not None else 1
+    forces = np.zeros((steps, nb, 2))
+    t = 1
+    t0 = time.perf_counter()
+    while t <= steps:
+        n = min(chunk, steps - t + 1)
+        lat.step(n, t)
+        forces[t - 1:t - 1 + n] = lat.force_history(n)
+        t += n
+    wall = time.perf_counter() - t0
+    _, m1 = lat.forces(with_mass=True)
+    avg = np.stack([lat.download(L.FIELD_AVG_U), lat.download(L.FIELD_AVG_V)])
+    lat.close()
+    return dict(forces=forces, mass0=m0, mass1=m1, avg=avg, wall_s=wall)
+
+
+def _l2(a, b):
+    return float(np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)))
+
+
+def config2_precision(steps=160000, avg=64000, collisions=(L.MRT, L.RR), log=None):
+    out = {}
+    for coll in collisions:
+        runs = {}
+        for st, name in ((L.F64, "f64"), (L.F32, "f32")):
+            sc = scenes.config2(collision=coll, storage=st)
+            r = _run(sc["nx"], sc["ny"], sc["params"], sc["init"], sc["markers"], sc["ds"], None,
+                     steps, steps - avg + 1)
+            q = 0.5 * sc["u_ref"] ** 2 * sc["d"]
+            f = r["forces"][steps - avg:, 0] / q
+            runs[name] = dict(cd=float(f[:, 0].mean()), cl=float(f[:, 1].mean()),
+                              st=strouhal(f[:, 1], sc["d"], sc["u_ref"]), avg=r["avg"], wall_s=r["wall_s"])
+            if log:
+                log(f"config2 {'MRT' if coll == L.MRT else 'RR'} {name}: Cd {runs[name]['cd']:.5f} "
+                    f"St {runs[name]['st']:.4f} ({r['wall_s']:.1f} s)")
+        a, b = runs["f32"], runs["f64"]
+        out["MRT" if coll == L.MRT else "RR"] = dict(
+            cd_f64=b["cd"], cd_f32=a["cd"], cd_rel_err=abs(a["cd"] - b["cd"]) / abs(b["cd"]),
+            cl_f64=b["cl"], cl_f32=a["cl"], st_f64=b["st"], st_f32=a["st"],
+            mean_velocity_l2=_l2(a["avg"], b["avg"]), wall_s_f64=b["wall_s"], wall_s_f32=a["wall_s"])
+    return out
+
+
+def seeded_cylinders(nx, ny, d, n, gap, seed=0, margin=None):
+    """n non-overlapping cylinder centres (centre distance >= d + gap), at
+    least `margin` from the lattice edges (default 2 d) and from the inlet
+    and outlet (3 d)."""
+    rng = np.random.default_rng(seed)
+    margin = 2 * d if margin is None else margin
+    pts = []
+    tries = 0
+    while len(pts) < n:
+        tries += 1
+        if tries > 100000:
+            raise RuntimeError("could not place the cylinders")
+        c = (rng.uniform(3 * d, nx - 3 * d), rng.uniform(margin, ny - margin))
+        if all(math.hypot(c[0] - p[0], c[1] - p[1]) >= d + gap for p in pts):
+            pts.append(c)
+    return np.array(pts)
+
+
+def config3_scene(nx=16384, ny=4096, d=48, n=64, re=1000.0, u=0.04, seed=0, collision=L.MRT,
+                  storage=L.F32):
+    centres = seeded_cylinders(nx, ny, d, n, 2 * d, seed)
+    sc = scenes.cylinder_channel(nx, ny, d, centres[0, 0], centres[0, 1], u, re, collision=collision,
+                                 storage=storage, seed=seed)
+    xs, dss, bodies = [], [], []
+    for b, (cx, cy) in enumerate(centres):
+        xy, ds = scenes.cylinder_markers(cx, cy, d)
+        xs.append(xy)
+        dss.append(ds)
+        bodies.append(np.full(len(ds), b, dtype=np.int32))
+    sc.update(markers=np.concatenate(xs), ds=np.concatenate(dss), bodies=np.concatenate(bodies),
+              centres=centres)
+    return sc
+
+
+def config3_precision(nx=16384, ny=4096, steps=20000, avg=10000, storages=("f64", "f32", "f16", "bf16"),
+                      log=None):
+    st_of = {"f64": L.F64, "f32": L.F32, "f16": L.F16, "bf16": L.BF16}
+    runs = {}
+    for name in storages:
+        sc = config3_scene(nx, ny, storage=st_of[name])
+        r = _run(nx, ny, sc["params"], sc["init"], sc["markers"], sc["ds"], sc["bodies"], steps,
+                 steps - avg + 1)
+        q = 0.5 * sc["u_ref"] ** 2 * sc["d"]
+        cd = r["forces"][steps - avg:, :, 0].mean(0) / q
+        runs[name] = dict(cd=cd, avg=r["avg"], mass_drift=(r["mass1"] - r["mass0"]) / r["mass0"],
+                          wall_s=r["wall_s"])
+        if log:
+            log(f"config3 {name}: mean Cd {cd.mean():.5f}, mass drift {runs[name]['mass_drift']:.3e}, "
+                f"{r['wall_s']:.1f} s")
+    ref = runs["f64"]
+    out = dict(nx=nx, ny=ny, steps=steps, cylinders=int(len(ref["cd"])), f64_mean_cd=float(ref["cd"].mean()),
+               f64_mass_drift=ref["mass_drift"], f64_wall_s=ref["wall_s"])
+    for name in storages:
+        if name == "f64":
+            continue
+        r = runs[name]
+        rel = np.abs(r["cd"] - ref["cd"]) / np.abs(ref["cd"])
+        out[name] = dict(cd_rel_err_max=float(rel.max()), cd_rel_err_mean=float(rel.mean()),
+                         mean_velocity_l2=_l2(r["avg"], ref["avg"]), mass_drift=r["mass_drift"],
+                         wall_s=r["wall_s"],
+                         mlups=nx * ny * steps / r["wall_s"] / 1e6)
+    return out

@@ -916,7 +916,8 @@ static void boundary_ref(orc* s)
 }
 
 /* Channel scene (no reference code for it): pull streaming with halfway
- * bounce-back on the y walls and a parabolic Zou-He velocity inlet at x = 0;
+ * bounce-back on the y walls and a parabolic Zou-He velocity inlet at x = 0
+ * (regularised);
  * those nodes then take their moments (CalMacro).  The outlet x = nx-1 is the
  * reference's outlet (mesh.cpp:273-286): rho = rho0, u copied from x = nx-2,
  * populations by non-equilibrium extrapolation from x = nx-2. */
@@ -944,11 +945,28 @@ static void streaming_channel(orc* s)
                     f[k] = FC(s, k, sx + 1, sy);
             }
             if (x == 0) {
+                /* Zou-He density and unknowns, then the regularised
+                 * reconstruction (Latt & Chopard 2008): equilibrium at
+                 * (rho, u_in, 0) plus the second-order projection of the
+                 * non-equilibrium part.  Plain Zou-He with BGK diverges at
+                 * tau = 0.53 in a 400 x 100 channel; this form does not. */
                 double ux = inlet_profile(s, y);
                 double rho = (f[0] + f[2] + f[4] + 2.0 * (f[3] + f[6] + f[7])) / (1.0 - ux);
                 f[1] = f[3] + (2.0 / 3.0) * rho * ux;
                 f[5] = f[7] - 0.5 * (f[2] - f[4]) + (1.0 / 6.0) * rho * ux;
                 f[8] = f[6] + 0.5 * (f[2] - f[4]) + (1.0 / 6.0) * rho * ux;
+                double fe[9], pxx = 0.0, pxy = 0.0, pyy = 0.0;
+                compute_feq(rho, ux, 0.0, fe);
+                for (int k = 0; k < 9; k++) {
+                    pxx += E[k][0] * E[k][0] * (f[k] - fe[k]);
+                    pxy += E[k][0] * E[k][1] * (f[k] - fe[k]);
+                    pyy += E[k][1] * E[k][1] * (f[k] - fe[k]);
+                }
+                for (int k = 0; k < 9; k++) {
+                    double qxx = E[k][0] * E[k][0] - 1.0 / 3.0, qyy = E[k][1] * E[k][1] - 1.0 / 3.0;
+                    double qxy = E[k][0] * E[k][1];
+                    f[k] = fe[k] + 4.5 * W[k] * (qxx * pxx + 2.0 * qxy * pxy + qyy * pyy);
+                }
             }
             size_t id = ID(s, i, y);
             for (int k = 0; k < 9; k++) FN(s, k, i, y) = f[k];

@@ -165,3 +165,29 @@ def test_adjoint_argument_checks():
     g.adjoint_forward(5, 1, 2)
     with pytest.raises(ip.IppiError, match="tau-field"):
         g.adjoint_backward(tau=True)
+
+
+def test_torch_autograd_wrapper_gives_the_adjoint_gradient():
+    torch = pytest.importorskip("torch")
+    from ippi_lbm.autograd import Rollout, TauFieldRollout
+
+    nx, ny, nsteps = 64, 32, 20
+    sc, p, rng = setup(nx, ny, ip.MRT, ip.LES_FIELD, seed=3)
+    tau0 = 0.56 + smooth_field(rng, ny, nx, 0.02)
+    a, b = loss_weights(rng, nsteps, nx, ny)
+    lat = ip.Lattice(nx, ny, **p)
+    lat.set_markers(sc["markers"], ds=sc["ds"])
+
+    def reset(lt_):
+        lt_.init_macros(*sc["init"])
+        lt_.set_tau_field(tau0)
+        lt_.step(PRE, 1)
+
+    roll = Rollout(lat, reset, nsteps, PRE + 1, 7)
+    tau = torch.tensor(tau0, dtype=torch.float64, requires_grad=True)
+    forces, macros = TauFieldRollout.apply(tau, roll)
+    loss = (forces * torch.from_numpy(a)).sum() + (macros * torch.from_numpy(b)).sum()
+    loss.backward()
+    L0, g = run_gpu(sc, p, nsteps, a, b, tau=tau0, grads=dict(tau=True))
+    assert float(loss.detach()) == pytest.approx(L0, rel=1e-12)
+    np.testing.assert_allclose(tau.grad.numpy(), g["tau"], rtol=1e-10, atol=1e-14)
