@@ -214,10 +214,10 @@ def run_ours(a):
 
     sc = ip.scenes.config2()
     lat = ip.Lattice(NX, NY, device=local, **sc["params"])
-    kernel_name = "step_kernel<F32,MRT,CHANNEL>"
-    # bulk kernel + IB chain (stencil nodes, markers + spread per direct-forcing
-    # pass, forced collision + force sums) on the side stream
-    launches_per_step = 1 + 2 + 2 * sc["params"].get("mdf_iters", 1)
+    kernel_name = "step_fast<F32,MRT,CHANNEL>"
+    # per step: the IB cluster kernel, then the bulk kernel as its
+    # programmatic dependent (one launch each)
+    launches_per_step = 2
     lat.init_macros(*sc["init"])
     lat.set_markers(sc["markers"], ds=sc["ds"])
     stream = torch.cuda.ExternalStream(lat.stream(), device=torch.device("cuda", local))
@@ -252,7 +252,14 @@ def run_ours(a):
     ms_bulk, ms_band, ms_ib = lat.profile_steps(nprof, t_next)
     t_next += nprof
     hbm, peak_kind = peaks()
-    achieved = NX * NY * BYTES_PER_NODE / (ms_bulk * 1e-3) / 1e9
+    # The bulk kernel spans the whole step: it launches as the programmatic
+    # dependent of the IB cluster and its last block waits for the cluster,
+    # so its per-launch duration in the timed graph replay is the device time
+    # per step (CUDA events on its stream over the K timed steps).  The
+    # isolated launch time from profile_steps (side-stream IB) is reported
+    # beside it.
+    ms_span = ms_max / a.steps
+    achieved = NX * NY * BYTES_PER_NODE / (ms_span * 1e-3) / 1e9
 
     # ---- end to end through the C ABI with host buffers --------------------
     # The reference's driver (main.cpp:105-120) runs OneLBMStep every step
@@ -306,8 +313,12 @@ def run_ours(a):
                          "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": NCU_TRAFFIC_BYTES,
                          "traffic_algorithmic": NX * NY * BYTES_PER_NODE,
                          "peak_source": peak_kind, "kernel": kernel_name,
-                         "kernel_ms": round(ms_bulk, 5), "band_ms": round(ms_band, 5),
-                         "ib_ms": round(ms_ib, 5), "bytes_per_node": BYTES_PER_NODE},
+                         "kernel_ms": round(ms_span, 5),
+                         "kernel_ms_basis": "bulk kernel span per step in the timed graph replay "
+                                            "(IB cluster overlapped inside it)",
+                         "kernel_ms_isolated_launch": round(ms_bulk, 5),
+                         "ib_ms_side_stream": round(ms_ib, 5), "band_ms": round(ms_band, 5),
+                         "bytes_per_node": BYTES_PER_NODE},
             "e2e": {"value": round(e2e, 1), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d),
                     "d2h_bytes_per_step": round(d2h), "steps": n_e2e},
             "gpu_launches": a.steps * launches_per_step,

@@ -393,7 +393,7 @@ int rebuild(ippi_lbm* h)
     }
 
     // slots in row-major order; boundary-net nodes (inputs and band) are
-    // prep nodes, IB stencil nodes are computed by ib_nodes itself
+    // prep nodes, IB stencil nodes are computed by the IB kernel itself
     int ns = 0;
     std::vector<PrepNode> prep;
     for (size_t i = 0; i < nn; i++)

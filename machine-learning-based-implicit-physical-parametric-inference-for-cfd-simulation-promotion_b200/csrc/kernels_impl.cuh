@@ -26,9 +26,50 @@ static void launch_prio(void (*kernel)(KArgs...), unsigned grid, unsigned block,
     cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
+template <int S, int SC, int CO, bool LRN>
+static void launch_ib(const LaunchSet& L, cudaStream_t st)
+{
+    // the whole IB sub-step: one cluster of kIbCtas CTAs
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kIbCtas);
+    cfg.blockDim = dim3(kIbThreads);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = L.side_prio;
+    attr[1].id = cudaLaunchAttributeClusterDimension;
+    attr[1].val.clusterDim.x = kIbCtas;
+    attr[1].val.clusterDim.y = 1;
+    attr[1].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 2;
+    if (L.ib_nst == 16)
+        cudaLaunchKernelEx(&cfg, ib_fused<S, SC, CO, LRN, 16>, L.ib_args, L.ib_passes);
+    else
+        cudaLaunchKernelEx(&cfg, ib_fused<S, SC, CO, LRN, 4>, L.ib_args, L.ib_passes);
+}
+
 template <int S, int CO, int SC, bool LRN>
 static cudaError_t launch_tpl(const LaunchSet& L)
 {
+    // Normal steps with markers and no boundary nets: IB cluster, then the
+    // bulk kernel as its programmatic dependent, both on the main stream.
+    // Timed launches (events) keep the side-stream form below, so the bulk
+    // kernel's own duration can be measured.
+    if (L.step.mode == MODE_STEP && L.ib && !L.band && L.nprep == 0 && !L.events) {
+        launch_ib<S, SC, CO, LRN>(L, L.stream);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = L.grid;
+        cfg.blockDim = dim3(kBlockX);
+        cfg.stream = L.stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, LRN>, L.step);
+        return cudaGetLastError();
+    }
     const bool side = L.nprep > 0 || L.band || L.ib;
     if (side) {
         cudaEventRecord(L.fork, L.stream);
@@ -40,25 +81,15 @@ static cudaError_t launch_tpl(const LaunchSet& L)
         if (L.band)
             launch_prio(band_kernel<S, CO>, L.band_blocks, kBandThreads, L.side, L.side_prio,
                         L.band_args);
-        if (L.ib) {
-            const IbArgs& I = L.ib_args;
-            const unsigned gn = (I.nforced + kIbThreads - 1) / kIbThreads;
-            const unsigned gm = (I.nmark + kIbThreads - 1) / kIbThreads;
-            launch_prio(ib_nodes<S, SC>, gn, kIbThreads, L.side, L.side_prio, I);
-            for (int it = 0; it < L.ib_passes; it++) {
-                if (L.ib_nst == 16)
-                    launch_prio(ib_markers<16>, gm, kIbThreads, L.side, L.side_prio, I, int(it == 0));
-                else
-                    launch_prio(ib_markers<4>, gm, kIbThreads, L.side, L.side_prio, I, int(it == 0));
-                launch_prio(ib_spread, gn, kIbThreads, L.side, L.side_prio, I);
-            }
-            launch_prio(ib_finish<S, CO, LRN>, (unsigned)I.nbody + gn, kIbThreads, L.side, L.side_prio, I);
-        }
+        if (L.ib) launch_ib<S, SC, CO, LRN>(L, L.side);
         if (L.events) cudaEventRecord(L.events[3], L.side);
         cudaEventRecord(L.join, L.side);
     }
     if (L.events) cudaEventRecord(L.events[0], L.stream);
-    step_kernel<S, CO, SC, LRN><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
+    if (L.step.mode == MODE_STEP)
+        step_fast<S, CO, SC, LRN><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
+    else
+        step_kernel<S, CO, SC, LRN><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
     if (L.events) cudaEventRecord(L.events[1], L.stream);
     if (side) cudaStreamWaitEvent(L.stream, L.join, 0);
     return cudaGetLastError();

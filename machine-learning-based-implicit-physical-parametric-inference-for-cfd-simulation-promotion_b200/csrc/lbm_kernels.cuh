@@ -459,6 +459,72 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
 }
 
 // ---------------------------------------------------------------------------
+// the same for normal steps (MODE_STEP), without the INIT / download paths:
+// the parameters are copied into registers once, node indices are 32-bit
+// (ippi_create bounds 9 * pitch * ny below 2^31), and an interior node pulls
+// its 9 populations from one base pointer at constant plane offsets.  Edge
+// nodes take the boundary rule of the scene.
+// ---------------------------------------------------------------------------
+template <int S, int CO, int SC, bool LRN>
+__global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step_fast(const StepArgs ap)
+{
+    using C = typename Store<S>::C;
+    using T = typename Store<S>::T;
+    const StepArgs a = ap;
+    const int tx = threadIdx.x, bx = blockIdx.x, by = blockIdx.y;
+    const int x = bx * kBlockX + tx, y = by;
+    const int nx = a.nx, ny = a.ny;
+    const int pitch = (int)a.pitch, plane = (int)a.plane;
+    const int t = __ldcg(&a.ctr->t[a.par]);
+    if (x < nx) {
+        const int node = y * nx + x;
+        bool deferred = false;
+        if (a.tile[by * a.tiles_x + bx]) deferred = a.nflag[node] & NF_DEFER;
+        if (!deferred) {
+            const C rbs = rbase<S>(a);
+            C f[9], rho, ux, uy;
+            const int cell = y * pitch + x;
+            if (x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
+                const T* p = reinterpret_cast<const T*>(a.f_in) + cell;
+#pragma unroll
+                for (int k = 0; k < 9; k++) f[k] = Store<S>::ld(__ldg(p + (k * plane - EY(k) * pitch - EX(k))));
+                macros<C>(f, rbs, rho, ux, uy);
+            } else if (SC == SC_REF) {
+                ref_state<S>(a, x, y, f, rho, ux, uy);
+            } else {
+                ch_state<S>(a, x, y, f, rho, ux, uy);
+            }
+            if (t >= a.avg_start) {
+                // Mesh::ComputeAvgVelocity (mesh.cpp:1969-1971)
+                C* av = reinterpret_cast<C*>(a.avg);
+                const int pl = nx * ny;
+                const C n0 = C(t - a.avg_start), n1 = C(t - a.avg_start + 1);
+                av[node] = (av[node] * n0 + ux) / n1;
+                av[pl + node] = (av[pl + node] * n0 + uy) / n1;
+                av[2 * pl + node] = (av[2 * pl + node] * n0 + rho) / n1;
+            }
+            // Mesh::ErrorCatch (mesh.cpp:2103): rho outside [0, 10]; NaN too
+            if (!(rho <= C(10) && rho >= C(0))) flag_error(a.ctr, t);
+            const C tau = a.les == 3 ? C(a.tau_field[node])
+                                     : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
+                                                        prm<C>(a.cs, a.f_cs), a.mlp);
+            collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
+            T* q = reinterpret_cast<T*>(a.f_out) + cell;
+#pragma unroll
+            for (int k = 0; k < 9; k++) q[k * plane] = Store<S>::st(f[k]);
+        }
+    }
+    if (bx == 0 && by == 0 && tx == 0) a.ctr->t[a.par ^ 1] = t + 1;
+    // One block waits for the programmatic primary (this step's IB cluster,
+    // when there is one) to complete: the grid cannot complete before that
+    // block, so the grid's completion implies the step's.  The last block is
+    // scheduled last, so the wait is normally over before it starts; it waits
+    // on a kernel that was resident before any bulk block started, so there
+    // is no circular wait.  Without a primary the wait returns at once.
+    if (bx == gridDim.x - 1 && by == gridDim.y - 1) asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
 // side-stream prep: post-stream state of the nodes other kernels need --
 // inputs of the boundary nets and IB stencil nodes (moments into side_m) and
 // deferred nodes (populations into side_f, plus their averages / outputs).
@@ -634,18 +700,30 @@ __global__ void __launch_bounds__(kBandThreads) band_kernel(const BandArgs ba)
 
 // ---------------------------------------------------------------------------
 // immersed boundary (mesh.cpp:514-832, 1244-1281 and NodeAndLattice.cpp:162-195)
-// as a chain of short, fully parallel kernels on the side stream:
-//   ib_nodes    post-stream state of every stencil node, from the previous
-//               field (the bulk kernel skips these nodes)
-//   ib_markers  InterpolateVel + CalParticleForce: F_m = 2 (U_b - sum u delta)
-//   ib_spread   SpreadForce + UpdateVelocity: node force, u += F / (2 rho)
-//               (markers and spread repeat for each direct-forcing pass)
-//   ib_finish   per-body force sums (FP64 tree, one block per body) and the
-//               forced nodes' collision with the corrected velocity + Guo term
-// Blocks are small (kIbThreads threads, at most 32 registers), so they fit
-// the first slots that retiring bulk blocks free.
+// as ONE kernel launched as a cluster of kIbCtas CTAs (the hardware
+// co-schedules a cluster, so its barriers cannot wait on an unscheduled CTA),
+// on the high-priority side stream, phases separated by cluster barriers
+// (release / acquire: global-memory writes of one phase are visible to every
+// CTA of the cluster in the next):
+//   nodes    post-stream state of every stencil node, from the previous field
+//            (the bulk kernel skips these nodes)
+//   markers  InterpolateVel + CalParticleForce: F_m = 2 (U_b - sum u delta)
+//   spread   SpreadForce + UpdateVelocity: node force, u += F / (2 rho)
+//            (markers and spread repeat for each direct-forcing pass)
+//   finish   per-body force sums (FP64 fixed-order tree, one CTA per body)
+//            and the forced nodes' collision with the corrected velocity and
+//            the operator's forcing term
+// One launch instead of a chain of dependent ones.  In a normal step it runs
+// on the main stream BEFORE the bulk kernel, which is its programmatic
+// dependent: the cluster triggers the bulk launch as soon as it is resident
+// (griddepcontrol.launch_dependents), the bulk kernel fills the rest of the
+// GPU, and the bulk kernel's last block waits for the cluster's completion
+// (griddepcontrol.wait) so that the end of the bulk grid is the end of the
+// step.  Launched beside the bulk kernel on another stream instead, the
+// cluster only found free SMs once the bulk kernel drained.
 // ---------------------------------------------------------------------------
-constexpr int kIbThreads = 128;
+constexpr int kIbThreads = 128;  // threads per CTA of the IB cluster
+constexpr int kIbCtas = 8;       // CTAs per cluster (portable cluster size)
 
 struct IbArgs {
     int nmark, nforced, nbody;
@@ -676,14 +754,17 @@ struct IbArgs {
     StepArgs s;
 };
 
+// cluster-wide barrier: arrive (release) + wait (acquire)
+__device__ __forceinline__ void cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+
 template <int S, int SC>
-__global__ void __launch_bounds__(kIbThreads, 8) ib_nodes(const IbArgs ia)
+__device__ __forceinline__ void ib_node_item(const IbArgs& ia, int n, int t)
 {
     using C = typename Store<S>::C;
     const StepArgs& a = ia.s;
-    const int n = blockIdx.x * kIbThreads + threadIdx.x;
-    if (n >= ia.nforced) return;
-    const int t = step_time(a);
     const int2 xy = ia.fn_xy[n];
     C f[9], rho, ux, uy;
     node_state<S, SC>(a, xy.x, xy.y, f, rho, ux, uy);
@@ -699,22 +780,15 @@ __global__ void __launch_bounds__(kIbThreads, 8) ib_nodes(const IbArgs ia)
 }
 
 template <int NST>
-__global__ void __launch_bounds__(kIbThreads, 8) ib_markers(const IbArgs ia, int first_pass)
+__device__ __forceinline__ void ib_marker_item(const IbArgs& ia, int m, bool first_pass)
 {
-    const int m = blockIdx.x * kIbThreads + threadIdx.x;
-    if (m >= ia.nmark) return;
-    int sn[NST];
-    double2 sw[NST];
-#pragma unroll
-    for (int q = 0; q < NST; q++) {
-        sn[q] = ia.st_node[m * 16 + q];
-        sw[q] = ia.st_w[m * 16 + q];
-    }
     double vx = 0.0, vy = 0.0;
 #pragma unroll
     for (int q = 0; q < NST; q++) {
-        vx += ia.ucx[sn[q]] * sw[q].x * sw[q].y;
-        vy += ia.ucy[sn[q]] * sw[q].x * sw[q].y;
+        const int sn = ia.st_node[m * 16 + q];
+        const double2 sw = ia.st_w[m * 16 + q];
+        vx += ia.ucx[sn] * sw.x * sw.y;
+        vy += ia.ucy[sn] * sw.x * sw.y;
     }
     const double2 u = ia.ub[m];
     const double2 d = make_double2(2.0 * (u.x - vx), 2.0 * (u.y - vy));
@@ -723,17 +797,31 @@ __global__ void __launch_bounds__(kIbThreads, 8) ib_markers(const IbArgs ia, int
     ia.mft[m] = make_double2(tot.x + d.x, tot.y + d.y);
 }
 
-static __global__ void __launch_bounds__(kIbThreads, 8) ib_spread(const IbArgs ia)
+__device__ __forceinline__ void ib_spread_item(const IbArgs& ia, int n)
 {
-    const int n = blockIdx.x * kIbThreads + threadIdx.x;
-    if (n >= ia.nforced) return;
+    // the node's markers in CSR (marker) order, kIbGather at a time with all
+    // loads of a group issued together: two memory round trips per group
+    // instead of two per marker
+    constexpr int kIbGather = 8;
     double dfx = 0.0, dfy = 0.0;
     const int e1 = ia.fn_ptr[n + 1];
-    for (int e = ia.fn_ptr[n]; e < e1; e++) {
-        const double2 d = ia.dmf[ia.fe_marker[e]];
-        const double2 wq = ia.fe_w[e];
-        dfx += d.x * wq.x * wq.y;
-        dfy += d.y * wq.x * wq.y;
+    for (int e0 = ia.fn_ptr[n]; e0 < e1; e0 += kIbGather) {
+        int mk[kIbGather];
+        double2 wq[kIbGather], d[kIbGather];
+#pragma unroll
+        for (int j = 0; j < kIbGather; j++) {
+            const bool on = e0 + j < e1;
+            mk[j] = on ? ia.fe_marker[e0 + j] : 0;
+            wq[j] = on ? ia.fe_w[e0 + j] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int j = 0; j < kIbGather; j++) d[j] = e0 + j < e1 ? ia.dmf[mk[j]] : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int j = 0; j < kIbGather; j++)
+            if (e0 + j < e1) {
+                dfx += d[j].x * wq[j].x * wq[j].y;
+                dfy += d[j].y * wq[j].x * wq[j].y;
+            }
     }
     const double r = ia.rho[n];
     ia.ucx[n] = ia.ucx[n] + 0.5 * 1 * dfx / r;
@@ -742,46 +830,45 @@ static __global__ void __launch_bounds__(kIbThreads, 8) ib_spread(const IbArgs i
     ia.fy[n] += dfy;
 }
 
+// body force -sum F ds over the body's markers: fixed-order tree over the CTA
+__device__ __forceinline__ void ib_body_sum(const IbArgs& ia, int b, int t, double (*red)[kIbThreads])
+{
+    const StepArgs& a = ia.s;
+    const int tid = threadIdx.x;
+    const int2 mr = ia.body_m[b];
+    double sx = 0.0, sy = 0.0;
+    for (int m = mr.x + tid; m < mr.y; m += kIbThreads) {
+        sx -= ia.mft[m].x * ia.ds[m];
+        sy -= ia.mft[m].y * ia.ds[m];
+    }
+    red[0][tid] = sx;
+    red[1][tid] = sy;
+    __syncthreads();
+    for (int w = kIbThreads / 2; w; w >>= 1) {
+        if (tid < w) {
+            red[0][tid] += red[0][tid + w];
+            red[1][tid] += red[1][tid + w];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        ia.force_now[2 * b] = red[0][0];
+        ia.force_now[2 * b + 1] = red[1][0];
+        if (a.mode == MODE_STEP || a.mode == MODE_INIT) {
+            const long long h = (long long)(((t % ia.hist_cap) + ia.hist_cap) % ia.hist_cap);
+            ia.force_hist[(h * ia.nbody + b) * 2] = red[0][0];
+            ia.force_hist[(h * ia.nbody + b) * 2 + 1] = red[1][0];
+        }
+    }
+    __syncthreads();  // red is reused by the next body
+}
+
+// collision of a forced node with the corrected velocity and forcing term
 template <int S, int CO, bool LRN>
-__global__ void __launch_bounds__(kIbThreads, LRN ? 4 : 8) ib_finish(const IbArgs ia)
+__device__ __forceinline__ void ib_collide_item(const IbArgs& ia, int n)
 {
     using C = typename Store<S>::C;
     const StepArgs& a = ia.s;
-    if ((int)blockIdx.x < ia.nbody) {
-        // body force: -sum F ds over the body's markers (fixed-order tree)
-        __shared__ double red[2][kIbThreads];
-        const int b = blockIdx.x, tid = threadIdx.x;
-        const int2 mr = ia.body_m[b];
-        double sx = 0.0, sy = 0.0;
-        for (int m = mr.x + tid; m < mr.y; m += kIbThreads) {
-            sx -= ia.mft[m].x * ia.ds[m];
-            sy -= ia.mft[m].y * ia.ds[m];
-        }
-        red[0][tid] = sx;
-        red[1][tid] = sy;
-        __syncthreads();
-        for (int w = kIbThreads / 2; w; w >>= 1) {
-            if (tid < w) {
-                red[0][tid] += red[0][tid + w];
-                red[1][tid] += red[1][tid + w];
-            }
-            __syncthreads();
-        }
-        if (tid == 0) {
-            ia.force_now[2 * b] = red[0][0];
-            ia.force_now[2 * b + 1] = red[1][0];
-            if (a.mode == MODE_STEP || a.mode == MODE_INIT) {
-                const int t = step_time(a);
-                const long long h = (long long)(((t % ia.hist_cap) + ia.hist_cap) % ia.hist_cap);
-                ia.force_hist[(h * ia.nbody + b) * 2] = red[0][0];
-                ia.force_hist[(h * ia.nbody + b) * 2 + 1] = red[1][0];
-            }
-        }
-        return;
-    }
-    // collision of the forced nodes with the corrected velocity and Guo term
-    const int n = (blockIdx.x - ia.nbody) * kIbThreads + threadIdx.x;
-    if (n >= ia.nforced) return;
     const C* sf = reinterpret_cast<const C*>(a.side_f) + (long long)ia.fn_slot[n] * 9;
     C f[9];
 #pragma unroll
@@ -801,6 +888,28 @@ __global__ void __launch_bounds__(kIbThreads, LRN ? 4 : 8) ib_finish(const IbArg
 #pragma unroll
         for (int q = 0; q < 9; q++) stf<S>(a, q, xy.x, xy.y, f[q]);
     }
+}
+
+// launched as exactly one cluster: gridDim.x == kIbCtas
+template <int S, int SC, int CO, bool LRN, int NST>
+__global__ void __launch_bounds__(kIbThreads) ib_fused(const IbArgs ia, int passes)
+{
+    __shared__ double red[2][kIbThreads];
+    // the dependent bulk kernel may launch now (a no-op without one)
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int T = gridDim.x * kIbThreads;
+    const int g = blockIdx.x * kIbThreads + threadIdx.x;
+    const int t = step_time(ia.s);
+    for (int n = g; n < ia.nforced; n += T) ib_node_item<S, SC>(ia, n, t);
+    cluster_sync();
+    for (int p = 0; p < passes; p++) {
+        for (int m = g; m < ia.nmark; m += T) ib_marker_item<NST>(ia, m, p == 0);
+        cluster_sync();
+        for (int n = g; n < ia.nforced; n += T) ib_spread_item(ia, n);
+        cluster_sync();
+    }
+    for (int b = blockIdx.x; b < ia.nbody; b += gridDim.x) ib_body_sum(ia, b, t, red);
+    for (int n = g; n < ia.nforced; n += T) ib_collide_item<S, CO, LRN>(ia, n);
 }
 
 // ---------------------------------------------------------------------------
