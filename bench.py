@@ -38,11 +38,11 @@ sys.path.insert(0, PKG)
 
 NX, NY = 4096, 1024
 BYTES_PER_NODE = 72  # FP32: 9 loads + 9 stores
-# DRAM bytes (read + write) of one step_kernel launch on this workload, from
+# DRAM bytes (read + write) of one bulk-kernel launch on this workload, from
 # the ncu capture summarised under profiles/ (dram__bytes_read.sum 151.22 MB +
-# dram__bytes_write.sum 104.20 MB; part of the writes is still in L2 when the
+# dram__bytes_write.sum 105.56 MB; part of the writes is still in L2 when the
 # kernel ends)
-NCU_TRAFFIC_BYTES = 255.42e6
+NCU_TRAFFIC_BYTES = 256.78e6
 METRIC = "MLUPS"
 WORKLOAD = "channel_cylinder_4096x1024_mrt_smagorinsky_ib_fp32"
 
