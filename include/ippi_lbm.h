@@ -245,6 +245,24 @@ int ippi_adjoint_forward(ippi_lbm* h, int nsteps, int t0, int ckpt_every);
 int ippi_adjoint_backward(ippi_lbm* h, const double* dl_dforce, const double* dl_dmacro,
                           double* grad_tau, double* grad_mlp, double* grad_f0);
 
+/* Implicit relaxation-time inference, Mesh::FindAndWriteTau (mesh.cpp:2625-
+ * 2715): for each of n interior nodes xy[n][2] and target moments
+ * target[n][3] (rho, u, v), the dtau = m * step, m = m_lo .. m_hi (the
+ * reference: -10000 .. 10000, 1e-5), for which the 9 upstream neighbours,
+ * relaxed with BGK at their tau + dtau and streamed into the node, give
+ * moments closest to the target in |rho - R| + |jx - U| + |jy - V| (first
+ * minimum).  best_dtau[n], best_err[n] are host arrays.  ippi_tau_scan uses
+ * the handle's current post-stream state (populations, moments, the tau of
+ * the next collision); ippi_tau_scan_state takes that state as device arrays
+ * f[9][ny][nx], m3[3][ny][nx], tau[ny][nx] (and device xy, target, outputs),
+ * enqueued on `stream`.  The scan reproduces the sequential FP64 scan bit for
+ * bit. */
+int ippi_tau_scan(ippi_lbm* h, int n, const int* xy, const double* target, int m_lo, int m_hi,
+                  double step, double* best_dtau, double* best_err);
+int ippi_tau_scan_state(const double* f, const double* m3, const double* tau, int nx, int ny, int n,
+                        const int* xy, const double* target, int m_lo, int m_hi, double step,
+                        double* best_dtau, double* best_err, void* stream);
+
 /* Last error message of the handle (or of the library when h is NULL). */
 int ippi_last_error(ippi_lbm* h, char* buf, size_t n);
 

@@ -38,6 +38,9 @@ FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", 
 # the FP32 parity tolerance.  The FP64 unit keeps IEEE division and sqrt.
 FAST_FP32 = {"kernels_f32.cu", "kernels_f16.cu", "kernels_bf16.cu"}
 FAST_FLAGS = ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]
+# Units whose FP64 results must equal a sequential CPU restatement bit for
+# bit: no FMA contraction.
+NO_FMA = {"tau_scan.cu"}
 
 
 def nvcc() -> str:
@@ -59,6 +62,8 @@ def _compile(src: str, force: bool) -> str:
                                                                            _newest_header()):
         return obj
     extra = FAST_FLAGS if os.path.basename(src) in FAST_FP32 else []
+    if os.path.basename(src) in NO_FMA:
+        extra = extra + ["-fmad=false"]
     cmd = [nvcc(), *ARCH, *FLAGS, *extra, "-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

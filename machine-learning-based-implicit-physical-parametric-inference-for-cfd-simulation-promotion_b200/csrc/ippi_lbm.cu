@@ -1468,3 +1468,39 @@ int ippi_adjoint_backward(ippi_lbm* h, const double* dl_dforce, const double* dl
     CK(h, cudaGetLastError());
     return IPPI_OK;
 }
+
+int ippi_tau_scan(ippi_lbm* h, int n, const int* xy, const double* target, int m_lo, int m_hi, double step,
+                  double* best_dtau, double* best_err)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (n < 0 || (n > 0 && (!xy || !target || !best_dtau || !best_err)) || m_lo > m_hi || !(step > 0))
+        return fail(h, IPPI_ERR_ARG, "bad tau-scan arguments");
+    if (n == 0) return IPPI_OK;
+    const int nx = h->p.nx, ny = h->p.ny;
+    for (int q = 0; q < n; q++)
+        if (xy[2 * q] < 1 || xy[2 * q] > nx - 2 || xy[2 * q + 1] < 1 || xy[2 * q + 1] > ny - 2)
+            return fail(h, IPPI_ERR_ARG, "tau-scan node %d is not an interior node", q);
+    CK(h, cudaSetDevice(h->p.device));
+    if (int rc = materialize(h)) return rc;
+    const size_t nn = (size_t)nx * ny;
+    int* dxy = nullptr;
+    double *dt = nullptr, *dout = nullptr;
+    cudaError_t e = dalloc(&dxy, 2 * (size_t)n * sizeof(int));
+    if (e == cudaSuccess) e = dalloc(&dt, 3 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = dalloc(&dout, 2 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dxy, xy, 2 * (size_t)n * sizeof(int), cudaMemcpyHostToDevice, h->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dt, target, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->st);
+    // the materialised post-stream state: f planes 0..8, rho/ux/uy 9..11,
+    // tau of the next collision 13
+    if (e == cudaSuccess)
+        e = tau_scan_launch(h->dl, h->dl + 9 * nn, h->dl + 13 * nn, nx, ny, n, dxy, dt, m_lo, m_hi, step, dout,
+                            dout + n, h->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(best_dtau, dout, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(best_err, dout + n, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    dfree(dxy);
+    dfree(dt);
+    dfree(dout);
+    CK(h, e);
+    return IPPI_OK;
+}

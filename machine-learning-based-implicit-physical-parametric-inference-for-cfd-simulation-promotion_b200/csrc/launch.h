@@ -30,6 +30,11 @@ struct LaunchSet {
     cudaEvent_t* events;
 };
 
+// Mesh::FindAndWriteTau's scan (tau_scan.cu) on device arrays
+cudaError_t tau_scan_launch(const double* f, const double* m3, const double* tau, int nx, int ny, int n,
+                            const int* xy, const double* target, int m_lo, int m_hi, double step,
+                            double* best_dtau, double* best_err, cudaStream_t st);
+
 cudaError_t launch_f64(const LaunchSet& L);
 cudaError_t launch_f32(const LaunchSet& L);
 cudaError_t launch_f16(const LaunchSet& L);

@@ -161,6 +161,17 @@ class Lattice:
             out["f0"] = gf
         return out
 
+    def tau_scan(self, xy, target, m_lo=-10000, m_hi=10000, step=1e-5):
+        """Mesh::FindAndWriteTau's scan at the current state: best dtau and
+        its error for interior nodes xy[n][2] and targets target[n][3]."""
+        xy = np.ascontiguousarray(xy, dtype=np.int32).reshape(-1, 2)
+        target = _f64(target).reshape(-1, 3)
+        n = xy.shape[0]
+        bd, be = np.zeros(n), np.zeros(n)
+        L.check(L.lib().ippi_tau_scan(self._h, n, xy.ctypes.data_as(C.POINTER(C.c_int)), _p(target), m_lo,
+                                      m_hi, step, _p(bd), _p(be)), self._h)
+        return bd, be
+
     def filter_snapshot(self, factor):
         """Box-filtered state [6][ny/f][nx/f]: rho, ux, uy (density-weighted),
         effective stress Sxx, Sxy, Syy (include/ippi_lbm.h)."""

@@ -1156,3 +1156,53 @@ void orc_ib_probe(orc* s, double* vref, double* mforce, double* nforce)
             }
     }
 }
+
+/* ---------------------------------------------------------------------- */
+/* Implicit tau inference: Mesh::FindAndWriteTau (mesh.cpp:2625-2715).    */
+/* ---------------------------------------------------------------------- */
+/* For a node (x, y) and target moments (R, U, V): for m = m_lo .. m_hi,
+ * dtau = m * step, relax each upstream neighbour (x - e_k, y - e_k) with
+ * BGK at tau + dtau -- fcol_k = (1 - 1/(tau + dtau)) fnew_k + feq_k/(tau +
+ * dtau) -- and stream it into (x, y); the candidate's error is
+ * |sum f - R| + |sum f e_x - U| + |sum f e_y - V| (momentum against the
+ * target velocity, as mesh.cpp:2675-2681 does).  The first minimum wins
+ * (strict <).  f [9][ny][nx] are the post-stream populations, m3 [3][ny][nx]
+ * their rho, ux, uy (feq is Compute_feq of those), tau [ny][nx]. */
+void orc_tau_scan_state(const double* f, const double* m3, const double* tau, int nx, int ny,
+                        int n, const int* xy, const double* target, int m_lo, int m_hi,
+                        double step, double* best_dtau, double* best_err)
+{
+    size_t nn = (size_t)nx * ny;
+    for (int q = 0; q < n; q++) {
+        int x = xy[2 * q], y = xy[2 * q + 1];
+        double fn[9], fe[9], tn[9];
+        for (int k = 0; k < 9; k++) {
+            /* the neighbour whose population k streams into (x, y) */
+            size_t g = (size_t)(y - E[k][1]) * nx + (x - E[k][0]);
+            double feq[9];
+            compute_feq(m3[g], m3[nn + g], m3[2 * nn + g], feq);
+            fn[k] = f[k * nn + g];
+            fe[k] = feq[k];
+            tn[k] = tau[g];
+        }
+        double R = target[3 * q], U = target[3 * q + 1], V = target[3 * q + 2];
+        double bestDeltaTau = 1e10, bestABS = 1e10;
+        for (int mm = m_lo; mm <= m_hi; mm++) {
+            double deltaTau = (double)mm * step;
+            double trho = 0, tu = 0, tv = 0;
+            for (int k = 0; k < 9; k++) {
+                double c = (1.0 - 1.0 / (tn[k] + deltaTau)) * fn[k] + fe[k] / (tn[k] + deltaTau);
+                trho += c;
+                tu += c * E[k][0];
+                tv += c * E[k][1];
+            }
+            double TargetAbs = fabs(trho - R) + fabs(tu - U) + fabs(tv - V);
+            if (TargetAbs < bestABS) {
+                bestABS = TargetAbs;
+                bestDeltaTau = deltaTau;
+            }
+        }
+        best_dtau[q] = bestDeltaTau;
+        best_err[q] = bestABS;
+    }
+}

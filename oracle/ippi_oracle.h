@@ -113,6 +113,12 @@ void orc_force_node(int collision, double ux, double uy, double fx, double fy, d
 int orc_load_tau_mlp(orc* s, const float* w, size_t n, const float* stats, size_t nstats);
 /* tau per node for les_model 3: [ny][nx] global. */
 int orc_set_tau_field(orc* s, const double* tau);
+/* Mesh::FindAndWriteTau's scan (mesh.cpp:2625-2715) over candidates m_lo..m_hi
+ * (dtau = m * step) for n nodes xy[n][2] with targets target[n][3]; state
+ * f [9][ny][nx], m3 [3][ny][nx] (rho, ux, uy), tau [ny][nx]. */
+void orc_tau_scan_state(const double* f, const double* m3, const double* tau, int nx, int ny,
+                        int n, const int* xy, const double* target, int m_lo, int m_hi,
+                        double step, double* best_dtau, double* best_err);
 /* tau0 + out_scale * softplus(MLP(features)), Smagorinsky outside [lo, hi];
  * p = the 1338 parameters + statistics as doubles */
 double orc_learned_tau(const double* fnew, double rho, double ux, double uy,

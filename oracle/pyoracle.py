@@ -74,6 +74,9 @@ def lib() -> C.CDLL:
         L.orc_les_tau.restype = C.c_double
         L.orc_les_tau.argtypes = [_dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
         L.orc_set_tau_field.argtypes = [C.c_void_p, _dp]
+        L.orc_tau_scan_state.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, C.c_int,
+                                         C.POINTER(C.c_int), _dp, C.c_int, C.c_int, C.c_double,
+                                         _dp, _dp]
         L.orc_force_node.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                      C.c_double, C.c_double, _dp]
         L.orc_load_tau_mlp.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_size_t,
@@ -244,3 +247,19 @@ class RefSim:
         if rc != 0:
             raise RuntimeError("ref_ib_probe failed")
         return xy.reshape(-1, 2), vref.reshape(-1, 2), mf.reshape(-1, 2), nf
+
+
+def tau_scan_state(f, m3, tau, xy, target, m_lo=-10000, m_hi=10000, step=1e-5):
+    """Mesh::FindAndWriteTau's scan on a given state (see ippi_oracle.h)."""
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    m3 = np.ascontiguousarray(m3, dtype=np.float64)
+    tau = np.ascontiguousarray(tau, dtype=np.float64)
+    xy = np.ascontiguousarray(xy, dtype=np.int32)
+    target = np.ascontiguousarray(target, dtype=np.float64)
+    n = xy.shape[0]
+    ny, nx = tau.shape
+    bd, be = np.zeros(n), np.zeros(n)
+    lib().orc_tau_scan_state(_ptr(f), _ptr(m3), _ptr(tau), nx, ny, n,
+                             xy.ctypes.data_as(C.POINTER(C.c_int)), _ptr(target), m_lo, m_hi, step,
+                             _ptr(bd), _ptr(be))
+    return bd, be
