@@ -263,6 +263,17 @@ int ippi_tau_scan_state(const double* f, const double* m3, const double* tau, in
                         const int* xy, const double* target, int m_lo, int m_hi, double step,
                         double* best_dtau, double* best_err, void* stream);
 
+/* Solid nodes (the reference's 's' style): solid[ny][nx] != 0 marks a solid
+ * node, at least 3 nodes inside the lattice (channel scene).  Fluid nodes
+ * with a link into a solid ('b') take halfway bounce-back on it; solid nodes
+ * are not updated and download as fluid at rest.  n = 0 removes them.
+ * ippi_solid_force: the momentum-exchange force on the solids after the
+ * last step, Mesh::OutputCd (mesh.cpp:1461-1526): the sum over 'b' nodes and
+ * directions k into a solid of e_k (fnew_opp(k) + fcol_k), FP64, as the
+ * reference sums it (before its 1/(rho U^2 R) scaling). */
+int ippi_set_solid(ippi_lbm* h, const uint8_t* solid, size_t n);
+int ippi_solid_force(ippi_lbm* h, double* force_xy);
+
 /* Last error message of the handle (or of the library when h is NULL). */
 int ippi_last_error(ippi_lbm* h, char* buf, size_t n);
 

@@ -100,6 +100,11 @@ struct ippi_lbm {
     // learned tau: parameters (FP32 values of the BF16 weights) + statistics
     float* mlp_dev = nullptr;
     double* tau_field = nullptr;  // IPPI_LES_FIELD: [ny][nx]
+    // solid nodes (halfway bounce-back) and their momentum-exchange links
+    std::vector<uint8_t> solid;   // [ny][nx] or empty
+    int2* solid_links = nullptr;  // (fluid node, direction into the solid)
+    int nlinks = 0;
+    double* solid_out = nullptr;
     // adjoint: the recorded rollout (checkpoints every K steps) and work buffers
     struct Adjoint {
         bool ready = false;
@@ -392,6 +397,33 @@ int rebuild(ippi_lbm* h)
         }
     }
 
+    // solid nodes and the fluid nodes with a link into one
+    std::vector<uint8_t> sflag(nn, 0);
+    std::vector<int2> links;
+    if (!h->solid.empty()) {
+        for (size_t i = 0; i < nn; i++)
+            if (h->solid[i]) sflag[i] = NF_SOLID;
+        for (int y = 1; y < ny - 1; y++)
+            for (int x = 1; x < nx - 1; x++) {
+                if (h->solid[id(x, y)]) continue;
+                for (int k = 1; k < 9; k++)
+                    if (h->solid[id(x + EX(k), y + EY(k))]) {
+                        sflag[id(x, y)] = NF_SBND;
+                        links.push_back(make_int2((int)id(x, y), k));
+                    }
+            }
+        for (size_t i = 0; i < nn; i++)
+            if (sflag[i] && (flag[i] & (NF_IB | NF_EXPORT)))
+                return fail(h, IPPI_ERR_ARG, "an IB stencil or boundary-net node touches the solid (node %zu)", i);
+    }
+    dfree(h->solid_links);
+    h->solid_links = nullptr;
+    h->nlinks = (int)links.size();
+    if (!links.empty()) {
+        CK(h, dalloc(&h->solid_links, links.size() * sizeof(int2)));
+        CK(h, cudaMemcpy(h->solid_links, links.data(), links.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    }
+
     // slots in row-major order; boundary-net nodes (inputs and band) are
     // prep nodes, IB stencil nodes are computed by the IB kernel itself
     int ns = 0;
@@ -408,11 +440,13 @@ int rebuild(ippi_lbm* h)
     std::vector<uint8_t> defer(nn, 0);
     std::vector<uint8_t> tile((size_t)h->gx * ny, 0);
     for (int y = 0; y < ny; y++)
-        for (int x = 0; x < nx; x++)
-            if (flag[id(x, y)] & NF_DEFER) {
-                defer[id(x, y)] = NF_DEFER;
+        for (int x = 0; x < nx; x++) {
+            const uint8_t d = (uint8_t)((flag[id(x, y)] & NF_DEFER) | sflag[id(x, y)]);
+            if (d) {
+                defer[id(x, y)] = d;
                 tile[(size_t)y * h->gx + x / kBlockX] = 1;
             }
+        }
 
     CK(h, cudaMemcpy(h->nflag, defer.data(), nn, cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->tile, tile.data(), tile.size(), cudaMemcpyHostToDevice));
@@ -871,6 +905,8 @@ int ippi_destroy(ippi_lbm* h)
     for (int b = 0; b < 2; b++) dfree(h->f[b]);
     dfree(h->mlp_dev);
     dfree(h->tau_field);
+    dfree(h->solid_links);
+    dfree(h->solid_out);
     dfree(h->ctr);
     if (h->ctr_h) cudaFreeHost(h->ctr_h);
     dfree(h->nflag);
@@ -951,6 +987,9 @@ int ippi_set_markers(ippi_lbm* h, int n, const double* xy, const double* ub, con
         nbody = std::max(nbody, b + 1);
         (void)nst;
     }
+    const int keep_n = h->nmark, keep_nb = h->nbody;
+    std::vector<double> keep_xy = h->mk_xy, keep_ub = h->mk_ub, keep_ds = h->mk_ds;
+    std::vector<int> keep_body = h->mk_body;
     h->nmark = n;
     h->nbody = n > 0 ? nbody : 0;
     h->mk_xy.assign(xy, xy + 2 * (size_t)n);
@@ -961,7 +1000,18 @@ int ippi_set_markers(ippi_lbm* h, int n, const double* xy, const double* ub, con
     h->mk_body.assign(n, 0);
     if (body) h->mk_body.assign(body, body + n);
     CK(h, cudaStreamSynchronize(h->st));
-    return rebuild(h);
+    int rc = rebuild(h);
+    if (rc) {
+        // rejected (a stencil on a solid): keep the previous markers
+        h->nmark = keep_n;
+        h->nbody = keep_nb;
+        h->mk_xy = keep_xy;
+        h->mk_ub = keep_ub;
+        h->mk_ds = keep_ds;
+        h->mk_body = keep_body;
+        rebuild(h);
+    }
+    return rc;
 }
 
 int ippi_load_band_net(ippi_lbm* h, int type, const float* w, size_t n)
@@ -1112,7 +1162,7 @@ int ippi_download(ippi_lbm* h, int field, void* host, size_t bytes)
         if (!h->dl_flags) CK(h, dalloc(&h->dl_flags, nn));
         style_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, h->st>>>(
             h->dl_flags, h->p.nx, h->p.ny, h->p.plate_x0,
-            h->p.bc_set == IPPI_BC_CHANNEL ? SC_CHANNEL : SC_REF);
+            h->p.bc_set == IPPI_BC_CHANNEL ? SC_CHANNEL : SC_REF, h->nflag);
         CK(h, cudaGetLastError());
         CK(h, cudaMemcpyAsync(host, h->dl_flags, nn, cudaMemcpyDeviceToHost, h->st));
         CK(h, cudaStreamSynchronize(h->st));
@@ -1304,6 +1354,7 @@ int ippi_adjoint_forward(ippi_lbm* h, int nsteps, int t0, int ckpt_every)
     if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
     if (nsteps < 1 || ckpt_every < 1) return fail(h, IPPI_ERR_ARG, "nsteps and ckpt_every must be positive");
     if (h->p.bc_set != IPPI_BC_CHANNEL) return fail(h, IPPI_ERR_STATE, "the adjoint is built for the channel scene");
+    if (!h->solid.empty()) return fail(h, IPPI_ERR_STATE, "the adjoint does not take solid nodes");
     if (h->ib_active && h->p.mdf_iters != 1)
         return fail(h, IPPI_ERR_STATE, "the adjoint supports one direct-forcing pass (mdf_iters = 1)");
     if (h->ib_active && (long long)nsteps > h->hist_cap)
@@ -1502,5 +1553,57 @@ int ippi_tau_scan(ippi_lbm* h, int n, const int* xy, const double* target, int m
     dfree(dt);
     dfree(dout);
     CK(h, e);
+    return IPPI_OK;
+}
+
+int ippi_set_solid(ippi_lbm* h, const uint8_t* solid, size_t n)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    const int nx = h->p.nx, ny = h->p.ny;
+    const size_t nn = (size_t)nx * ny;
+    if (n == 0) {
+        h->solid.clear();
+        return rebuild(h);
+    }
+    if (!solid || n != nn) return fail(h, IPPI_ERR_ARG, "solid mask needs nx * ny = %zu entries", nn);
+    if (h->p.bc_set != IPPI_BC_CHANNEL) return fail(h, IPPI_ERR_ARG, "solid nodes are built for the channel scene");
+    for (size_t i = 0; i < nn; i++) {
+        const int x = (int)(i % nx), y = (int)(i / nx);
+        if (solid[i] && (x < 3 || x > nx - 4 || y < 3 || y > ny - 4))
+            return fail(h, IPPI_ERR_ARG, "solid node %zu is closer than 3 nodes to the lattice edge", i);
+    }
+    std::vector<uint8_t> keep = h->solid;
+    h->solid.assign(solid, solid + nn);
+    for (auto& v : h->solid) v = v ? 1 : 0;
+    int rc = rebuild(h);
+    if (rc) {
+        h->solid = keep;
+        rebuild(h);
+    }
+    return rc;
+}
+
+int ippi_solid_force(ippi_lbm* h, double* force_xy)
+{
+    if (!h || !force_xy) return fail(h, IPPI_ERR_ARG, "null argument");
+    if (h->nlinks == 0) {
+        force_xy[0] = force_xy[1] = 0.0;
+        return IPPI_OK;
+    }
+    if (h->pending_init) return fail(h, IPPI_ERR_STATE, "no step taken yet");
+    CK(h, cudaSetDevice(h->p.device));
+    if (int rc = materialize(h)) return rc;
+    if (!h->solid_out) CK(h, dalloc(&h->solid_out, 2 * sizeof(double)));
+    // the last step started from f[cur ^ 1]: its post-collision field
+    const StepArgs a = make_launch(h, MODE_STEP, h->f[h->cur ^ 1], nullptr, 0).step;
+    switch (h->S) {
+    case ST_F64: solid_force_kernel<ST_F64><<<1, 256, 0, h->st>>>(a, h->solid_links, h->nlinks, h->dl, h->solid_out); break;
+    case ST_F32: solid_force_kernel<ST_F32><<<1, 256, 0, h->st>>>(a, h->solid_links, h->nlinks, h->dl, h->solid_out); break;
+    case ST_F16: solid_force_kernel<ST_F16><<<1, 256, 0, h->st>>>(a, h->solid_links, h->nlinks, h->dl, h->solid_out); break;
+    default: solid_force_kernel<ST_BF16><<<1, 256, 0, h->st>>>(a, h->solid_links, h->nlinks, h->dl, h->solid_out); break;
+    }
+    CK(h, cudaGetLastError());
+    CK(h, cudaMemcpyAsync(force_xy, h->solid_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
     return IPPI_OK;
 }

@@ -21,10 +21,12 @@ enum { ST_F64 = 0, ST_F32 = 1, ST_F16 = 2, ST_BF16 = 3 };
 enum { CO_BGK = 0, CO_MRT = 1, CO_RR = 2 };
 enum { SC_REF = 0, SC_CHANNEL = 1 };
 
-// per-node side flags: NF_DEFER is the only one on the device (the bulk
-// kernel skips those nodes); NF_EXPORT marks boundary-net inputs and NF_IB
-// immersed-boundary stencil nodes (host-side tables only)
-enum : uint8_t { NF_EXPORT = 1, NF_DEFER = 2, NF_IB = 4 };
+// per-node flags.  On the device: NF_DEFER (the bulk kernel skips the node,
+// another kernel finishes it), NF_SOLID (a solid node: never updated) and
+// NF_SBND (a fluid node with a link into a solid: halfway bounce-back on
+// that link).  NF_EXPORT (boundary-net inputs) and NF_IB (immersed-boundary
+// stencil nodes) live in the host-side tables only.
+enum : uint8_t { NF_EXPORT = 1, NF_DEFER = 2, NF_IB = 4, NF_SOLID = 8, NF_SBND = 16 };
 
 // step kernel modes
 enum { MODE_STEP = 0, MODE_INIT = 1, MODE_MAT = 2, MODE_MAT_INIT = 3 };

@@ -356,6 +356,19 @@ __device__ __forceinline__ int step_time(const StepArgs& a)
     return a.mode >= MODE_MAT ? a.fixed_t : __ldcg(&a.ctr->t[a.par]);
 }
 
+// pull of an interior fluid node next to solid nodes: a population whose
+// source is solid is the node's own opposite post-collision population
+// (halfway bounce-back, as the reference's 'b' nodes next to 's' nodes)
+template <int S>
+__device__ __forceinline__ void solid_pull(const StepArgs& a, int x, int y, typename Store<S>::C* f)
+{
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const int sx = x - EX(k), sy = y - EY(k);
+        f[k] = (a.nflag[sy * a.nx + sx] & NF_SOLID) ? ldf<S>(a, OPP(k), x, y) : ldf<S>(a, k, sx, sy);
+    }
+}
+
 // post-stream state of node (x, y): the boundary rule of its kind and its
 // moments, or (INIT modes) the equilibrium of the initial moments
 template <int S, int SC>
@@ -435,10 +448,24 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
         uint8_t nf = 0;
         if (a.tile[blockIdx.y * a.tiles_x + blockIdx.x]) nf = a.nflag[node];
         const bool deferred = nf & NF_DEFER;
-        if (!deferred || a.mode == MODE_INIT) {
+        if ((nf & NF_SOLID) && a.mode >= MODE_MAT) {
+            // a solid node reads as fluid at rest
+            const long long pl = (long long)a.nx * a.ny;
+#pragma unroll
+            for (int q = 0; q < 9; q++) a.dl_f[q * pl + node] = WK<double>(q) * a.rho0;
+            a.dl_m[node] = a.rho0;
+            a.dl_m[pl + node] = 0.0;
+            a.dl_m[2 * pl + node] = 0.0;
+            a.dl_tau[node] = a.tau0;
+        } else if ((!deferred && !(nf & NF_SOLID)) || a.mode == MODE_INIT) {
             const C rbs = rbase<S>(a);
             C f[9], rho, ux, uy;
-            node_state<S, SC>(a, x, y, f, rho, ux, uy);
+            if ((nf & NF_SBND) && a.mode != MODE_INIT && a.mode != MODE_MAT_INIT) {
+                solid_pull<S>(a, x, y, f);
+                macros<C>(f, rbs, rho, ux, uy);
+            } else {
+                node_state<S, SC>(a, x, y, f, rho, ux, uy);
+            }
             if (!deferred) {
                 node_epilogue<S>(a, node, t, f, rho, ux, uy);
                 const C tau = a.les == 3 ? C(a.tau_field[node])
@@ -478,13 +505,16 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
     const int t = __ldcg(&a.ctr->t[a.par]);
     if (x < nx) {
         const int node = y * nx + x;
-        bool deferred = false;
-        if (a.tile[by * a.tiles_x + bx]) deferred = a.nflag[node] & NF_DEFER;
-        if (!deferred) {
+        uint8_t nf = 0;
+        if (a.tile[by * a.tiles_x + bx]) nf = a.nflag[node];
+        if (!(nf & (NF_DEFER | NF_SOLID))) {
             const C rbs = rbase<S>(a);
             C f[9], rho, ux, uy;
             const int cell = y * pitch + x;
-            if (x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
+            if (nf & NF_SBND) {
+                solid_pull<S>(a, x, y, f);
+                macros<C>(f, rbs, rho, ux, uy);
+            } else if (x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
                 const T* p = reinterpret_cast<const T*>(a.f_in) + cell;
 #pragma unroll
                 for (int k = 0; k < 9; k++) f[k] = Store<S>::ld(__ldg(p + (k * plane - EY(k) * pitch - EX(k))));
@@ -915,15 +945,58 @@ __global__ void __launch_bounds__(kIbThreads) ib_fused(const IbArgs ia, int pass
 // ---------------------------------------------------------------------------
 // small utility kernels
 // ---------------------------------------------------------------------------
-static __global__ void style_kernel(uint8_t* out, int nx, int ny, int plate_x0, int scene)
+static __global__ void style_kernel(uint8_t* out, int nx, int ny, int plate_x0, int scene,
+                                   const uint8_t* nflag)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (long long)nx * ny) return;
     const int x = (int)(i % nx), y = (int)(i / nx);
+    if (nflag[i] & (NF_SOLID | NF_SBND)) {
+        out[i] = (uint8_t)((nflag[i] & NF_SOLID) ? 's' : 'b');  // JudgeStyle's solid / boundary
+        return;
+    }
     if (scene == SC_REF) {
         out[i] = (uint8_t)ref_style(x, y, nx, ny, plate_x0);
     } else {
         out[i] = (uint8_t)(x == 0 ? 'i' : (x == nx - 1 ? 'o' : ((y == 0 || y == ny - 1) ? 'w' : 'f')));
+    }
+}
+
+// Momentum exchange on solid links (Mesh::OutputCd, mesh.cpp:1461-1526):
+// F = sum over fluid nodes x and directions k with x + e_k solid of
+// e_k (fnew_opp(k)(x) + fcol_k(x)); fnew is the materialised post-stream
+// field (FP64), fcol the post-collision field the last step started from.
+// One block, fixed-order tree: deterministic.
+template <int S>
+__global__ void __launch_bounds__(256) solid_force_kernel(const StepArgs a, const int2* links, int nlink,
+                                                         const double* fnew, double* out)
+{
+    __shared__ double red[2][256];
+    const int tid = threadIdx.x;
+    const long long pl = (long long)a.nx * a.ny;
+    const double rb = double(rbase<S>(a));
+    double sx = 0.0, sy = 0.0;
+    for (int l = tid; l < nlink; l += 256) {
+        const int node = links[l].x, k = links[l].y;
+        const int x = node % a.nx, y = node / a.nx;
+        const double fc = double(ldf<S>(a, k, x, y)) + WK<double>(k) * rb;
+        const double v = fnew[OPP(k) * pl + node] + fc;
+        sx += EX(k) * v;
+        sy += EY(k) * v;
+    }
+    red[0][tid] = sx;
+    red[1][tid] = sy;
+    __syncthreads();
+    for (int w = 128; w; w >>= 1) {
+        if (tid < w) {
+            red[0][tid] += red[0][tid + w];
+            red[1][tid] += red[1][tid + w];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        out[0] = red[0][0];
+        out[1] = red[1][0];
     }
 }
 

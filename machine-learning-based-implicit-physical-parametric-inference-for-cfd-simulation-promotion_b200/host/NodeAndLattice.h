@@ -47,6 +47,7 @@ public:
     double avg_u = 0;
     double avg_v = 0;
     double avg_density = 0;
+    double cp = 0;  // time-averaged pressure coefficient ('b' nodes, Mesh::OutputCp)
     char style = 'f';
     bool NNflag = false;
 

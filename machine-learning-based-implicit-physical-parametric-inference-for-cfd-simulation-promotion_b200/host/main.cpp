@@ -7,8 +7,8 @@
 //
 //   ippi_main [--scene plate|channel] [--nx N] [--ny N] [--steps N]
 //             [--save N] [--avg N] [--re R] [--u U] [--cs C]
-//             [--cylinder X Y D] [--markers N] [--nets DIR] [--init FILE]
-//             [--batched] [--print N] [--device N]
+//             [--cylinder X Y D] [--markers N] [--solid] [--cp START]
+//             [--nets DIR] [--init FILE] [--batched] [--print N] [--device N]
 //
 //   plate    the reference's scene: flat plate, NEE inlet u = --u, Re 5e5,
 //            tau = 0.5 + 6 (Ny U / Re) (main.cpp:37-43)
@@ -16,6 +16,12 @@
 //            walls; with --cylinder an IB cylinder of diameter D,
 //            nu = U D / Re, tau = 3 nu + 1/2; its body force goes to
 //            particle/forces.dat every step
+//   --solid        the cylinder as solid nodes (halfway bounce-back) instead
+//                  of IB markers; Mesh::OutputCd's momentum-exchange Cd / Cl
+//                  go to particle/CD_CL.dat every step (every save point
+//                  with --batched)
+//   --cp START     with --solid: surface pressure coefficient averaged from
+//                  step START (= --avg) to cp/cp_Merged_<t>.dat at save points
 //   --nets DIR     boundary nets AutoT0<k>.f32 (raw float32 TorchScript
 //                  parameters) for the plate scene
 //   --init FILE    initial rho, ux, uy as 3 x Ny x Nx float64 (raw)
@@ -42,6 +48,8 @@ struct Options {
     bool cylinder = false;
     double cx = 0, cy = 0, d = 0;
     int markers = 0;
+    bool solid = false;
+    int cp = -1;
     string nets, init;
     bool batched = false;
     int print = 1;
@@ -74,6 +82,8 @@ bool parse(int argc, char** argv, Options& o)
             o.cy = atof(argv[++i]);
             o.d = atof(argv[++i]);
         } else if (a == "--markers" && need(1)) o.markers = atoi(argv[++i]);
+        else if (a == "--solid") o.solid = true;
+        else if (a == "--cp" && need(1)) o.cp = atoi(argv[++i]);
         else if (a == "--nets" && need(1)) o.nets = argv[++i];
         else if (a == "--init" && need(1)) o.init = argv[++i];
         else if (a == "--batched") o.batched = true;
@@ -106,7 +116,8 @@ int main(int argc, char* argv[])
     if (!parse(argc, argv, o)) {
         cerr << "usage: ippi_main [--scene plate|channel] [--nx N] [--ny N] [--steps N] [--save N]\n"
                 "                 [--avg N] [--re R] [--u U] [--cs C] [--cylinder X Y D] [--markers N]\n"
-                "                 [--nets DIR] [--init FILE] [--batched] [--print N] [--device N]"
+                "                 [--solid] [--cp START] [--nets DIR] [--init FILE] [--batched]\n"
+                "                 [--print N] [--device N]"
              << endl;
         return 2;
     }
@@ -140,6 +151,8 @@ int main(int argc, char* argv[])
     mesh.InitialFile();
 
     mesh.InitialLatMesh(Nx, Ny, tau, StartVel, Rho, RankID, CoreNum, 0);
+    const bool solid = channel && o.cylinder && o.solid;
+    mesh.SolidCylinder = solid;
     mesh.JudgeStyle(mesh.center, (REAL)mesh.radius, RankID, CoreNum);
     if (!o.init.empty()) {
         vector<double> m(3 * (size_t)Nx * Ny);
@@ -151,7 +164,7 @@ int main(int argc, char* argv[])
         const size_t nn = (size_t)Nx * Ny;
         mesh.SetInitialField(m.data(), m.data() + nn, m.data() + 2 * nn);
     }
-    if (channel && o.cylinder) {
+    if (channel && o.cylinder && !solid) {
         const int n = o.markers > 0 ? o.markers : (int)std::ceil(M_PI * o.d);
         mesh.InitialIBParticle(n, o.d / 2, o.cx, o.cy, Point2D{0, 0});
         mesh.WriteDatParticle(0);
@@ -172,13 +185,14 @@ int main(int argc, char* argv[])
     cout << endl;
     cout << "Start Computing" << endl;
 
-    const bool forces = channel && o.cylinder;
+    const bool forces = channel && o.cylinder && !solid;
     for (int t = 1; t <= o.steps;) {
         int n = 1;
         if (o.batched) {
             // up to the next save point
             n = o.save > 0 ? std::min(o.steps - t + 1, o.save - (t - 1) % o.save) : o.steps - t + 1;
             mesh.RunSteps(t, n);
+            if (solid) mesh.OutputCd(RankID, CoreNum, t + n - 1, mesh.radius);
             if (forces) {
                 vector<double> hist(2 * (size_t)n);
                 const int got = ippi_force_history(mesh.Handle(), hist.data(), n);
@@ -192,12 +206,18 @@ int main(int argc, char* argv[])
         } else {
             mesh.OneLBMStep(RankID, CoreNum, Cs, Pr, t);
             if (forces) mesh.OutputForces(t, o.u, o.d);
+            if (solid) mesh.OutputCd(RankID, CoreNum, t, mesh.radius);
         }
         t += n;
         const int last = t - 1;
+        if (solid && o.cp >= 0) mesh.ComputeCp(o.cp, last);
         if (o.save > 0 && last % o.save == 0) {
             mesh.WriteDatFluid(last, RankID, Nx, CoreNum);
             mesh.MergeDatFluid(last, CoreNum);
+            if (solid && o.cp >= 0) {
+                mesh.OutputCp(RankID, CoreNum, last, mesh.radius);
+                mesh.MergeCp(last, CoreNum);
+            }
         }
         mesh.ComputeAvgVelocity(last);
         if (o.print > 0 && (last % o.print == 0 || last == o.steps))

@@ -144,6 +144,15 @@ void Mesh::JudgeStyle(Point2D CylinderCenter1, REAL Radius, int RankID, int Core
     center = CylinderCenter1;
     radius = Radius;
     if (!h_) return;
+    if (SolidCylinder) {
+        std::vector<unsigned char> m((size_t)nx_ * ny_, 0);
+        for (int y = 0; y < ny_; y++)
+            for (int x = 0; x < nx_; x++) {
+                const double dx = x - (double)CylinderCenter1.x, dy = y - (double)CylinderCenter1.y;
+                m[(size_t)y * nx_ + x] = dx * dx + dy * dy <= (double)Radius * Radius;
+            }
+        if (!SetSolid(m.data())) return;
+    }
     std::vector<unsigned char> fl((size_t)nx_ * ny_);
     if (!check(ippi_download(h_, IPPI_FIELD_FLAGS, fl.data(), fl.size()), "ippi_download")) return;
     for (int x = 0; x < nx_; x++)
@@ -340,6 +349,79 @@ void Mesh::GetSt(int t)
                         << L.avg_v << std::endl;
                 }
         }
+}
+
+bool Mesh::SetSolid(const unsigned char* solid)
+{
+    if (!h_) return false;
+    const size_t nn = solid ? (size_t)nx_ * ny_ : 0;
+    return check(ippi_set_solid(h_, solid, nn), "ippi_set_solid");
+}
+
+// Mesh::OutputCd (mesh.cpp:1461-1526): momentum exchange over the links from
+// 'b' nodes into 's' nodes after the last step, Cd / Cl = F / (0.5 U^2 2R)
+// with U = startU.x; "t cd cl" appended to particle/CD_CL.dat.
+void Mesh::OutputCd(int RankID, int CoreNum, int time, double Radius)
+{
+    (void)CoreNum;
+    double f[2] = {0, 0};
+    if (!h_ || !check(ippi_solid_force(h_, f), "ippi_solid_force")) return;
+    const double q = 0.5 * (double)startU.x * (double)startU.x * 2 * Radius;
+    const double cd = f[0] / q, cl = f[1] / q;
+    if (RankID == 0) {
+        cerr << "cd:" << cd << " " << "cl:" << cl << endl;
+        std::ofstream out("particle/CD_CL.dat", std::ios::app);
+        out << time << " " << cd << " " << cl << endl;
+    }
+}
+
+// Mesh::ComputeCp (mesh.cpp:1642-1655) keeps, on every 'b' node, the running
+// mean from step startcp of (p - 1/3) / (0.5 U^2), p = rho / 3.  It is linear
+// in rho, so it is the mean density the step accumulates from startAvg on,
+// taken through the same map: startcp must equal startAvg.
+void Mesh::ComputeCp(int startcp, int t)
+{
+    if (t < startcp) return;
+    if (cp_start_ != startcp && startcp != startAvg)
+        cerr << "ComputeCp: the pressure mean starts at startAvg = " << startAvg << ", not " << startcp << endl;
+    cp_start_ = startcp;
+}
+
+// Mesh::OutputCp (mesh.cpp:1575-1597): "x y cp" of every 'b' node (interior
+// columns) to cp/cp_<time>_<rank>.dat
+void Mesh::OutputCp(int RankID, int CoreNum, int time, double Radius)
+{
+    (void)CoreNum;
+    (void)Radius;
+    ensure_synced();
+    const double q = 0.5 * (double)startU.x * (double)startU.x;
+    const bool have = cp_start_ >= 0 && last_t_ >= startAvg;
+    std::ostringstream name;
+    name << "cp/cp_" << time << "_" << RankID << ".dat";
+    std::ofstream out(name.str());
+    for (int i = 1; i < nx_ + 1; i++)
+        for (int j = 0; j < ny_; j++) {
+            Lattice& L = LatMesh[i][j];
+            if (L.style != 'b') continue;
+            L.cp = have ? (L.avg_density / 3.0 - 1.0 / 3.0) / q : 0.0;
+            out << L.pos.x << " " << L.pos.y << " " << L.cp << "\n";
+        }
+}
+
+// Mesh::MergeCp (mesh.cpp:1598-1641): cp/cp_<t>_<r>.dat of every rank into
+// cp/cp_Merged_<t>.dat, the parts removed (empty parts skipped)
+void Mesh::MergeCp(int t, int CoreNum)
+{
+    std::ofstream merged("cp/cp_Merged_" + std::to_string(t) + ".dat");
+    for (int r = 0; r < CoreNum; r++) {
+        const std::string part = "cp/cp_" + std::to_string(t) + "_" + std::to_string(r) + ".dat";
+        {
+            std::ifstream in(part);
+            if (!in) continue;
+            if (in.peek() != std::ifstream::traits_type::eof()) merged << in.rdbuf();
+        }
+        std::remove(part.c_str());
+    }
 }
 
 int Mesh::BodyForces(double* fxy, int max_bodies)

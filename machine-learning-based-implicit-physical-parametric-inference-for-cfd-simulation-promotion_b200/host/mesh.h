@@ -78,8 +78,18 @@ public:
     void MergeAvgu(int t, int CoreNum);
     void WriteDatParticle(int t);
     void GetSt(int t);
+    void OutputCd(int RankID, int CoreNum, int time, double Radius);
+    void OutputCp(int RankID, int CoreNum, int time, double Radius);
+    void MergeCp(int t, int CoreNum);
+    void ComputeCp(int startcp, int t);
 
     // ---- additions ----------------------------------------------------
+    // JudgeStyle marks the nodes within Radius of CylinderCenter1 as solid
+    // ('s', halfway bounce-back; their fluid neighbours become 'b'), the
+    // cylinder OutputCd / OutputCp read (channel scene)
+    bool SolidCylinder = false;
+    // solid nodes from a mask solid[Ny][Nx] (NULL removes them)
+    bool SetSolid(const unsigned char* solid);
     // initial macroscopic fields rho/ux/uy[Ny][Nx] (NULL: rho 1, u 0)
     void SetInitialField(const double* rho, const double* ux, const double* uy);
     // boundary net weights (NNmodel/AutoT0<type>.pt in TorchScript order)
@@ -102,6 +112,7 @@ private:
     bool synced_ = false;
     int last_t_ = 0;
     std::vector<double> init_rho_, init_ux_, init_uy_;
+    int cp_start_ = -1;
     bool check(int rc, const char* what);
     void ensure_synced();
 };

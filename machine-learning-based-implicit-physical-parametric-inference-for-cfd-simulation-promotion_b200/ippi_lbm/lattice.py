@@ -161,6 +161,20 @@ class Lattice:
             out["f0"] = gf
         return out
 
+    def set_solid(self, mask):
+        """Solid nodes: mask[ny][nx] (nonzero = solid); None removes them."""
+        if mask is None:
+            L.check(L.lib().ippi_set_solid(self._h, None, 0), self._h)
+            return
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        L.check(L.lib().ippi_set_solid(self._h, m.ctypes.data_as(C.POINTER(C.c_uint8)), m.size), self._h)
+
+    def solid_force(self):
+        """Momentum-exchange force (Fx, Fy) on the solids after the last step."""
+        out = np.zeros(2)
+        L.check(L.lib().ippi_solid_force(self._h, _p(out)), self._h)
+        return out
+
     def tau_scan(self, xy, target, m_lo=-10000, m_hi=10000, step=1e-5):
         """Mesh::FindAndWriteTau's scan at the current state: best dtau and
         its error for interior nodes xy[n][2] and targets target[n][3]."""

@@ -24,6 +24,13 @@ def cylinder_markers(cx, cy, d, n=None):
     return np.stack([x, y], axis=1), np.full(n, math.pi * d / n)
 
 
+def cylinder_solid(nx, ny, cx, cy, d):
+    """Solid mask [ny][nx] of a staircase cylinder: nodes (x, y) with
+    (x - cx)^2 + (y - cy)^2 <= (d / 2)^2."""
+    yy, xx = np.mgrid[0:ny, 0:nx].astype(np.float64)
+    return ((xx - cx) ** 2 + (yy - cy) ** 2 <= 0.25 * d * d).astype(np.uint8)
+
+
 def channel_init(nx, ny, u_max, noise=1e-4, seed=0):
     y = np.arange(ny, dtype=np.float64) + 0.5
     prof = 4.0 * u_max * y * (ny - y) / ny ** 2

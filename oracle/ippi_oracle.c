@@ -53,6 +53,7 @@ struct orc {
     double mlp[1313 + 25];      /* learned tau network (les_model 2) */
     double* tau_field;          /* les_model 3: tau per node, [ny][nx] global */
     int mlp_loaded;
+    unsigned char* solid;       /* [NX*NY] solid nodes, or NULL */
 };
 
 #define ID(s, i, j) ((size_t)(i) * (size_t)(s)->NY + (size_t)(j))
@@ -511,11 +512,24 @@ static void judge_style(orc* s)
             }
             s->style[ID(s, i, j)] = st;
         }
+    if (!s->solid) return;
+    /* solid 's' and fluid nodes with a link into a solid 'b' (the styles
+     * Mesh::OutputCd, mesh.cpp:1472-1478, sums over) */
+    for (int i = 2; i < NX - 2; i++)
+        for (int j = 1; j < Ny - 1; j++) {
+            if (s->solid[ID(s, i, j)]) {
+                s->style[ID(s, i, j)] = 's';
+                continue;
+            }
+            for (int k = 1; k < 9; k++)
+                if (s->solid[ID(s, i + E[k][0], j + E[k][1])]) s->style[ID(s, i, j)] = 'b';
+        }
 }
 
 orc* orc_create(const orc_params* p)
 {
     if (p->nx < 4 || p->ny < 4) return NULL;
+    if (p->delta_kernel != 0 && p->delta_kernel != 1) return NULL;
     orc* s = (orc*)calloc(1, sizeof(orc));
     s->p = *p;
     if (s->p.mdf_iters < 1) s->p.mdf_iters = 1;
@@ -549,6 +563,7 @@ void orc_destroy(orc* s)
     free(s->avg_rho); free(s->nnflag); free(s->style); free(s->mk);
     free(s->body_force);
     free(s->tau_field);
+    free(s->solid);
     for (int t = 0; t < 8; t++) free(s->nets[t].w);
     free(s);
 }
@@ -935,12 +950,22 @@ static void streaming_channel(orc* s)
         for (int y = 0; y < ny; y++) {
             int i = x + 1;
             double f[9];
+            if (s->solid && s->solid[ID(s, i, y)]) {
+                /* a solid node: not updated, reads as fluid at rest */
+                size_t id = ID(s, i, y);
+                for (int k = 0; k < 9; k++) FN(s, k, i, y) = W[k] * s->p.rho0;
+                s->rho[id] = s->p.rho0;
+                s->ux[id] = s->uy[id] = 0.0;
+                continue;
+            }
             for (int k = 0; k < 9; k++) {
                 int sx = x - E[k][0], sy = y - E[k][1];
                 if (sy < 0 || sy >= ny)
                     f[k] = FC(s, OPP[k], i, y);
                 else if (sx < 0)
                     f[k] = 0.0; /* replaced by Zou-He below */
+                else if (s->solid && s->solid[ID(s, sx + 1, sy)])
+                    f[k] = FC(s, OPP[k], i, y); /* halfway bounce-back on the solid */
                 else
                     f[k] = FC(s, k, sx + 1, sy);
             }
@@ -988,6 +1013,7 @@ static void average(orc* s, int t)
     double a = (double)(t - s->p.avg_start), b = (double)(t - s->p.avg_start + 1);
     size_t n = (size_t)s->NX * s->NY;
     for (size_t id = 0; id < n; id++) {
+        if (s->solid && s->solid[id]) continue;
         s->avg_u[id] = (s->avg_u[id] * a + s->ux[id]) / b;
         s->avg_v[id] = (s->avg_v[id] * a + s->uy[id]) / b;
         s->avg_rho[id] = (s->avg_rho[id] * a + s->rho[id]) / b;
@@ -1205,4 +1231,48 @@ void orc_tau_scan_state(const double* f, const double* m3, const double* tau, in
         best_dtau[q] = bestDeltaTau;
         best_err[q] = bestABS;
     }
+}
+
+int orc_set_solid(orc* s, const unsigned char* solid)
+{
+    free(s->solid);
+    s->solid = NULL;
+    if (solid) {
+        int nx = s->p.nx, ny = s->p.ny;
+        s->solid = (unsigned char*)calloc((size_t)s->NX * s->NY, 1);
+        for (int y = 0; y < ny; y++)
+            for (int x = 0; x < nx; x++) {
+                if (!solid[(size_t)y * nx + x]) continue;
+                if (s->p.bc_set != BC_CHANNEL || x < 3 || x > nx - 4 || y < 3 || y > ny - 4) {
+                    free(s->solid);
+                    s->solid = NULL;
+                    judge_style(s);
+                    return -1;
+                }
+                s->solid[ID(s, x + 1, y)] = 1;
+            }
+    }
+    judge_style(s);
+    return 0;
+}
+
+/* Mesh::OutputCd (mesh.cpp:1461-1488): sum over 'b' nodes, i then j, and
+ * every k whose neighbour is 's' of e_k (fnew_opp(k) + fcol_k); fcol is the
+ * collision whose streaming produced the current fnew. */
+void orc_solid_force(orc* s, double* force_xy)
+{
+    double fx = 0.0, fy = 0.0;
+    for (int i = 1; i < s->NX - 1; i++)
+        for (int j = 1; j < s->NY - 1; j++) {
+            if (s->style[ID(s, i, j)] != 'b') continue;
+            for (int k = 0; k < 9; k++) {
+                int ip = i + E[k][0], jp = j + E[k][1];
+                if (s->style[ID(s, ip, jp)] == 's') {
+                    fx += E[k][0] * (FN(s, OPP[k], i, j) + FC(s, k, i, j));
+                    fy += E[k][1] * (FN(s, OPP[k], i, j) + FC(s, k, i, j));
+                }
+            }
+        }
+    force_xy[0] = fx;
+    force_xy[1] = fy;
 }

@@ -90,6 +90,14 @@ int orc_forces(orc* s, double* force_xy, double* mass);
 void orc_ib_probe(orc* s, double* vref, double* mforce, double* nforce);
 int orc_num_bodies(orc* s);
 
+/* Solid nodes (channel scene): solid[ny][nx] != 0, at least 3 nodes from
+ * the edges, or NULL to remove them.  Fluid links into a solid take halfway
+ * bounce-back; solid nodes read as fluid at rest.  Returns 0 or -1. */
+int orc_set_solid(orc* s, const unsigned char* solid);
+/* Momentum-exchange force on the solids after the last step
+ * (Mesh::OutputCd's sum, before its scaling). */
+void orc_solid_force(orc* s, double* force_xy);
+
 /* Building blocks exposed for unit tests. */
 double orc_peskin_phi(double r);
 float orc_band_forward(const float* w, int nin, const float* in);

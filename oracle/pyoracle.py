@@ -74,6 +74,8 @@ def lib() -> C.CDLL:
         L.orc_les_tau.restype = C.c_double
         L.orc_les_tau.argtypes = [_dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
         L.orc_set_tau_field.argtypes = [C.c_void_p, _dp]
+        L.orc_set_solid.argtypes = [C.c_void_p, C.POINTER(C.c_uint8)]
+        L.orc_solid_force.argtypes = [C.c_void_p, _dp]
         L.orc_tau_scan_state.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, C.c_int,
                                          C.POINTER(C.c_int), _dp, C.c_int, C.c_int, C.c_double,
                                          _dp, _dp]
@@ -147,6 +149,16 @@ class Oracle:
     def set_tau_field(self, tau):
         tau = np.ascontiguousarray(tau, dtype=np.float64)
         lib().orc_set_tau_field(self._h, _ptr(tau))
+
+    def set_solid(self, mask):
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+        if lib().orc_set_solid(self._h, None if m is None else m.ctypes.data_as(C.POINTER(C.c_uint8))):
+            raise ValueError("solid nodes must be at least 3 nodes inside a channel lattice")
+
+    def solid_force(self):
+        out = np.zeros(2)
+        lib().orc_solid_force(self._h, _ptr(out))
+        return out
 
     def step(self, n, t0=1):
         return lib().orc_step(self._h, n, t0)

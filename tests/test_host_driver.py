@@ -87,3 +87,56 @@ def test_driver_channel_cylinder_batched_equals_per_step(tmp_path):
     n = math.ceil(math.pi * 12)
     with open(a / "particle" / "particle_t0.dat") as f:
         assert f"N={n}, E={n}" in f.read()
+
+
+@pytest.mark.gpu
+def test_driver_solid_cylinder_cd_and_cp(tmp_path):
+    """--solid: the cylinder as solid nodes, Mesh::OutputCd every step (every
+    save point when batched) and the time-averaged Cp of its 'b' nodes; the
+    values the driver prints (6 digits) are those of the Python API on the
+    same lattice (the driver's defaults: BGK, FP64, Smagorinsky)."""
+    ip = pytest.importorskip("ippi_lbm")
+    from ippi_lbm import scenes
+
+    nx, ny, u, d = 400, 100, 0.05, 20
+    init = np.stack(scenes.channel_init(nx, ny, u))
+    init.tofile(tmp_path / "init.f64")
+    common = ["--scene", "channel", "--nx", str(nx), "--ny", str(ny), "--u", str(u), "--re", "100",
+              "--cs", "0.1", "--cylinder", "100", "50", str(d), "--solid", "--steps", "2000", "--save", "1000",
+              "--avg", "1000", "--cp", "1000", "--print", "0", "--init", str(tmp_path / "init.f64")]
+    a, b = tmp_path / "a", tmp_path / "b"
+    a.mkdir()
+    b.mkdir()
+    run_main(common, cwd=a)
+    run_main(common + ["--batched"], cwd=b)
+    ca = np.loadtxt(a / "particle" / "CD_CL.dat")
+    cb = np.loadtxt(b / "particle" / "CD_CL.dat")
+    assert ca.shape == (2000, 3) and np.array_equal(ca[:, 0], np.arange(1, 2001))
+    assert cb.shape == (2, 3)
+    np.testing.assert_array_equal(ca[[999, 1999]], cb)
+    assert 1.0 < ca[-500:, 1].mean() < 2.0
+    assert not (a / "particle" / "forces.dat").exists()
+    cp = np.loadtxt(a / "cp" / "cp_Merged_2000.dat")
+    np.testing.assert_array_equal(cp, np.loadtxt(b / "cp" / "cp_Merged_2000.dat"))
+    assert not (a / "cp" / "cp_2000_0.dat").exists()
+
+    q = 0.5 * u * u * d
+    g = ip.Lattice(nx, ny, collision=ip.BGK, storage=ip.F64, bc_set=ip.BC_CHANNEL,
+                   les_model=ip.LES_SMAGORINSKY, tau0=3.0 * (u * d / 100) + 0.5, cs=0.1, u_in=u, rho0=1.0,
+                   avg_start=1000)
+    g.set_solid(scenes.cylinder_solid(nx, ny, 100, 50, d))
+    g.init_macros(*init)
+    for t, row in ((1, cb[0]), (1001, cb[1])):
+        g.step(1000, t)
+        np.testing.assert_allclose(g.solid_force() / q, row[1:], rtol=2e-5, atol=1e-6)
+    # the 'b' ring around a D = 20 staircase cylinder (317 's' nodes): 88 nodes
+    style = g.download(ip.FIELD_FLAGS)
+    ys, xs = np.nonzero(style == ord("b"))
+    assert len(cp) == 88 == len(xs)
+    want = (g.download(ip.FIELD_AVG_RHO)[ys, xs] / 3 - 1 / 3) / (0.5 * u * u)
+    order = np.lexsort((ys, xs))  # the driver writes x-major
+    np.testing.assert_allclose(cp[:, 2], want[order], rtol=2e-5, atol=1e-6)
+    front = cp[np.argmin(cp[:, 0])]
+    assert front[2] > 0.5  # stagnation side
+    assert cp[:, 2].min() < 0  # suction on the flanks
+    g.close()
