@@ -10,8 +10,10 @@
  *                      (Parameter.h:8-21) and main.cpp constants (main.cpp:12-65)
  *                      become ippi_params fields
  *   ippi_init_macros   Lattice::InitialLatticeFeq over the mesh
- *                      (NodeAndLattice.cpp:69-123; mesh.cpp:159-166), and the
- *                      field reset of Mesh::ManageDataFromXflow (mesh.cpp:2189)
+ *                      (NodeAndLattice.cpp:69-123; mesh.cpp:159-166)
+ *   ippi_reequilibrate the same in the middle of a run, as
+ *                      Mesh::ManageDataFromXflow / XflowABS do
+ *                      (mesh.cpp:2391-2398, 2615-2620)
  *   ippi_set_markers   Mesh::InitialIBParticle (mesh.cpp:173-191) -- the IB
  *                      sub-step InterpolateVel / CalParticleForce / SpreadForce /
  *                      UpdateVelocity (mesh.cpp:552, 514, 656, 1244) then runs
@@ -125,6 +127,12 @@ int ippi_destroy(ippi_lbm* h);
 /* Set rho/u on every node and the populations to their equilibrium
  * (InitialLatticeFeq).  NULL arrays mean rho = 1 / u = 0.  Resets averages. */
 int ippi_init_macros(ippi_lbm* h, const double* rho, const double* ux, const double* uy);
+/* Lattice::InitialLatticeFeq on every node in the middle of a run (the
+ * reference's ManageDataFromXflow / XflowABS, mesh.cpp:2391-2398, 2615-2620):
+ * populations replaced by the equilibrium of the given moments (NULL: rho 1,
+ * u 0), with the running means and the force history kept.  Needs a step
+ * taken. */
+int ippi_reequilibrate(ippi_lbm* h, const double* rho, const double* ux, const double* uy);
 
 /* Immersed-boundary markers: positions xy[2n], prescribed velocities ub[2n]
  * (NULL = at rest), body id per marker body[n] (NULL = all 0), arc length per

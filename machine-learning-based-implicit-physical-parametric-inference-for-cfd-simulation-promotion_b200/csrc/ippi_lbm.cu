@@ -933,7 +933,23 @@ int ippi_destroy(ippi_lbm* h)
     return IPPI_OK;
 }
 
+namespace {
+int init_macros(ippi_lbm* h, const double* rho, const double* ux, const double* uy, bool keep_means);
+}
+
 int ippi_init_macros(ippi_lbm* h, const double* rho, const double* ux, const double* uy)
+{
+    return init_macros(h, rho, ux, uy, false);
+}
+
+int ippi_reequilibrate(ippi_lbm* h, const double* rho, const double* ux, const double* uy)
+{
+    if (h && h->pending_init) return fail(h, IPPI_ERR_STATE, "no step taken yet (use ippi_init_macros)");
+    return init_macros(h, rho, ux, uy, true);
+}
+
+namespace {
+int init_macros(ippi_lbm* h, const double* rho, const double* ux, const double* uy, bool keep_means)
 {
     if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
     CK(h, cudaSetDevice(h->p.device));
@@ -951,7 +967,7 @@ int ippi_init_macros(ippi_lbm* h, const double* rho, const double* ux, const dou
     init_fields_kernel<<<std::min<size_t>((nn + 255) / 256, 4096), 256, 0, h->st>>>(
         h->init_m, (long long)nn, rho != nullptr, ux != nullptr, uy != nullptr, bad);
     CK(h, cudaGetLastError());
-    CK(h, cudaMemsetAsync(h->avg, 0, 3 * nn * h->csize, h->st));
+    if (!keep_means) CK(h, cudaMemsetAsync(h->avg, 0, 3 * nn * h->csize, h->st));
     unsigned long long first_bad = 0;
     CK(h, cudaMemcpyAsync(&first_bad, bad, sizeof first_bad, cudaMemcpyDeviceToHost, h->st));
     CK(h, cudaStreamSynchronize(h->st));
@@ -961,9 +977,10 @@ int ippi_init_macros(ippi_lbm* h, const double* rho, const double* ux, const dou
     // is launched outside them: they stay valid
     h->pending_init = true;
     h->dl_valid = false;
-    h->hist_written = 0;
+    if (!keep_means) h->hist_written = 0;
     return IPPI_OK;
 }
+}  // namespace
 
 int ippi_set_markers(ippi_lbm* h, int n, const double* xy, const double* ub, const int* body,
                      const double* ds)

@@ -48,6 +48,12 @@ public:
     double avg_v = 0;
     double avg_density = 0;
     double cp = 0;  // time-averaged pressure coefficient ('b' nodes, Mesh::OutputCp)
+    // differences to the imported XFlow state (Mesh::ManageDataFromXflow,
+    // XflowABS): u - u_xflow, rho - rho_xflow, tau - (3 nu_xflow + 1/2)
+    Point2D absU = {0, 0};
+    REAL absRHO = 0;
+    double xflowtau = 0;
+    double abstau = 0;
     char style = 'f';
     bool NNflag = false;
 

@@ -9,6 +9,7 @@
 //             [--save N] [--avg N] [--re R] [--u U] [--cs C]
 //             [--cylinder X Y D] [--markers N] [--solid] [--cp START]
 //             [--nets DIR] [--init FILE] [--batched] [--print N] [--device N]
+//             [--xflow DIR] [--xflow-offset N] [--xflow-init] [--xflow-abs N]
 //
 //   plate    the reference's scene: flat plate, NEE inlet u = --u, Re 5e5,
 //            tau = 0.5 + 6 (Ny U / Re) (main.cpp:37-43)
@@ -27,6 +28,10 @@
 //   --init FILE    initial rho, ux, uy as 3 x Ny x Nx float64 (raw)
 //   --batched      advance between save points in one call (CUDA graphs)
 //                  instead of one OneLBMStep call per step
+//   --xflow DIR    XFlow exports DIR/pb_<t + offset>.csv (offset 10014, or
+//                  --xflow-offset); --xflow-init: Mesh::ManageDataFromXflow
+//                  after step 1; --xflow-abs N: Mesh::XflowABS every N steps
+//                  (the coupling blocks of the reference's main.cpp:132-156)
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -50,6 +55,10 @@ struct Options {
     int markers = 0;
     bool solid = false;
     int cp = -1;
+    string xflow;
+    int xflow_offset = 10014;
+    bool xflow_init = false;
+    int xflow_abs = 0;
     string nets, init;
     bool batched = false;
     int print = 1;
@@ -83,6 +92,10 @@ bool parse(int argc, char** argv, Options& o)
             o.d = atof(argv[++i]);
         } else if (a == "--markers" && need(1)) o.markers = atoi(argv[++i]);
         else if (a == "--solid") o.solid = true;
+        else if (a == "--xflow" && need(1)) o.xflow = argv[++i];
+        else if (a == "--xflow-offset" && need(1)) o.xflow_offset = atoi(argv[++i]);
+        else if (a == "--xflow-init") o.xflow_init = true;
+        else if (a == "--xflow-abs" && need(1)) o.xflow_abs = atoi(argv[++i]);
         else if (a == "--cp" && need(1)) o.cp = atoi(argv[++i]);
         else if (a == "--nets" && need(1)) o.nets = argv[++i];
         else if (a == "--init" && need(1)) o.init = argv[++i];
@@ -117,7 +130,8 @@ int main(int argc, char* argv[])
         cerr << "usage: ippi_main [--scene plate|channel] [--nx N] [--ny N] [--steps N] [--save N]\n"
                 "                 [--avg N] [--re R] [--u U] [--cs C] [--cylinder X Y D] [--markers N]\n"
                 "                 [--solid] [--cp START] [--nets DIR] [--init FILE] [--batched]\n"
-                "                 [--print N] [--device N]"
+                "                 [--print N] [--device N] [--xflow DIR] [--xflow-offset N]\n"
+                "                 [--xflow-init] [--xflow-abs N]"
              << endl;
         return 2;
     }
@@ -144,6 +158,8 @@ int main(int argc, char* argv[])
     mesh.LatmeshSizeNx = Nx;
     mesh.LatmeshSizeNy = Ny;
     mesh.Device = o.device;
+    if (!o.xflow.empty()) mesh.XflowDir = o.xflow;
+    mesh.XflowStepOffset = o.xflow_offset;
     if (channel) {
         mesh.BoundarySet = IPPI_BC_CHANNEL;
         mesh.DeltaKernel = IPPI_DELTA_PESKIN4;
@@ -191,6 +207,9 @@ int main(int argc, char* argv[])
         if (o.batched) {
             // up to the next save point
             n = o.save > 0 ? std::min(o.steps - t + 1, o.save - (t - 1) % o.save) : o.steps - t + 1;
+            // stop where a coupling hook runs
+            if (o.xflow_init && t == 1) n = 1;
+            if (o.xflow_abs > 0) n = std::min(n, o.xflow_abs - (t - 1) % o.xflow_abs);
             mesh.RunSteps(t, n);
             if (solid) mesh.OutputCd(RankID, CoreNum, t + n - 1, mesh.radius);
             if (forces) {
@@ -210,6 +229,8 @@ int main(int argc, char* argv[])
         }
         t += n;
         const int last = t - 1;
+        if (o.xflow_init && last == 1) mesh.ManageDataFromXflow(last);
+        if (o.xflow_abs > 0 && last % o.xflow_abs == 0) mesh.XflowABS(last);
         if (solid && o.cp >= 0) mesh.ComputeCp(o.cp, last);
         if (o.save > 0 && last % o.save == 0) {
             mesh.WriteDatFluid(last, RankID, Nx, CoreNum);

@@ -82,6 +82,12 @@ void Mesh::InitialLatMesh(int Nx_P, int Ny, double tau, Point2D StartVel, double
         std::vector<double> r((size_t)nx * Ny, Rho);
         if (!check(ippi_init_macros(h_, r.data(), nullptr, nullptr), "ippi_init_macros")) return;
     }
+    tau_field_.clear();
+    if (LesModel == IPPI_LES_FIELD) {
+        // the tau-field model starts from every node's TauAtBeginning
+        tau_field_.assign((size_t)nx * Ny, tau);
+        if (!check(ippi_set_tau_field(h_, tau_field_.data()), "ippi_set_tau_field")) return;
+    }
     LatMesh.assign(nx + 2, vector<Lattice>(Ny));
     for (int i = 0; i < nx + 2; i++)
         for (int j = 0; j < Ny; j++) {
@@ -421,6 +427,190 @@ void Mesh::MergeCp(int t, int CoreNum)
             if (in.peek() != std::ifstream::traits_type::eof()) merged << in.rdbuf();
         }
         std::remove(part.c_str());
+    }
+}
+
+// ---------------------------------------------------------------------------
+// XFlow coupling.  The reference matches every node against every point
+// (O(nodes x points), mesh.cpp:2368-2390); a point lands on exactly one node,
+// so here each point finds its node directly.  Relaxation times written by
+// these methods reach the collision under the tau-field model
+// (IPPI_LES_FIELD); under the others the collision recomputes tau every step,
+// as the reference's does, and they stay in the mirror.
+// ---------------------------------------------------------------------------
+
+// Mesh::ReadXflowdata (mesh.cpp:2413-2547)
+vector<PointData> Mesh::ReadXflowdata(int t)
+{
+    std::vector<PointData> pts;
+    const std::string name = XflowDir + "/pb_" + std::to_string(t + XflowStepOffset) + ".csv";
+    if (!ippi_host::read_xflow_csv(name, pts)) cerr << "cannot open " << name << endl;
+    ippi_host::clip_xflow(pts, MyrankID, MyCoreNum, ParallelSize, LatmeshSizeNx);
+    return pts;
+}
+
+void Mesh::set_tau_node(int x, int y, double tau)
+{
+    if (LesModel != IPPI_LES_FIELD) return;
+    if (tau_field_.empty()) {
+        // the relaxation times the mirror holds
+        tau_field_.resize((size_t)nx_ * ny_);
+        for (int yy = 0; yy < ny_; yy++)
+            for (int xx = 0; xx < nx_; xx++) tau_field_[(size_t)yy * nx_ + xx] = LatMesh[xx + 1][yy].tau;
+    }
+    tau_field_[(size_t)y * nx_ + x] = tau;
+}
+
+void Mesh::upload_tau_field()
+{
+    if (h_ && LesModel == IPPI_LES_FIELD && !tau_field_.empty())
+        check(ippi_set_tau_field(h_, tau_field_.data()), "ippi_set_tau_field");
+}
+
+// Lattice::InitialLatticeFeq on every node from the mirror's rho and u
+void Mesh::reequilibrate_mirror()
+{
+    if (!h_) return;
+    const size_t nn = (size_t)nx_ * ny_;
+    std::vector<double> m(3 * nn);
+    for (int y = 0; y < ny_; y++)
+        for (int x = 0; x < nx_; x++) {
+            const Lattice& L = LatMesh[x + 1][y];
+            const size_t g = (size_t)y * nx_ + x;
+            m[g] = L.rho;
+            m[nn + g] = L.u.x;
+            m[2 * nn + g] = L.u.y;
+        }
+    if (last_t_ > 0)
+        check(ippi_reequilibrate(h_, m.data(), m.data() + nn, m.data() + 2 * nn), "ippi_reequilibrate");
+    else
+        check(ippi_init_macros(h_, m.data(), m.data() + nn, m.data() + 2 * nn), "ippi_init_macros");
+    synced_ = false;
+}
+
+// Mesh::ManageDataFromXflow (mesh.cpp:2189-2399): the imported rho, u and
+// tau = 3 nu + 1/2 on the nodes the points land on, then every node at the
+// equilibrium of its moments
+void Mesh::ManageDataFromXflow(int t)
+{
+    const std::vector<PointData> pts = ReadXflowdata(t);
+    ensure_synced();
+    for (const PointData& p : pts) {
+        int x, y;
+        if (!ippi_host::xflow_node(p, nx_, ny_, &x, &y)) continue;
+        Lattice& L = LatMesh[x + 1][y];
+        L.absU.x = (REAL)(L.u.x - p.ux);
+        L.absU.y = (REAL)(L.u.y - p.uy);
+        L.absRHO = (REAL)(L.rho - p.TotalPressure);
+        L.u.x = (REAL)p.ux;
+        L.u.y = (REAL)p.uy;
+        L.rho = (REAL)p.TotalPressure;
+        L.tau = (REAL)(3 * p.viscosity + 0.5);
+        set_tau_node(x, y, L.tau);
+    }
+    reequilibrate_mirror();
+    upload_tau_field();
+}
+
+// Mesh::XflowABS (mesh.cpp:2585-2624): differences to the imported state on
+// the nodes the points land on, then every node at the equilibrium of its
+// moments
+void Mesh::XflowABS(int t)
+{
+    const std::vector<PointData> pts = ReadXflowdata(t);
+    ensure_synced();
+    for (const PointData& p : pts) {
+        int x, y;
+        if (!ippi_host::xflow_node(p, nx_, ny_, &x, &y)) continue;
+        Lattice& L = LatMesh[x + 1][y];
+        L.absU.x = (REAL)(L.u.x - p.ux);
+        L.absU.y = (REAL)(L.u.y - p.uy);
+        L.absRHO = (REAL)(L.rho - p.TotalPressure);
+        L.xflowtau = p.viscosity * 3.0 + 0.5;
+        L.abstau = L.tau - L.xflowtau;
+    }
+    reequilibrate_mirror();
+}
+
+// Mesh::ChangeTauFromXflow (mesh.cpp:2717-2766): tau = 1/2 + 3 nu on every
+// node, and the mean square velocity and density differences appended to
+// cp/InletMSE.dat.  The reference carries the last matched point's values
+// into nodes no point lands on (from uninitialised ones before the first
+// match); here the carry starts from nu = (startTau - 1/2) / 3 and zero
+// errors.  Nodes are visited x-major over the lattice columns.
+void Mesh::ChangeTauFromXflow(int t)
+{
+    const std::vector<PointData> pts = ReadXflowdata(t);
+    ensure_synced();
+    std::vector<int> at((size_t)nx_ * ny_, -1);
+    for (size_t q = 0; q < pts.size(); q++) {
+        int x, y;
+        if (ippi_host::xflow_node(pts[q], nx_, ny_, &x, &y)) at[(size_t)y * nx_ + x] = (int)q;
+    }
+    double nu = (startTau - 0.5) / 3.0, ev = 0, er = 0, total_v = 0, total_r = 0;
+    for (int x = 0; x < nx_; x++)
+        for (int y = 0; y < ny_; y++) {
+            Lattice& L = LatMesh[x + 1][y];
+            const int q = at[(size_t)y * nx_ + x];
+            if (q >= 0) {
+                const PointData& p = pts[q];
+                nu = p.viscosity;
+                ev = (L.u.x - p.ux) * (L.u.x - p.ux) + (L.u.y - p.uy) * (L.u.y - p.uy);
+                er = (L.rho - p.TotalPressure) * (L.rho - p.TotalPressure);
+            }
+            total_v += ev;
+            total_r += er;
+            L.tau = (REAL)(0.5 + 3.0 * nu);
+            set_tau_node(x, y, L.tau);
+        }
+    upload_tau_field();
+    const double n = (double)nx_ * ny_;
+    std::ofstream out("cp/InletMSE.dat", std::ios::app);
+    out << t << " " << total_v / n << " " << total_r / n << endl;
+}
+
+// Mesh::FindAndWriteTau (mesh.cpp:2625-2715): the dtau in [-0.1, 0.1] (step
+// 1e-5) whose BGK relaxation of the 9 upstream neighbours best reproduces the
+// imported moments of step t + 1 at node (i, j) of the mirror (column i =
+// x + 1), scanned on the GPU (ippi_tau_scan); the 9 neighbours' tau += dtau;
+// "t dtau tau_0 .. tau_8" appended to cp/BestTau.dat
+void Mesh::FindAndWriteTau(int i, int j, int t)
+{
+    static const int e[9][2] = {{0, 0}, {1, 0}, {0, 1}, {-1, 0}, {0, -1}, {1, 1}, {-1, 1}, {-1, -1}, {1, -1}};
+    if (!h_) return;
+    const int x = i - 1, y = j;
+    const std::vector<PointData> pts = ReadXflowdata(t + 1);
+    double target[3];
+    bool found = false;
+    for (const PointData& p : pts) {
+        int px, py;
+        if (ippi_host::xflow_node(p, nx_, ny_, &px, &py) && px == x && py == y) {
+            target[0] = p.TotalPressure;
+            target[1] = p.ux;
+            target[2] = p.uy;
+            found = true;
+        }
+    }
+    if (!found) {
+        cerr << "FindAndWriteTau: no XFlow point on node (" << x << ", " << y << ") at step " << t + 1 << endl;
+        return;
+    }
+    const int xy[2] = {x, y};
+    double best = 0, err = 0;
+    if (!check(ippi_tau_scan(h_, 1, xy, target, -10000, 10000, 1e-5, &best, &err), "ippi_tau_scan")) return;
+    ensure_synced();
+    for (int k = 0; k < 9; k++) {
+        Lattice& L = LatMesh[i + e[k][0]][j + e[k][1]];
+        L.tau = (REAL)(L.tau + best);
+        set_tau_node(x + e[k][0], y + e[k][1], L.tau);
+    }
+    upload_tau_field();
+    if (MyrankID == 0) {
+        cerr << "Timestep:" << t << " " << "BestTau:" << best << endl;
+        std::ofstream out("cp/BestTau.dat", std::ios::app);
+        out << t << " " << best << " ";
+        for (int k = 0; k < 9; k++) out << LatMesh[i + e[k][0]][j + e[k][1]].tau << " ";
+        out << endl;
     }
 }
 

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "NodeAndLattice.h"
+#include "xflow.h"
 
 class Mesh {
 public:
@@ -61,6 +62,8 @@ public:
     int PlateX0 = 400;  // flat plate: specular bottom for x < PlateX0 (mesh.cpp:1413)
     int Device = 0;
     bool AbortOnError = true;
+    std::string XflowDir = "Xflowdata_pingban_every_1_step";  // mesh.cpp:2197
+    int XflowStepOffset = 10014;                               // mesh.cpp:2192
 
     // ---- the reference's API ------------------------------------------
     void InitialLatMesh(int Nx_P, int Ny, double tau, Point2D StartVel, double Rho, int RankID,
@@ -82,6 +85,12 @@ public:
     void OutputCp(int RankID, int CoreNum, int time, double Radius);
     void MergeCp(int t, int CoreNum);
     void ComputeCp(int startcp, int t);
+    // XFlow coupling (mesh.cpp:2189-2766); files XflowDir/pb_<t + XflowStepOffset>.csv
+    vector<PointData> ReadXflowdata(int t);
+    void ManageDataFromXflow(int t);
+    void XflowABS(int t);
+    void FindAndWriteTau(int i, int j, int t);
+    void ChangeTauFromXflow(int t);
 
     // ---- additions ----------------------------------------------------
     // JudgeStyle marks the nodes within Radius of CylinderCenter1 as solid
@@ -113,6 +122,10 @@ private:
     int last_t_ = 0;
     std::vector<double> init_rho_, init_ux_, init_uy_;
     int cp_start_ = -1;
+    std::vector<double> tau_field_;  // the tau-field model's tau[Ny][Nx]
+    void reequilibrate_mirror();
+    void set_tau_node(int x, int y, double tau);
+    void upload_tau_field();
     bool check(int rc, const char* what);
     void ensure_synced();
 };

@@ -64,6 +64,13 @@ class Lattice:
         rho, ux, uy = _f64(rho, n), _f64(ux, n), _f64(uy, n)
         L.check(L.lib().ippi_init_macros(self._h, _p(rho), _p(ux), _p(uy)), self._h)
 
+    def reequilibrate(self, rho=None, ux=None, uy=None):
+        """Populations at the equilibrium of the given moments, keeping the
+        running means and the force history (a step must have been taken)."""
+        n = self.nx * self.ny
+        rho, ux, uy = _f64(rho, n), _f64(ux, n), _f64(uy, n)
+        L.check(L.lib().ippi_reequilibrate(self._h, _p(rho), _p(ux), _p(uy)), self._h)
+
     def set_markers(self, xy, ub=None, body=None, ds=None):
         xy = _f64(xy).reshape(-1)
         n = xy.size // 2
