@@ -75,6 +75,14 @@ extern "C" {
 #define IPPI_LES_LEARNED 2     /* per-node network (ippi_load_tau_mlp), Smagorinsky
                                   outside its training range; channel scene only */
 #define IPPI_LES_FIELD 3       /* a given relaxation time per node (ippi_set_tau_field) */
+/* The closures the reference keeps as alternatives in Mesh::CaculateLESTau
+ * (channel scene only): */
+#define IPPI_LES_WALE 4        /* WALE on forward-difference velocity gradients,
+                                  mesh.cpp:934-967 */
+#define IPPI_LES_CSM 5         /* coherent-structure Cs (ComputeDynamicCs), mesh.cpp:1034-1071,
+                                  2113-2146 */
+#define IPPI_LES_DYNAMIC 6     /* wall-damped Cs = 3 / (1 + 1.71828^(6 - d)),
+                                  mesh.cpp:968-1000; d from ippi_set_wall_distance */
 /* IB interpolation/spreading kernel */
 #define IPPI_DELTA_BILINEAR 0 /* mesh.cpp:606-644 (default of Parameter.h) */
 #define IPPI_DELTA_PESKIN4 1  /* Dirac_Delta, mesh.cpp:555-605, 1354-1389 */
@@ -281,6 +289,10 @@ int ippi_tau_scan_state(const double* f, const double* m3, const double* tau, in
  * reference sums it (before its 1/(rho U^2 R) scaling). */
 int ippi_set_solid(ippi_lbm* h, const uint8_t* solid, size_t n);
 int ippi_solid_force(ippi_lbm* h, double* force_xy);
+
+/* IPPI_LES_DYNAMIC: the wall distance d[ny][nx] of every node (Mesh::
+ * SetNormalDis, mesh.cpp:1935-1953, computes it for the cylinder). */
+int ippi_set_wall_distance(ippi_lbm* h, const double* dist);
 
 /* Last error message of the handle (or of the library when h is NULL). */
 int ippi_last_error(ippi_lbm* h, char* buf, size_t n);

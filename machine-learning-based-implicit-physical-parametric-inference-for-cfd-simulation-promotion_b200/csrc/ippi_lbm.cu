@@ -100,6 +100,8 @@ struct ippi_lbm {
     // learned tau: parameters (FP32 values of the BF16 weights) + statistics
     float* mlp_dev = nullptr;
     double* tau_field = nullptr;  // IPPI_LES_FIELD: [ny][nx]
+    void* mac = nullptr;          // IPPI_LES_WALE / CSM: [2][ny][nx] compute type, velocities
+    double* wall_dist = nullptr;  // IPPI_LES_DYNAMIC: [ny][nx]
     // solid nodes (halfway bounce-back) and their momentum-exchange links
     std::vector<uint8_t> solid;   // [ny][nx] or empty
     int2* solid_links = nullptr;  // (fluid node, direction into the solid)
@@ -647,6 +649,8 @@ LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int pa
     a.les = h->p.les_model;
     a.mlp = h->mlp_dev;
     a.tau_field = h->tau_field;
+    a.mac = h->mac;
+    a.wall_dist = h->wall_dist;
     a.plate_x0 = h->p.plate_x0;
     a.tau0 = h->p.tau0;
     a.cs = h->p.cs;
@@ -730,6 +734,8 @@ int tau_ready(ippi_lbm* h)
         return fail(h, IPPI_ERR_STATE, "learned tau selected but no network loaded (ippi_load_tau_mlp)");
     if (h->p.les_model == IPPI_LES_FIELD && !h->tau_field)
         return fail(h, IPPI_ERR_STATE, "tau field selected but none set (ippi_set_tau_field)");
+    if (h->p.les_model == IPPI_LES_DYNAMIC && !h->wall_dist)
+        return fail(h, IPPI_ERR_STATE, "wall-damped closure selected but no wall distance set (ippi_set_wall_distance)");
     return IPPI_OK;
 }
 
@@ -834,9 +840,11 @@ int ippi_create(const ippi_params* p, ippi_lbm** out)
     if (p->collision < 0 || p->collision > 2) return fail(nullptr, IPPI_ERR_ARG, "bad collision");
     if (p->storage < 0 || p->storage > 3) return fail(nullptr, IPPI_ERR_ARG, "bad storage");
     if (p->bc_set < 0 || p->bc_set > 1) return fail(nullptr, IPPI_ERR_ARG, "bad bc_set");
-    if (p->les_model < 0 || p->les_model > 3) return fail(nullptr, IPPI_ERR_ARG, "bad les_model");
+    if (p->les_model < 0 || p->les_model > 6) return fail(nullptr, IPPI_ERR_ARG, "bad les_model");
     if (p->les_model == IPPI_LES_LEARNED && p->bc_set != IPPI_BC_CHANNEL)
         return fail(nullptr, IPPI_ERR_ARG, "the learned relaxation time is built for the channel scene");
+    if (p->les_model >= IPPI_LES_WALE && p->bc_set != IPPI_BC_CHANNEL)
+        return fail(nullptr, IPPI_ERR_ARG, "the WALE, coherent and wall-damped closures are built for the channel scene");
     if (p->delta_kernel < 0 || p->delta_kernel > 1) return fail(nullptr, IPPI_ERR_ARG, "bad delta_kernel");
     if (!(p->tau0 > 0.5)) return fail(nullptr, IPPI_ERR_ARG, "tau0 must exceed 0.5");
     if (!(p->rho0 > 0)) return fail(nullptr, IPPI_ERR_ARG, "rho0 must be positive");
@@ -886,6 +894,9 @@ int ippi_create(const ippi_params* p, ippi_lbm** out)
         dalloc(&h->init_m, 3 * nn * sizeof(double)) != cudaSuccess ||
         dalloc(&h->red, 4096 * sizeof(double)) != cudaSuccess)
         return bail(fail(nullptr, IPPI_ERR_NOMEM, "device allocation failed"));
+    if ((p->les_model == IPPI_LES_WALE || p->les_model == IPPI_LES_CSM) &&
+        (dalloc(&h->mac, 2 * nn * h->csize) != cudaSuccess || cudaMemset(h->mac, 0, 2 * nn * h->csize) != cudaSuccess))
+        return bail(fail(nullptr, IPPI_ERR_NOMEM, "velocity field for the gradient closures"));
     cudaMemset(h->ctr, 0, sizeof(Ctr));
     cudaMemset(h->corner, 0, 24 * (size_t)h->csize);
     rc = rebuild(h);
@@ -905,6 +916,8 @@ int ippi_destroy(ippi_lbm* h)
     for (int b = 0; b < 2; b++) dfree(h->f[b]);
     dfree(h->mlp_dev);
     dfree(h->tau_field);
+    dfree(h->mac);
+    dfree(h->wall_dist);
     dfree(h->solid_links);
     dfree(h->solid_out);
     dfree(h->ctr);
@@ -1372,6 +1385,8 @@ int ippi_adjoint_forward(ippi_lbm* h, int nsteps, int t0, int ckpt_every)
     if (nsteps < 1 || ckpt_every < 1) return fail(h, IPPI_ERR_ARG, "nsteps and ckpt_every must be positive");
     if (h->p.bc_set != IPPI_BC_CHANNEL) return fail(h, IPPI_ERR_STATE, "the adjoint is built for the channel scene");
     if (!h->solid.empty()) return fail(h, IPPI_ERR_STATE, "the adjoint does not take solid nodes");
+    if (h->p.les_model >= IPPI_LES_WALE)
+        return fail(h, IPPI_ERR_STATE, "the adjoint takes the relaxation-time models 0-3");
     if (h->ib_active && h->p.mdf_iters != 1)
         return fail(h, IPPI_ERR_STATE, "the adjoint supports one direct-forcing pass (mdf_iters = 1)");
     if (h->ib_active && (long long)nsteps > h->hist_cap)
@@ -1622,5 +1637,20 @@ int ippi_solid_force(ippi_lbm* h, double* force_xy)
     CK(h, cudaGetLastError());
     CK(h, cudaMemcpyAsync(force_xy, h->solid_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     CK(h, cudaStreamSynchronize(h->st));
+    return IPPI_OK;
+}
+
+int ippi_set_wall_distance(ippi_lbm* h, const double* dist)
+{
+    if (!h || !dist) return fail(h, IPPI_ERR_ARG, "null argument");
+    const size_t nn = (size_t)h->p.nx * h->p.ny;
+    for (size_t i = 0; i < nn; i++)
+        if (!std::isfinite(dist[i])) return fail(h, IPPI_ERR_ARG, "wall distance must be finite (node %zu)", i);
+    CK(h, cudaSetDevice(h->p.device));
+    CK(h, cudaStreamSynchronize(h->st));
+    if (!h->wall_dist) CK(h, dalloc(&h->wall_dist, nn * sizeof(double)));
+    CK(h, cudaMemcpy(h->wall_dist, dist, nn * sizeof(double), cudaMemcpyHostToDevice));
+    drop_graphs(h);
+    h->dl_valid = false;
     return IPPI_OK;
 }

@@ -26,7 +26,7 @@ static void launch_prio(void (*kernel)(KArgs...), unsigned grid, unsigned block,
     cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-template <int S, int SC, int CO, bool LRN>
+template <int S, int SC, int CO, bool LRN, int XT = 0>
 static void launch_ib(const LaunchSet& L, cudaStream_t st)
 {
     // the whole IB sub-step: one cluster of kIbCtas CTAs
@@ -44,14 +44,52 @@ static void launch_ib(const LaunchSet& L, cudaStream_t st)
     cfg.attrs = attr;
     cfg.numAttrs = 2;
     if (L.ib_nst == 16)
-        cudaLaunchKernelEx(&cfg, ib_fused<S, SC, CO, LRN, 16>, L.ib_args, L.ib_passes);
+        cudaLaunchKernelEx(&cfg, ib_fused<S, SC, CO, LRN, 16, XT>, L.ib_args, L.ib_passes);
     else
-        cudaLaunchKernelEx(&cfg, ib_fused<S, SC, CO, LRN, 4>, L.ib_args, L.ib_passes);
+        cudaLaunchKernelEx(&cfg, ib_fused<S, SC, CO, LRN, 4, XT>, L.ib_args, L.ib_passes);
 }
 
-template <int S, int CO, int SC, bool LRN>
+template <int S, int CO, int SC, bool LRN, int XT = 0>
 static cudaError_t launch_tpl(const LaunchSet& L)
 {
+    // Closures that read neighbour velocities (WALE, coherent structure,
+    // wall-damped Cs): the post-stream velocities of all nodes first, then
+    // the IB kernel (which overwrites its nodes' with the corrected ones),
+    // then the bulk kernel, in stream order.  Channel scene only: no
+    // boundary-net work.
+    if (XT && L.step.les == 6 && L.step.mode == MODE_STEP && L.ib && !L.events) {
+        // the wall-damped closure is local: the same overlap of the IB
+        // kernel and its dependent bulk kernel as the normal step below
+        launch_ib<S, SC, CO, LRN, XT>(L, L.stream);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = L.grid;
+        cfg.blockDim = dim3(kBlockX);
+        cfg.stream = L.stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, LRN, XT>, L.step);
+        return cudaGetLastError();
+    }
+    if (XT) {
+        // timed launches: events 2-3 around the velocity pass and the IB
+        // kernel, 0-1 around the bulk kernel
+        if (L.events) cudaEventRecord(L.events[2], L.stream);
+        if (L.step.les != 6) mac_kernel<S, SC><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
+        if (L.ib) launch_ib<S, SC, CO, LRN, XT>(L, L.stream);
+        if (L.events) {
+            cudaEventRecord(L.events[3], L.stream);
+            cudaEventRecord(L.events[0], L.stream);
+        }
+        if (L.step.mode == MODE_STEP)
+            step_fast<S, CO, SC, LRN, XT><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
+        else
+            step_kernel<S, CO, SC, LRN, XT><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
+        if (L.events) cudaEventRecord(L.events[1], L.stream);
+        return cudaGetLastError();
+    }
     // Normal steps with markers and no boundary nets: IB cluster, then the
     // bulk kernel as its programmatic dependent, both on the main stream.
     // Timed launches (events) keep the side-stream form below, so the bulk
@@ -103,6 +141,14 @@ static cudaError_t launch_store(const LaunchSet& L)
         case CO_MRT: return launch_tpl<S, CO_MRT, SC_REF, false>(L);
         case CO_RR: return launch_tpl<S, CO_RR, SC_REF, false>(L);
         default: return launch_tpl<S, CO_BGK, SC_REF, false>(L);
+        }
+    }
+    // the closures 4..6 are built for the channel scene
+    if (L.step.les >= 4) {
+        switch (L.coll) {
+        case CO_MRT: return launch_tpl<S, CO_MRT, SC_CHANNEL, false, 1>(L);
+        case CO_RR: return launch_tpl<S, CO_RR, SC_CHANNEL, false, 1>(L);
+        default: return launch_tpl<S, CO_BGK, SC_CHANNEL, false, 1>(L);
         }
     }
     // the learned relaxation time (les == 2) is built for the channel scene

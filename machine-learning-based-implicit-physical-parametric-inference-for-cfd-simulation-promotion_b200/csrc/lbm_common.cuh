@@ -162,6 +162,61 @@ __device__ __forceinline__ C les_tau(C pxx, C pxy, C pyy, C rho, C tau0, C cs)
     return (sqrt(g1) + tau0) * C(0.5);
 }
 
+// The closures of Mesh::CaculateLESTau left as alternatives in the reference
+// (mesh.cpp:934-1071, 2113-2146), delta = 1.  g = (du/dx, du/dy, dv/dx,
+// dv/dy), the forward differences of GetDuxDx .. GetDuyDy.
+//
+// WALE (mesh.cpp:934-967): Cw = 0.45,
+// nu_t = Cw^2 (Gd:Gd)^3/2 / ((S:S)^5/2 + (Gd:Gd)^5/4 + 1e-12), tau = tau0 + 3 nu_t.
+template <typename C>
+__device__ __forceinline__ C wale_tau(const C* g, C tau0)
+{
+    const C gxx = g[0], gxy = g[1], gyx = g[2], gyy = g[3];
+    const C sxy = C(0.5) * (gxy + gyx);
+    const C ss = gxx * gxx + sxy * sxy + sxy * sxy + gyy * gyy;
+    const C gxx2 = gxx * gxx + gxy * gyx, gxy2 = gxx * gxy + gxy * gyy;
+    const C gyx2 = gyx * gxx + gyy * gyx, gyy2 = gyx * gxy + gyy * gyy;
+    const C grr2 = gxx * gxx + gxy * gyx + gyx * gxy + gyy * gyy;
+    const C dxx = C(0.5) * (gxx2 + gxx2) - grr2 / C(3.0);
+    const C dxy = C(0.5) * (gxy2 + gyx2);
+    const C dyy = C(0.5) * (gyy2 + gyy2) - grr2 / C(3.0);
+    const C gg = dxx * dxx + dxy * dxy + dxy * dxy + dyy * dyy;
+    const C vt = C(0.45 * 0.45) * pow(gg, C(1.5)) / (pow(ss, C(2.5)) + pow(gg, C(1.25)) + C(1e-12));
+    return tau0 + C(3) * vt;
+}
+
+// Coherent-structure model (mesh.cpp:1034-1071 with ComputeDynamicCs,
+// 2113-2146): F = |Q/E| from the gradient's rotation and strain,
+// C = F^3/2 (1 - F) / 11 (0.016 where E = 0), nu_t = C sqrt(2 Pi_neq:Pi_neq)
+// on the unscaled non-equilibrium moments, tau = tau0 + 3 nu_t.
+template <typename C>
+__device__ __forceinline__ C csm_tau(const C* g, C pxx, C pxy, C pyy, C tau0)
+{
+    const C sxy = C(0.5) * (g[1] + g[2]);
+    const C ss = g[0] * g[0] + sxy * sxy + sxy * sxy + g[3] * g[3];
+    const C wxy = C(0.5) * (g[1] - g[2]);
+    const C ww = C(2) * wxy * wxy;
+    const C q = C(0.5) * (ww - ss), e = C(0.5) * (ww + ss);
+    C ccsm = C(0.016);
+    if (e != C(0)) {
+        const C fcs = fabs(q / e);
+        ccsm = (C(1) / C(11.0)) * pow(fcs, C(1.5)) * (C(1) - fcs);
+    }
+    const C s2 = pxx * pxx + pxy * pxy + pxy * pxy + pyy * pyy;
+    return tau0 + C(3) * (ccsm * sqrt(C(2) * s2));
+}
+
+// Wall-damped ("dynamic") Cs (mesh.cpp:968-1000): Cs = 3 / (1 + 1.71828^(6 -
+// d)) at wall distance d, Q = sqrt(2 Pi_neq:Pi_neq) unscaled,
+// tau = tau0 + (sqrt(tau0^2 + 18 Cs^2 Q / rho) - tau0) / 2.
+template <typename C>
+__device__ __forceinline__ C dyncs_tau(C pxx, C pxy, C pyy, C rho, C tau0, C dist)
+{
+    const C sc = C(3) / (C(1) + pow(C(1.71828), C(6) - dist));
+    const C q = sqrt(C(2) * (pxx * pxx + pxy * pxy + pxy * pxy + pyy * pyy));
+    return tau0 + (sqrt(tau0 * tau0 + C(18) * sc * sc * q / rho) - tau0) / C(2);
+}
+
 // BGK (Lattice::ComputeBGKCollision, NodeAndLattice.cpp:150-161).
 template <typename C>
 __device__ __forceinline__ void collide_bgk(C* f, const C* feq, C tau)

@@ -57,6 +57,9 @@ struct StepArgs {
     const double* init_m; // [3][ny][nx] initial rho, ux, uy (INIT modes)
     const float* mlp;     // learned tau: parameters + feature statistics (LRN kernels)
     const double* tau_field; // les == 3: relaxation time per node [ny][nx]
+    void* mac;            // les 4, 5: [2][ny][nx] compute type, ux and uy of this step's
+                          // post-stream (and IB-corrected) state, for the velocity gradient
+    const double* wall_dist; // les 6: distance to the wall per node [ny][nx]
     double* dl_f;         // MAT: fnew [9][ny][nx]
     double* dl_m;         // MAT: rho, ux, uy, boundary-net flag [4][ny][nx]
     double* dl_tau;       // MAT: tau of the next collision [ny][nx]
@@ -369,6 +372,53 @@ __device__ __forceinline__ void solid_pull(const StepArgs& a, int x, int y, type
     }
 }
 
+// velocity gradient (du/dx, du/dy, dv/dx, dv/dy) by forward differences of
+// the stored velocities: GetDuxDx / GetDuyDx (mesh.cpp:1659-1724, 1795-1864)
+// give 0 in the last column and towards a solid node, GetDuxDy / GetDuyDy
+// (mesh.cpp:1725-1794, 1865-1934) from the second-to-last row up and towards
+// a solid node
+template <int S>
+__device__ __forceinline__ void vel_grad(const StepArgs& a, int x, int y, typename Store<S>::C* g)
+{
+    using C = typename Store<S>::C;
+    const C* m = reinterpret_cast<const C*>(a.mac);
+    const int pl = a.nx * a.ny, node = y * a.nx + x;
+    const C u0 = m[node], v0 = m[pl + node];
+    g[0] = g[1] = g[2] = g[3] = C(0);
+    if (x < a.nx - 1 && !(a.nflag[node + 1] & NF_SOLID)) {
+        g[0] = m[node + 1] - u0;
+        g[2] = m[pl + node + 1] - v0;
+    }
+    if (y + 1 < a.ny - 1 && !(a.nflag[node + a.nx] & NF_SOLID)) {
+        g[1] = m[node + a.nx] - u0;
+        g[3] = m[pl + node + a.nx] - v0;
+    }
+}
+
+// relaxation time of the closures 4 (WALE), 5 (coherent structure), 6 (wall-
+// damped Cs), from the post-stream state f / rho / u of node (x, y)
+template <int S>
+__device__ __forceinline__ typename Store<S>::C ext_tau(const StepArgs& a, int x, int y,
+                                                         const typename Store<S>::C* f,
+                                                         typename Store<S>::C rho, typename Store<S>::C ux,
+                                                         typename Store<S>::C uy, typename Store<S>::C rb)
+{
+    using C = typename Store<S>::C;
+    const C tau0 = prm<C>(a.tau0, a.f_tau0);
+    C g[4];
+    if (a.les == 4) {
+        vel_grad<S>(a, x, y, g);
+        return wale_tau<C>(g, tau0);
+    }
+    C pxx, pxy, pyy;
+    pi_neq<C>(f, rho, ux, uy, rb, pxx, pxy, pyy);
+    if (a.les == 5) {
+        vel_grad<S>(a, x, y, g);
+        return csm_tau<C>(g, pxx, pxy, pyy, tau0);
+    }
+    return dyncs_tau<C>(pxx, pxy, pyy, rho, tau0, C(a.wall_dist[y * a.nx + x]));
+}
+
 // post-stream state of node (x, y): the boundary rule of its kind and its
 // moments, or (INIT modes) the equilibrium of the initial moments
 template <int S, int SC>
@@ -436,7 +486,7 @@ __device__ __forceinline__ void node_epilogue(const StepArgs& a, long long node,
 // ---------------------------------------------------------------------------
 // (the learned-tau variant keeps the network's hidden layer in registers:
 // fewer resident blocks)
-template <int S, int CO, int SC, bool LRN>
+template <int S, int CO, int SC, bool LRN, int XT = 0>
 __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step_kernel(const StepArgs a)
 {
     using C = typename Store<S>::C;
@@ -468,9 +518,10 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
             }
             if (!deferred) {
                 node_epilogue<S>(a, node, t, f, rho, ux, uy);
-                const C tau = a.les == 3 ? C(a.tau_field[node])
-                                         : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
-                                                            prm<C>(a.cs, a.f_cs), a.mlp);
+                const C tau = XT            ? ext_tau<S>(a, x, y, f, rho, ux, uy, rbs)
+                              : a.les == 3 ? C(a.tau_field[node])
+                                           : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
+                                                              prm<C>(a.cs, a.f_cs), a.mlp);
                 if (a.mode >= MODE_MAT) {
                     a.dl_tau[node] = double(tau);
                 } else {
@@ -492,7 +543,7 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
 // its 9 populations from one base pointer at constant plane offsets.  Edge
 // nodes take the boundary rule of the scene.
 // ---------------------------------------------------------------------------
-template <int S, int CO, int SC, bool LRN>
+template <int S, int CO, int SC, bool LRN, int XT = 0>
 __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step_fast(const StepArgs ap)
 {
     using C = typename Store<S>::C;
@@ -535,8 +586,9 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
             }
             // Mesh::ErrorCatch (mesh.cpp:2103): rho outside [0, 10]; NaN too
             if (!(rho <= C(10) && rho >= C(0))) flag_error(a.ctr, t);
-            const C tau = a.les == 3 ? C(a.tau_field[node])
-                                     : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
+            const C tau = XT            ? ext_tau<S>(a, x, y, f, rho, ux, uy, rbs)
+                          : a.les == 3 ? C(a.tau_field[node])
+                                       : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
                                                         prm<C>(a.cs, a.f_cs), a.mlp);
             collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
             T* q = reinterpret_cast<T*>(a.f_out) + cell;
@@ -894,7 +946,7 @@ __device__ __forceinline__ void ib_body_sum(const IbArgs& ia, int b, int t, doub
 }
 
 // collision of a forced node with the corrected velocity and forcing term
-template <int S, int CO, bool LRN>
+template <int S, int CO, bool LRN, int XT>
 __device__ __forceinline__ void ib_collide_item(const IbArgs& ia, int n)
 {
     using C = typename Store<S>::C;
@@ -907,9 +959,10 @@ __device__ __forceinline__ void ib_collide_item(const IbArgs& ia, int n)
     const C ux = C(ia.ucx[n]), uy = C(ia.ucy[n]);
     const C rbs = rbase<S>(a);
     const int2 xy = ia.fn_xy[n];
-    const C tau = a.les == 3 ? C(a.tau_field[(long long)xy.y * a.nx + xy.x])
-                             : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
-                                                prm<C>(a.cs, a.f_cs), a.mlp);
+    const C tau = XT            ? ext_tau<S>(a, xy.x, xy.y, f, rho, ux, uy, rbs)
+                  : a.les == 3 ? C(a.tau_field[(long long)xy.y * a.nx + xy.x])
+                               : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
+                                                  prm<C>(a.cs, a.f_cs), a.mlp);
     if (a.mode >= MODE_MAT) {
         a.dl_tau[(long long)xy.y * a.nx + xy.x] = double(tau);
     } else {
@@ -921,7 +974,7 @@ __device__ __forceinline__ void ib_collide_item(const IbArgs& ia, int n)
 }
 
 // launched as exactly one cluster: gridDim.x == kIbCtas
-template <int S, int SC, int CO, bool LRN, int NST>
+template <int S, int SC, int CO, bool LRN, int NST, int XT = 0>
 __global__ void __launch_bounds__(kIbThreads) ib_fused(const IbArgs ia, int passes)
 {
     __shared__ double red[2][kIbThreads];
@@ -938,8 +991,45 @@ __global__ void __launch_bounds__(kIbThreads) ib_fused(const IbArgs ia, int pass
         for (int n = g; n < ia.nforced; n += T) ib_spread_item(ia, n);
         cluster_sync();
     }
+    if (XT && ia.s.les != 6) {
+        // the corrected velocities into the gradient field (WALE and the
+        // coherent model; the wall-damped closure has none), before any
+        // forced node reads its neighbours'
+        using C = typename Store<S>::C;
+        C* m = reinterpret_cast<C*>(ia.s.mac);
+        const int pl = ia.s.nx * ia.s.ny;
+        for (int n = g; n < ia.nforced; n += T) {
+            const int2 xy = ia.fn_xy[n];
+            m[xy.y * ia.s.nx + xy.x] = C(ia.ucx[n]);
+            m[pl + xy.y * ia.s.nx + xy.x] = C(ia.ucy[n]);
+        }
+        cluster_sync();
+    }
     for (int b = blockIdx.x; b < ia.nbody; b += gridDim.x) ib_body_sum(ia, b, t, red);
-    for (int n = g; n < ia.nforced; n += T) ib_collide_item<S, CO, LRN>(ia, n);
+    for (int n = g; n < ia.nforced; n += T) ib_collide_item<S, CO, LRN, XT>(ia, n);
+}
+
+// the post-stream velocity of every node into StepArgs::mac (closures 4, 5):
+// the state the step's collision sees, before the IB correction
+template <int S, int SC>
+__global__ void __launch_bounds__(kBlockX) mac_kernel(const StepArgs a)
+{
+    using C = typename Store<S>::C;
+    const int x = blockIdx.x * kBlockX + threadIdx.x, y = blockIdx.y;
+    if (x >= a.nx) return;
+    const int node = y * a.nx + x, pl = a.nx * a.ny;
+    const uint8_t nf = a.nflag[node];
+    C f[9], rho, ux = C(0), uy = C(0);
+    if (nf & NF_SOLID) {
+    } else if ((nf & NF_SBND) && a.mode != MODE_INIT && a.mode != MODE_MAT_INIT) {
+        solid_pull<S>(a, x, y, f);
+        macros<C>(f, rbase<S>(a), rho, ux, uy);
+    } else {
+        node_state<S, SC>(a, x, y, f, rho, ux, uy);
+    }
+    C* m = reinterpret_cast<C*>(a.mac);
+    m[node] = ux;
+    m[pl + node] = uy;
 }
 
 // ---------------------------------------------------------------------------

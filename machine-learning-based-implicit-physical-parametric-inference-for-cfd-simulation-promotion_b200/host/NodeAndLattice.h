@@ -54,6 +54,8 @@ public:
     REAL absRHO = 0;
     double xflowtau = 0;
     double abstau = 0;
+    double normalDis = 0;   // distance to the cylinder surface (Mesh::SetNormalDis)
+    double CoherentCS = 0;  // coherent-structure coefficient (Mesh::ComputeDynamicCs)
     char style = 'f';
     bool NNflag = false;
 

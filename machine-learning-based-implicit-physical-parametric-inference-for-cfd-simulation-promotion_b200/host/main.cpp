@@ -10,6 +10,7 @@
 //             [--cylinder X Y D] [--markers N] [--solid] [--cp START]
 //             [--nets DIR] [--init FILE] [--batched] [--print N] [--device N]
 //             [--xflow DIR] [--xflow-offset N] [--xflow-init] [--xflow-abs N]
+//             [--les none|smagorinsky|wale|csm|dynamic]
 //
 //   plate    the reference's scene: flat plate, NEE inlet u = --u, Re 5e5,
 //            tau = 0.5 + 6 (Ny U / Re) (main.cpp:37-43)
@@ -28,6 +29,11 @@
 //   --init FILE    initial rho, ux, uy as 3 x Ny x Nx float64 (raw)
 //   --batched      advance between save points in one call (CUDA graphs)
 //                  instead of one OneLBMStep call per step
+//   --les NAME     the relaxation-time closure (default: Parameter.h's);
+//                  wale / csm / dynamic are the alternatives the reference
+//                  keeps in Mesh::CaculateLESTau (channel scene); dynamic
+//                  damps Cs with the distance to the --cylinder surface
+//                  (Mesh::SetNormalDis)
 //   --xflow DIR    XFlow exports DIR/pb_<t + offset>.csv (offset 10014, or
 //                  --xflow-offset); --xflow-init: Mesh::ManageDataFromXflow
 //                  after step 1; --xflow-abs N: Mesh::XflowABS every N steps
@@ -59,6 +65,7 @@ struct Options {
     int xflow_offset = 10014;
     bool xflow_init = false;
     int xflow_abs = 0;
+    int les = -1;
     string nets, init;
     bool batched = false;
     int print = 1;
@@ -96,6 +103,13 @@ bool parse(int argc, char** argv, Options& o)
         else if (a == "--xflow-offset" && need(1)) o.xflow_offset = atoi(argv[++i]);
         else if (a == "--xflow-init") o.xflow_init = true;
         else if (a == "--xflow-abs" && need(1)) o.xflow_abs = atoi(argv[++i]);
+        else if (a == "--les" && need(1)) {
+            const string m = argv[++i];
+            o.les = m == "none" ? IPPI_LES_NONE : m == "smagorinsky" ? IPPI_LES_SMAGORINSKY
+                    : m == "wale" ? IPPI_LES_WALE : m == "csm" ? IPPI_LES_CSM
+                    : m == "dynamic" ? IPPI_LES_DYNAMIC : -2;
+            if (o.les == -2) return false;
+        }
         else if (a == "--cp" && need(1)) o.cp = atoi(argv[++i]);
         else if (a == "--nets" && need(1)) o.nets = argv[++i];
         else if (a == "--init" && need(1)) o.init = argv[++i];
@@ -131,7 +145,7 @@ int main(int argc, char* argv[])
                 "                 [--avg N] [--re R] [--u U] [--cs C] [--cylinder X Y D] [--markers N]\n"
                 "                 [--solid] [--cp START] [--nets DIR] [--init FILE] [--batched]\n"
                 "                 [--print N] [--device N] [--xflow DIR] [--xflow-offset N]\n"
-                "                 [--xflow-init] [--xflow-abs N]"
+                "                 [--xflow-init] [--xflow-abs N] [--les none|smagorinsky|wale|csm|dynamic]"
              << endl;
         return 2;
     }
@@ -158,6 +172,7 @@ int main(int argc, char* argv[])
     mesh.LatmeshSizeNx = Nx;
     mesh.LatmeshSizeNy = Ny;
     mesh.Device = o.device;
+    if (o.les >= 0) mesh.LesModel = o.les;
     if (!o.xflow.empty()) mesh.XflowDir = o.xflow;
     mesh.XflowStepOffset = o.xflow_offset;
     if (channel) {
@@ -170,6 +185,7 @@ int main(int argc, char* argv[])
     const bool solid = channel && o.cylinder && o.solid;
     mesh.SolidCylinder = solid;
     mesh.JudgeStyle(mesh.center, (REAL)mesh.radius, RankID, CoreNum);
+    if (mesh.LesModel == IPPI_LES_DYNAMIC) mesh.SetNormalDis();
     if (!o.init.empty()) {
         vector<double> m(3 * (size_t)Nx * Ny);
         ifstream in(o.init, ios::binary);

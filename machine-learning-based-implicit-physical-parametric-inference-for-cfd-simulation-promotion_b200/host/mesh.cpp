@@ -430,6 +430,77 @@ void Mesh::MergeCp(int t, int CoreNum)
     }
 }
 
+// Mesh::GetDuxDx .. GetDuyDy (mesh.cpp:1659-1934) on the mirror: forward
+// differences; 0 towards a solid node, in the last column and from the
+// second-to-last row up.  The device closures use the same rule.
+double Mesh::GetDuxDx(int i, int j)
+{
+    ensure_synced();
+    const int imax = i + 1, Nx = (int)LatMesh.size();
+    if (LatMesh[imax][j].style == 's' || imax == Nx - 1) return 0.0;
+    return (LatMesh[imax][j].u.x - LatMesh[i][j].u.x) / 1.0;
+}
+
+double Mesh::GetDuxDy(int i, int j)
+{
+    ensure_synced();
+    const int jmax = j + 1, Ny = (int)LatMesh[0].size();
+    if (jmax >= Ny - 1 || LatMesh[i][jmax].style == 's') return 0.0;
+    return (LatMesh[i][jmax].u.x - LatMesh[i][j].u.x) / 1.0;
+}
+
+double Mesh::GetDuyDx(int i, int j)
+{
+    ensure_synced();
+    const int imax = i + 1, Nx = (int)LatMesh.size();
+    if (LatMesh[imax][j].style == 's' || imax == Nx - 1) return 0.0;
+    return (LatMesh[imax][j].u.y - LatMesh[i][j].u.y) / 1.0;
+}
+
+double Mesh::GetDuyDy(int i, int j)
+{
+    ensure_synced();
+    const int jmax = j + 1, Ny = (int)LatMesh[0].size();
+    if (jmax >= Ny - 1 || LatMesh[i][jmax].style == 's') return 0.0;
+    return (LatMesh[i][jmax].u.y - LatMesh[i][j].u.y) / 1.0;
+}
+
+// Mesh::SetNormalDis (mesh.cpp:1935-1953): distance of every non-solid node
+// to the cylinder surface, measured from the mirror index (i, j) as the
+// reference does (for one rank: x + 1, y); handed to the wall-damped closure
+void Mesh::SetNormalDis()
+{
+    const int Nx = (int)LatMesh.size(), Ny = (int)LatMesh[0].size();
+    for (int i = 0; i < Nx; i++)
+        for (int j = 0; j < Ny; j++) {
+            if (LatMesh[i][j].style == 's') continue;
+            const double x = i, y = j, lx = center.x, ly = center.y;
+            LatMesh[i][j].normalDis = std::sqrt((x - lx) * (x - lx) + (y - ly) * (y - ly)) - radius;
+        }
+    if (!h_ || LesModel != IPPI_LES_DYNAMIC) return;
+    std::vector<double> d((size_t)nx_ * ny_);
+    for (int y = 0; y < ny_; y++)
+        for (int x = 0; x < nx_; x++) d[(size_t)y * nx_ + x] = LatMesh[x + 1][y].normalDis;
+    check(ippi_set_wall_distance(h_, d.data()), "ippi_set_wall_distance");
+}
+
+// Mesh::ComputeDynamicCs (mesh.cpp:2113-2146): the coherent-structure
+// coefficient of node (i, j) from the mirror's velocities
+double Mesh::ComputeDynamicCs(int i, int j)
+{
+    const double Sxx = 0.5 * (GetDuxDx(i, j) + GetDuxDx(i, j));
+    const double Sxy = 0.5 * (GetDuxDy(i, j) + GetDuyDx(i, j));
+    const double Syx = Sxy;
+    const double Syy = 0.5 * (GetDuyDy(i, j) + GetDuyDy(i, j));
+    const double SS = Sxx * Sxx + Sxy * Sxy + Syx * Syx + Syy * Syy;
+    const double Wxy = 0.5 * (GetDuxDy(i, j) - GetDuyDx(i, j));
+    const double WW = 2 * Wxy * Wxy;
+    const double Q = 0.5 * (WW - SS), E = 0.5 * (WW + SS);
+    if (E == 0) return LatMesh[i][j].CoherentCS = 0.016;
+    const double F = std::fabs(Q / E);
+    return LatMesh[i][j].CoherentCS = (1 / 11.0) * std::pow(F, 1.5) * (1 - F);
+}
+
 // ---------------------------------------------------------------------------
 // XFlow coupling.  The reference matches every node against every point
 // (O(nodes x points), mesh.cpp:2368-2390); a point lands on exactly one node,

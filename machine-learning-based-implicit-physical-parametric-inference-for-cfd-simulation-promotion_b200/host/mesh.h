@@ -85,6 +85,15 @@ public:
     void OutputCp(int RankID, int CoreNum, int time, double Radius);
     void MergeCp(int t, int CoreNum);
     void ComputeCp(int startcp, int t);
+    // velocity-gradient helpers and the closures' per-node inputs on the
+    // mirror (mesh.cpp:1659-1953, 2113-2146); SetNormalDis also hands the
+    // distances to the wall-damped closure (IPPI_LES_DYNAMIC)
+    double GetDuxDx(int i, int j);
+    double GetDuxDy(int i, int j);
+    double GetDuyDx(int i, int j);
+    double GetDuyDy(int i, int j);
+    void SetNormalDis();
+    double ComputeDynamicCs(int i, int j);
     // XFlow coupling (mesh.cpp:2189-2766); files XflowDir/pb_<t + XflowStepOffset>.csv
     vector<PointData> ReadXflowdata(int t);
     void ManageDataFromXflow(int t);

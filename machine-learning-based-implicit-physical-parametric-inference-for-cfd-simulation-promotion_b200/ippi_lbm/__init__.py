@@ -7,7 +7,8 @@ Lattice, main.cpp) is mirrored in C++ by ../host/ over the same ABI.
 from ._lib import (BC_CHANNEL, BC_REF_NEE, BF16, BGK, DELTA_BILINEAR, DELTA_PESKIN4, F16, F32,
                    F64, FIELD_AVG_RHO, FIELD_AVG_U, FIELD_AVG_V, FIELD_F, FIELD_FLAGS,
                    FIELD_NNFLAG, FIELD_RHO, FIELD_TAU, FIELD_UX, FIELD_UY, LES_NONE,
-                   LES_FIELD, LES_LEARNED, LES_SMAGORINSKY, MRT, RR, DivergedError, IppiError, lib)
+                   LES_CSM, LES_DYNAMIC, LES_FIELD, LES_LEARNED, LES_SMAGORINSKY, LES_WALE, MRT, RR,
+                   DivergedError, IppiError, lib)
 from . import scenes
 from .lattice import Lattice
 
@@ -15,4 +16,4 @@ __all__ = ["Lattice", "lib", "IppiError", "DivergedError", "BGK", "MRT", "RR", "
            "F16", "BF16", "BC_REF_NEE", "BC_CHANNEL", "LES_NONE", "LES_SMAGORINSKY",
            "DELTA_BILINEAR", "DELTA_PESKIN4", "FIELD_F", "FIELD_RHO", "FIELD_UX", "FIELD_UY",
            "FIELD_TAU", "FIELD_AVG_U", "FIELD_AVG_V", "FIELD_AVG_RHO", "FIELD_FLAGS",
-           "FIELD_NNFLAG", "LES_LEARNED", "LES_FIELD"]
+           "FIELD_NNFLAG", "LES_LEARNED", "LES_FIELD", "LES_WALE", "LES_CSM", "LES_DYNAMIC"]

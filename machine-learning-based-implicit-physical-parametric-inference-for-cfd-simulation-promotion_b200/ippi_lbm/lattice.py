@@ -168,6 +168,11 @@ class Lattice:
             out["f0"] = gf
         return out
 
+    def set_wall_distance(self, dist):
+        """Wall distance per node [ny][nx] for the wall-damped closure."""
+        d = _f64(dist, self.nx * self.ny)
+        L.check(L.lib().ippi_set_wall_distance(self._h, _p(d)), self._h)
+
     def set_solid(self, mask):
         """Solid nodes: mask[ny][nx] (nonzero = solid); None removes them."""
         if mask is None:

@@ -54,6 +54,7 @@ struct orc {
     double* tau_field;          /* les_model 3: tau per node, [ny][nx] global */
     int mlp_loaded;
     unsigned char* solid;       /* [NX*NY] solid nodes, or NULL */
+    double* wall_dist;          /* les_model 6: [ny][nx] global */
 };
 
 #define ID(s, i, j) ((size_t)(i) * (size_t)(s)->NY + (size_t)(j))
@@ -146,6 +147,96 @@ double orc_les_tau(const double* fnew, double rho, double ux, double uy,
     double Q = sqrt(2.0 * S2);
     double g1 = tau0 * tau0 + 18.0 * cs * cs * Q / (rhoTemp);
     return (sqrt(g1) + tau0) / 2.0;
+}
+
+/* Mesh::GetDuxDx / GetDuyDx (mesh.cpp:1659-1724, 1795-1864) and GetDuxDy /
+ * GetDuyDy (1725-1794, 1865-1934) on one rank: forward differences of the
+ * current u (comp 0) or v (comp 1) along x (dir 0) or y (dir 1); 0 towards a
+ * solid node, in the last column (imax = NX - 1) and from the second-to-last
+ * row up (jmax >= Ny - 1). */
+static double grad_u(const orc* s, int i, int j, int comp, int dir)
+{
+    const double* u = comp ? s->uy : s->ux;
+    if (dir == 0) {
+        int imax = i + 1;
+        if ((s->solid && s->solid[ID(s, imax, j)]) || imax == s->NX - 1) return 0.0;
+        return (u[ID(s, imax, j)] - u[ID(s, i, j)]) / 1.0;
+    }
+    int jmax = j + 1;
+    if (jmax >= s->NY - 1 || (s->solid && s->solid[ID(s, i, jmax)])) return 0.0;
+    return (u[ID(s, i, jmax)] - u[ID(s, i, j)]) / 1.0;
+}
+
+/* sum_k e_a e_b (fnew - feq) */
+static void pi_noneq(const double* fnew, double rho, double ux, double uy, double* qxx, double* qxy,
+                     double* qyy)
+{
+    double feq[9];
+    compute_feq(rho, ux, uy, feq);
+    *qxx = *qxy = *qyy = 0.0;
+    for (int k = 0; k < 9; k++) {
+        *qxx += E[k][0] * E[k][0] * (fnew[k] - feq[k]);
+        *qxy += E[k][0] * E[k][1] * (fnew[k] - feq[k]);
+        *qyy += E[k][1] * E[k][1] * (fnew[k] - feq[k]);
+    }
+}
+
+/* The alternative closures of Mesh::CaculateLESTau for node (i, j):
+ * 4 WALE (mesh.cpp:934-967), 5 coherent structure (1034-1071 with
+ * ComputeDynamicCs, 2113-2146), 6 wall-damped Cs (968-1000). */
+static double ext_tau(const orc* s, int i, int j, const double* fnew, double rho, double ux, double uy)
+{
+    double startTau = s->p.tau0, delta = 1.0;
+    if (s->p.les_model == 4) {
+        double Cw = 0.45;
+        double gxx = grad_u(s, i, j, 0, 0), gxy = grad_u(s, i, j, 0, 1);
+        double gyx = grad_u(s, i, j, 1, 0), gyy = grad_u(s, i, j, 1, 1);
+        double Sxx = 0.5 * (gxx + gxx), Sxy = 0.5 * (gxy + gyx), Syx = Sxy, Syy = 0.5 * (gyy + gyy);
+        double SS = Sxx * Sxx + Sxy * Sxy + Syx * Syx + Syy * Syy;
+        double gxx2 = gxx * gxx + gxy * gyx, gxy2 = gxx * gxy + gxy * gyy;
+        double gyx2 = gyx * gxx + gyy * gyx, gyy2 = gyx * gxy + gyy * gyy;
+        double grr2 = gxx * gxx + gxy * gyx + gyx * gxy + gyy * gyy;
+        double Gxx = 0.5 * (gxx2 + gxx2) - grr2 / 3.0, Gxy = 0.5 * (gxy2 + gyx2);
+        double Gyx = 0.5 * (gyx2 + gxy2), Gyy = 0.5 * (gyy2 + gyy2) - grr2 / 3.0;
+        double GG = Gxx * Gxx + Gxy * Gxy + Gyx * Gyx + Gyy * Gyy;
+        double vt = Cw * Cw * delta * delta * pow(GG, 1.5) / (pow(SS, 2.5) + pow(GG, 1.25) + 1e-12);
+        return startTau + 3 * vt;
+    }
+    double Qxx, Qxy, Qyy;
+    pi_noneq(fnew, rho, ux, uy, &Qxx, &Qxy, &Qyy);
+    double Qyx = Qxy;
+    if (s->p.les_model == 5) {
+        double gxx = grad_u(s, i, j, 0, 0), gxy = grad_u(s, i, j, 0, 1);
+        double gyx = grad_u(s, i, j, 1, 0), gyy = grad_u(s, i, j, 1, 1);
+        double Sxx = 0.5 * (gxx + gxx), Sxy = 0.5 * (gxy + gyx), Syx = Sxy, Syy = 0.5 * (gyy + gyy);
+        double SS = Sxx * Sxx + Sxy * Sxy + Syx * Syx + Syy * Syy;
+        double Wxy = 0.5 * (gxy - gyx);
+        double WW = 2 * Wxy * Wxy;
+        double Q = 0.5 * (WW - SS), Ev = 0.5 * (WW + SS);
+        double Ccsm;
+        if (Ev == 0) {
+            Ccsm = 0.016;
+        } else {
+            double Fcs = fabs(Q / Ev);
+            Ccsm = (1 / 11.0) * pow(Fcs, 1.5) * (1 - Fcs);
+        }
+        double S2 = Qxx * Qxx + Qxy * Qxy + Qyx * Qyx + Qyy * Qyy;
+        double vt = Ccsm * delta * delta * sqrt(2 * S2);
+        return startTau + 3 * vt;
+    }
+    double d = s->wall_dist[(size_t)j * s->p.nx + (i - 1)];
+    double SC = 3.0 / (1 + pow(1.71828, 6.0 - 1.0 * d));
+    double Q = sqrt(2 * (Qxx * Qxx + Qxy * Qxy + Qyx * Qyx + Qyy * Qyy));
+    double tauT = (sqrt(startTau * startTau + 18.0 * delta * SC * SC * Q / rho) - startTau) / 2.0;
+    return startTau + tauT;
+}
+
+int orc_set_wall_distance(orc* s, const double* d)
+{
+    size_t n = (size_t)s->p.nx * s->p.ny;
+    if (!s->wall_dist) s->wall_dist = (double*)malloc(n * sizeof(double));
+    memcpy(s->wall_dist, d, n * sizeof(double));
+    return 0;
 }
 
 /* Learned relaxation time (no reference code).  Features from the node's
@@ -564,6 +655,7 @@ void orc_destroy(orc* s)
     free(s->body_force);
     free(s->tau_field);
     free(s->solid);
+    free(s->wall_dist);
     for (int t = 0; t < 8; t++) free(s->nets[t].w);
     free(s);
 }
@@ -817,7 +909,11 @@ static int collide_all(orc* s)
             double fn[9], fc[9];
             for (int k = 0; k < 9; k++) fn[k] = FN(s, k, i, j);
             int use_les = s->p.les_model == 1 && !(coll == COLL_BGK && s->nnflag[id]);
-            if (s->p.les_model == 3 && !(coll == COLL_BGK && s->nnflag[id]))
+            if (s->solid && s->solid[id])
+                s->tau[id] = s->p.tau0;
+            else if (s->p.les_model >= 4)
+                s->tau[id] = ext_tau(s, i, j, fn, r, s->ux[id], s->uy[id]);
+            else if (s->p.les_model == 3 && !(coll == COLL_BGK && s->nnflag[id]))
                 s->tau[id] = s->tau_field[(size_t)j * s->p.nx + (i - 1)];
             else if (s->p.les_model == 2)
                 s->tau[id] = orc_learned_tau(fn, r, s->ux[id], s->uy[id], s->p.tau0, s->p.cs, s->mlp);
@@ -1033,6 +1129,7 @@ int orc_step(orc* s, int nsteps, int t0)
     int status = 0;
     if (s->p.les_model == 2 && !s->mlp_loaded) return -1;
     if (s->p.les_model == 3 && !s->tau_field) return -1;
+    if (s->p.les_model == 6 && !s->wall_dist) return -1;
     for (int t = t0; t < t0 + nsteps; t++) {
         ib_substep(s);
         if (s->p.collision == COLL_BGK) nn_band(s);
@@ -1081,8 +1178,12 @@ static void next_tau(orc* s, double* tau_out, unsigned char* flag_out)
             for (int k = 0; k < 9; k++) fn[k] = FN(s, k, i, j);
             double t;
             int nnf = (s->p.collision == COLL_BGK) && s->nnflag[id];
-            if (nnf)
+            if (s->solid && s->solid[id])
+                t = s->p.tau0; /* a solid node reads as fluid at rest */
+            else if (nnf)
                 t = s->tau[id];
+            else if (s->p.les_model >= 4)
+                t = ext_tau(s, i, j, fn, s->rho[id], s->ux[id], s->uy[id]);
             else if (s->p.les_model == 3)
                 t = s->tau_field[(size_t)j * s->p.nx + (i - 1)];
             else if (s->p.les_model == 2)

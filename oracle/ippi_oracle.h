@@ -48,7 +48,9 @@ typedef struct {
     int collision;       /* 0 BGK, 1 MRT, 2 RR                                   */
     int bc_set;          /* 0 reference flat plate (NEE), 1 channel (ZH/ZG/BB)   */
     int les_model;       /* 0 constant tau0, 1 Smagorinsky "hybrid", 2 learned,
-                            3 given tau per node (orc_set_tau_field)            */
+                            3 given tau per node (orc_set_tau_field), 4 WALE,
+                            5 coherent structure, 6 wall-damped Cs
+                            (orc_set_wall_distance)                              */
     double tau0;         /* startTau                                              */
     double cs;           /* Smagorinsky constant                                 */
     double u_in;         /* inlet velocity (flat plate) / u_max (channel)         */
@@ -119,6 +121,8 @@ void orc_force_node(int collision, double ux, double uy, double fx, double fy, d
  * W2[32][32] b2[32] w3[32] b3) and stats[25] (mean[6] std[6] lo[6] hi[6]
  * out_scale).  Returns 0, or -1 on a bad size. */
 int orc_load_tau_mlp(orc* s, const float* w, size_t n, const float* stats, size_t nstats);
+/* wall distance per node for les_model 6 (wall-damped Cs): [ny][nx] global. */
+int orc_set_wall_distance(orc* s, const double* d);
 /* tau per node for les_model 3: [ny][nx] global. */
 int orc_set_tau_field(orc* s, const double* tau);
 /* Mesh::FindAndWriteTau's scan (mesh.cpp:2625-2715) over candidates m_lo..m_hi

@@ -75,6 +75,7 @@ def lib() -> C.CDLL:
         L.orc_les_tau.argtypes = [_dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
         L.orc_set_tau_field.argtypes = [C.c_void_p, _dp]
         L.orc_set_solid.argtypes = [C.c_void_p, C.POINTER(C.c_uint8)]
+        L.orc_set_wall_distance.argtypes = [C.c_void_p, _dp]
         L.orc_solid_force.argtypes = [C.c_void_p, _dp]
         L.orc_tau_scan_state.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, C.c_int,
                                          C.POINTER(C.c_int), _dp, C.c_int, C.c_int, C.c_double,
@@ -149,6 +150,10 @@ class Oracle:
     def set_tau_field(self, tau):
         tau = np.ascontiguousarray(tau, dtype=np.float64)
         lib().orc_set_tau_field(self._h, _ptr(tau))
+
+    def set_wall_distance(self, d):
+        d = np.ascontiguousarray(d, dtype=np.float64)
+        lib().orc_set_wall_distance(self._h, _ptr(d))
 
     def set_solid(self, mask):
         m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
