@@ -74,7 +74,8 @@ extern "C" {
 #define IPPI_LES_SMAGORINSKY 1 /* SmagorinskyByHybrid, mesh.cpp:852-911 */
 #define IPPI_LES_LEARNED 2     /* per-node network (ippi_load_tau_mlp), Smagorinsky
                                   outside its training range; channel scene only */
-#define IPPI_LES_FIELD 3       /* a given relaxation time per node (ippi_set_tau_field) */
+#define IPPI_LES_FIELD 3       /* a given relaxation time per node (ippi_set_tau_field);
+                                  channel scene */
 /* The closures the reference keeps as alternatives in Mesh::CaculateLESTau
  * (channel scene only): */
 #define IPPI_LES_WALE 4        /* WALE on forward-difference velocity gradients,

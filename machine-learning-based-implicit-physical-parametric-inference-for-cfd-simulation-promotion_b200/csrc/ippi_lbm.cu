@@ -117,8 +117,12 @@ struct ippi_lbm {
     } adj;
     bool no_avg = false;         // forward recomputes must not touch the averages
     // graphs of two steps and of one step: [start buffer][step parity]
-    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-    cudaGraphExec_t graph1[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    // step graphs by [start buffer][parity of the first step][averaging]
+    cudaGraphExec_t graph[2][2][2] = {};
+    cudaGraphExec_t graph1[2][2][2] = {};
+    // rows with flagged tiles (StepArgs::rowmask / row_shift)
+    unsigned rowmask[kRowMaskWords] = {};
+    int row_shift = 0;
     char err[512] = "";
 };
 
@@ -216,11 +220,12 @@ void drop_graphs(ippi_lbm* h)
 {
     for (int b = 0; b < 2; b++)
         for (int q = 0; q < 2; q++)
-            for (cudaGraphExec_t* g : {&h->graph[b][q], &h->graph1[b][q]})
-                if (*g) {
-                    cudaGraphExecDestroy(*g);
-                    *g = nullptr;
-                }
+            for (int v = 0; v < 2; v++)
+                for (cudaGraphExec_t* g : {&h->graph[b][q][v], &h->graph1[b][q][v]})
+                    if (*g) {
+                        cudaGraphExecDestroy(*g);
+                        *g = nullptr;
+                    }
 }
 
 void adjoint_free(ippi_lbm* h)
@@ -450,6 +455,16 @@ int rebuild(ippi_lbm* h)
             }
         }
 
+    // rows holding a flagged tile, in groups of 2^row_shift rows per bit
+    h->row_shift = 0;
+    while (((ny - 1) >> h->row_shift) >= kRowMaskWords * 32) h->row_shift++;
+    std::memset(h->rowmask, 0, sizeof h->rowmask);
+    for (int y = 0; y < ny; y++)
+        for (int bx = 0; bx < h->gx; bx++)
+            if (tile[(size_t)y * h->gx + bx]) {
+                const int r = y >> h->row_shift;
+                h->rowmask[r >> 5] |= 1u << (r & 31);
+            }
     CK(h, cudaMemcpy(h->nflag, defer.data(), nn, cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->tile, tile.data(), tile.size(), cudaMemcpyHostToDevice));
     dfree(h->prep_d);
@@ -651,6 +666,8 @@ LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int pa
     a.tau_field = h->tau_field;
     a.mac = h->mac;
     a.wall_dist = h->wall_dist;
+    std::memcpy(a.rowmask, h->rowmask, sizeof a.rowmask);
+    a.row_shift = h->row_shift;
     a.plate_x0 = h->p.plate_x0;
     a.tau0 = h->p.tau0;
     a.cs = h->p.cs;
@@ -756,16 +773,19 @@ int run_init(ippi_lbm* h)
     return IPPI_OK;
 }
 
-// n (1 or 2) steps starting from buffer b with parity q, as one CUDA graph
-int build_graph(ippi_lbm* h, int n, int b, int q)
+// n (1 or 2) steps starting from buffer b with parity q, with or without
+// the running means (av), as one CUDA graph
+int build_graph(ippi_lbm* h, int n, int b, int q, int av)
 {
     cudaGraph_t g;
-    cudaGraphExec_t& slot = n == 2 ? h->graph[b][q] : h->graph1[b][q];
+    cudaGraphExec_t& slot = n == 2 ? h->graph[b][q][av] : h->graph1[b][q][av];
     CK(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
     LaunchSet L0 = make_launch(h, MODE_STEP, h->f[b], h->f[b ^ 1], q);
+    L0.avg_on = av;
     cudaError_t e0 = launch(L0, h->S), e1 = cudaSuccess;
     if (n == 2) {
         LaunchSet L1 = make_launch(h, MODE_STEP, h->f[b ^ 1], h->f[b], q ^ 1);
+        L1.avg_on = av;
         e1 = launch(L1, h->S);
     }
     cudaError_t ec = cudaStreamEndCapture(h->st, &g);
@@ -843,8 +863,9 @@ int ippi_create(const ippi_params* p, ippi_lbm** out)
     if (p->les_model < 0 || p->les_model > 6) return fail(nullptr, IPPI_ERR_ARG, "bad les_model");
     if (p->les_model == IPPI_LES_LEARNED && p->bc_set != IPPI_BC_CHANNEL)
         return fail(nullptr, IPPI_ERR_ARG, "the learned relaxation time is built for the channel scene");
-    if (p->les_model >= IPPI_LES_WALE && p->bc_set != IPPI_BC_CHANNEL)
-        return fail(nullptr, IPPI_ERR_ARG, "the WALE, coherent and wall-damped closures are built for the channel scene");
+    if (p->les_model >= IPPI_LES_FIELD && p->bc_set != IPPI_BC_CHANNEL)
+        return fail(nullptr, IPPI_ERR_ARG,
+                    "the tau field and the WALE, coherent and wall-damped closures are built for the channel scene");
     if (p->delta_kernel < 0 || p->delta_kernel > 1) return fail(nullptr, IPPI_ERR_ARG, "bad delta_kernel");
     if (!(p->tau0 > 0.5)) return fail(nullptr, IPPI_ERR_ARG, "tau0 must exceed 0.5");
     if (!(p->rho0 > 0)) return fail(nullptr, IPPI_ERR_ARG, "rho0 must be positive");
@@ -1096,25 +1117,22 @@ int ippi_step(ippi_lbm* h, int nsteps, int t0)
     }
     int rc = set_time(h, t0);
     if (rc) return rc;
-    int left = nsteps;
-    const int q = h->kcount & 1;  // parity of the first step; graphs keep it
-    while (left >= 2) {
-        if (!h->graph[h->cur][q]) {
-            rc = build_graph(h, 2, h->cur, q);
+    // two steps per graph, one where the averaging starts between them and
+    // for an odd last step (a driver calling once per step)
+    const long long avs = h->no_avg ? 0x7fffffffll : (long long)h->p.avg_start;
+    for (int done = 0; done < nsteps;) {
+        const long long t = (long long)t0 + done;
+        const int q = (int)((h->kcount + done) & 1);
+        const int av = t >= avs;
+        const int n = (nsteps - done >= 2 && (av || t + 1 < avs)) ? 2 : 1;
+        cudaGraphExec_t& g = n == 2 ? h->graph[h->cur][q][av] : h->graph1[h->cur][q][av];
+        if (!g) {
+            rc = build_graph(h, n, h->cur, q, av);
             if (rc) return rc;
         }
-        CK(h, cudaGraphLaunch(h->graph[h->cur][q], h->st));
-        left -= 2;
-    }
-    if (left) {
-        // one step (a driver calling once per step): its own graph
-        const int q1 = q;  // an even number of steps came before in this call
-        if (!h->graph1[h->cur][q1]) {
-            rc = build_graph(h, 1, h->cur, q1);
-            if (rc) return rc;
-        }
-        CK(h, cudaGraphLaunch(h->graph1[h->cur][q1], h->st));
-        h->cur ^= 1;
+        CK(h, cudaGraphLaunch(g, h->st));
+        if (n == 1) h->cur ^= 1;
+        done += n;
     }
     h->kcount += nsteps;
     h->last_t = t0 + nsteps - 1;
@@ -1143,6 +1161,7 @@ int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk, double*
     for (auto& e : ev) CK(h, cudaEventCreate(&e));
     for (int s = 0; s < nsteps; s++) {
         LaunchSet L = make_launch(h, MODE_STEP, h->f[h->cur], h->f[h->cur ^ 1], (h->kcount + s) & 1);
+        L.avg_on = (long long)t0 + s >= (long long)L.step.avg_start;
         L.events = &ev[(size_t)s * 4];
         CK(h, launch(L, h->S));
         h->cur ^= 1;

@@ -49,42 +49,61 @@ static void launch_ib(const LaunchSet& L, cudaStream_t st)
         cudaLaunchKernelEx(&cfg, ib_fused<S, SC, CO, LRN, 4, XT>, L.ib_args, L.ib_passes);
 }
 
+// the bulk kernel of a normal step, optionally as the programmatic
+// dependent of the kernel launched before it on the stream
+template <int S, int CO, int SC, bool LRN, int XT>
+static void launch_bulk(const LaunchSet& L, bool pdl)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = L.grid;
+    cfg.blockDim = dim3(kBlockX);
+    cfg.stream = L.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    if (pdl) {
+        if (L.avg_on)
+            cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, LRN, XT, 1, 1>, L.step);
+        else
+            cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, LRN, XT, 0, 1>, L.step);
+    } else {
+        if (L.avg_on)
+            cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, LRN, XT, 1, 0>, L.step);
+        else
+            cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, LRN, XT, 0, 0>, L.step);
+    }
+}
+
 template <int S, int CO, int SC, bool LRN, int XT = 0>
 static cudaError_t launch_tpl(const LaunchSet& L)
 {
-    // Closures that read neighbour velocities (WALE, coherent structure,
-    // wall-damped Cs): the post-stream velocities of all nodes first, then
-    // the IB kernel (which overwrites its nodes' with the corrected ones),
-    // then the bulk kernel, in stream order.  Channel scene only: no
-    // boundary-net work.
-    if (XT && L.step.les == 6 && L.step.mode == MODE_STEP && L.ib && !L.events) {
-        // the wall-damped closure is local: the same overlap of the IB
-        // kernel and its dependent bulk kernel as the normal step below
+    // Closures that read neighbour velocities (WALE, coherent structure):
+    // the post-stream velocities of all nodes first, then the IB kernel
+    // (which overwrites its nodes' with the corrected ones), then the bulk
+    // kernel, in stream order; the local models (tau field, wall-damped Cs)
+    // in timed launches.  Channel scene only: no boundary-net work.
+    if (XT && (L.step.les == 3 || L.step.les == 6) && L.step.mode == MODE_STEP && L.ib && !L.events) {
+        // the tau field and the wall-damped closure are local: the same
+        // overlap of the IB kernel and its dependent bulk kernel as the
+        // normal step below
         launch_ib<S, SC, CO, LRN, XT>(L, L.stream);
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = L.grid;
-        cfg.blockDim = dim3(kBlockX);
-        cfg.stream = L.stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, LRN, XT>, L.step);
+        launch_bulk<S, CO, SC, LRN, XT>(L, true);
         return cudaGetLastError();
     }
     if (XT) {
         // timed launches: events 2-3 around the velocity pass and the IB
         // kernel, 0-1 around the bulk kernel
         if (L.events) cudaEventRecord(L.events[2], L.stream);
-        if (L.step.les != 6) mac_kernel<S, SC><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
+        if (L.step.les == 4 || L.step.les == 5) mac_kernel<S, SC><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
         if (L.ib) launch_ib<S, SC, CO, LRN, XT>(L, L.stream);
         if (L.events) {
             cudaEventRecord(L.events[3], L.stream);
             cudaEventRecord(L.events[0], L.stream);
         }
         if (L.step.mode == MODE_STEP)
-            step_fast<S, CO, SC, LRN, XT><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
+            launch_bulk<S, CO, SC, LRN, XT>(L, false);
         else
             step_kernel<S, CO, SC, LRN, XT><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
         if (L.events) cudaEventRecord(L.events[1], L.stream);
@@ -96,16 +115,7 @@ static cudaError_t launch_tpl(const LaunchSet& L)
     // kernel's own duration can be measured.
     if (L.step.mode == MODE_STEP && L.ib && !L.band && L.nprep == 0 && !L.events) {
         launch_ib<S, SC, CO, LRN>(L, L.stream);
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = L.grid;
-        cfg.blockDim = dim3(kBlockX);
-        cfg.stream = L.stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, LRN>, L.step);
+        launch_bulk<S, CO, SC, LRN, 0>(L, true);
         return cudaGetLastError();
     }
     const bool side = L.nprep > 0 || L.band || L.ib;
@@ -125,7 +135,7 @@ static cudaError_t launch_tpl(const LaunchSet& L)
     }
     if (L.events) cudaEventRecord(L.events[0], L.stream);
     if (L.step.mode == MODE_STEP)
-        step_fast<S, CO, SC, LRN><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
+        launch_bulk<S, CO, SC, LRN, 0>(L, false);
     else
         step_kernel<S, CO, SC, LRN><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
     if (L.events) cudaEventRecord(L.events[1], L.stream);
@@ -143,8 +153,8 @@ static cudaError_t launch_store(const LaunchSet& L)
         default: return launch_tpl<S, CO_BGK, SC_REF, false>(L);
         }
     }
-    // the closures 4..6 are built for the channel scene
-    if (L.step.les >= 4) {
+    // the tau field (3) and the closures 4..6 are built for the channel scene
+    if (L.step.les >= 3) {
         switch (L.coll) {
         case CO_MRT: return launch_tpl<S, CO_MRT, SC_CHANNEL, false, 1>(L);
         case CO_RR: return launch_tpl<S, CO_RR, SC_CHANNEL, false, 1>(L);

@@ -28,6 +28,9 @@ struct LaunchSet {
     // optional device timing: events[0..3] around the bulk kernel and the
     // side-stream chain (only when not capturing)
     cudaEvent_t* events;
+    // this step updates the running means (t >= avg_start): the bulk
+    // kernel's averaging instance
+    bool avg_on;
 };
 
 // Mesh::FindAndWriteTau's scan (tau_scan.cu) on device arrays

@@ -30,6 +30,9 @@
 namespace ippi {
 
 constexpr int kBlockX = 256;
+// rows (in groups of 2^row_shift) with any flagged tile, one bit each, as a
+// kernel parameter: the bulk kernel reads the tile flags only in those rows
+constexpr int kRowMaskWords = 128;
 
 struct StepArgs {
     const void* f_in;   // post-collision populations of the previous step
@@ -60,6 +63,8 @@ struct StepArgs {
     void* mac;            // les 4, 5: [2][ny][nx] compute type, ux and uy of this step's
                           // post-stream (and IB-corrected) state, for the velocity gradient
     const double* wall_dist; // les 6: distance to the wall per node [ny][nx]
+    unsigned rowmask[kRowMaskWords]; // bit (y >> row_shift): a tile of row y is flagged
+    int row_shift;
     double* dl_f;         // MAT: fnew [9][ny][nx]
     double* dl_m;         // MAT: rho, ux, uy, boundary-net flag [4][ny][nx]
     double* dl_tau;       // MAT: tau of the next collision [ny][nx]
@@ -395,8 +400,9 @@ __device__ __forceinline__ void vel_grad(const StepArgs& a, int x, int y, typena
     }
 }
 
-// relaxation time of the closures 4 (WALE), 5 (coherent structure), 6 (wall-
-// damped Cs), from the post-stream state f / rho / u of node (x, y)
+// relaxation time of the given field (3) and of the closures 4 (WALE), 5
+// (coherent structure), 6 (wall-damped Cs), from the post-stream state
+// f / rho / u of node (x, y)
 template <int S>
 __device__ __forceinline__ typename Store<S>::C ext_tau(const StepArgs& a, int x, int y,
                                                          const typename Store<S>::C* f,
@@ -404,6 +410,7 @@ __device__ __forceinline__ typename Store<S>::C ext_tau(const StepArgs& a, int x
                                                          typename Store<S>::C uy, typename Store<S>::C rb)
 {
     using C = typename Store<S>::C;
+    if (a.les == 3) return C(a.tau_field[y * a.nx + x]);
     const C tau0 = prm<C>(a.tau0, a.f_tau0);
     C g[4];
     if (a.les == 4) {
@@ -543,21 +550,30 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
 // its 9 populations from one base pointer at constant plane offsets.  Edge
 // nodes take the boundary rule of the scene.
 // ---------------------------------------------------------------------------
-template <int S, int CO, int SC, bool LRN, int XT = 0>
+template <int S, int CO, int SC, bool LRN, int XT = 0, int AV = 0, int PD = 0>
 __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step_fast(const StepArgs ap)
 {
+    // Everything that is not the node's own pull, collision and stores is
+    // kept out of the common instance: the flag tables are read only in rows
+    // the parameter mask marks, the step counter only by the averaging
+    // instances (AV, chosen per step on the host) and on the error path, the
+    // per-node relaxation-time field only by the XT instances.  PD: launched
+    // as the programmatic dependent of the step's IB kernel, which advances
+    // the step counter; the other instances advance it here.  At 8 blocks of
+    // 256 threads per SM the kernel has 32 registers, and each extra branch
+    // with its own loads cost 1-3 % of the step (measured interleaved).
     using C = typename Store<S>::C;
     using T = typename Store<S>::T;
-    const StepArgs a = ap;
+    const StepArgs& a = ap;
     const int tx = threadIdx.x, bx = blockIdx.x, by = blockIdx.y;
     const int x = bx * kBlockX + tx, y = by;
     const int nx = a.nx, ny = a.ny;
     const int pitch = (int)a.pitch, plane = (int)a.plane;
-    const int t = __ldcg(&a.ctr->t[a.par]);
     if (x < nx) {
         const int node = y * nx + x;
         uint8_t nf = 0;
-        if (a.tile[by * a.tiles_x + bx]) nf = a.nflag[node];
+        const int rbit = y >> a.row_shift;
+        if (((a.rowmask[rbit >> 5] >> (rbit & 31)) & 1u) && a.tile[by * a.tiles_x + bx]) nf = a.nflag[node];
         if (!(nf & (NF_DEFER | NF_SOLID))) {
             const C rbs = rbase<S>(a);
             C f[9], rho, ux, uy;
@@ -575,8 +591,15 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
             } else {
                 ch_state<S>(a, x, y, f, rho, ux, uy);
             }
-            if (t >= a.avg_start) {
-                // Mesh::ComputeAvgVelocity (mesh.cpp:1969-1971)
+            // Mesh::ErrorCatch (mesh.cpp:2103): rho outside [0, 10]; NaN too
+            const bool bad = !(rho <= C(10) && rho >= C(0));
+            const C tau = XT ? ext_tau<S>(a, x, y, f, rho, ux, uy, rbs)
+                             : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
+                                                prm<C>(a.cs, a.f_cs), a.mlp);
+            if (AV) {
+                // Mesh::ComputeAvgVelocity (mesh.cpp:1969-1971) of the post-stream
+                // moments, which the collision below overwrites in f only
+                const int t = __ldcg(&a.ctr->t[a.par]);
                 C* av = reinterpret_cast<C*>(a.avg);
                 const int pl = nx * ny;
                 const C n0 = C(t - a.avg_start), n1 = C(t - a.avg_start + 1);
@@ -584,26 +607,21 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
                 av[pl + node] = (av[pl + node] * n0 + uy) / n1;
                 av[2 * pl + node] = (av[2 * pl + node] * n0 + rho) / n1;
             }
-            // Mesh::ErrorCatch (mesh.cpp:2103): rho outside [0, 10]; NaN too
-            if (!(rho <= C(10) && rho >= C(0))) flag_error(a.ctr, t);
-            const C tau = XT            ? ext_tau<S>(a, x, y, f, rho, ux, uy, rbs)
-                          : a.les == 3 ? C(a.tau_field[node])
-                                       : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
-                                                        prm<C>(a.cs, a.f_cs), a.mlp);
             collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
             T* q = reinterpret_cast<T*>(a.f_out) + cell;
 #pragma unroll
             for (int k = 0; k < 9; k++) q[k * plane] = Store<S>::st(f[k]);
+            if (bad) flag_error(a.ctr, __ldcg(&a.ctr->t[a.par]));
         }
     }
-    if (bx == 0 && by == 0 && tx == 0) a.ctr->t[a.par ^ 1] = t + 1;
-    // One block waits for the programmatic primary (this step's IB cluster,
-    // when there is one) to complete: the grid cannot complete before that
-    // block, so the grid's completion implies the step's.  The last block is
-    // scheduled last, so the wait is normally over before it starts; it waits
-    // on a kernel that was resident before any bulk block started, so there
-    // is no circular wait.  Without a primary the wait returns at once.
-    if (bx == gridDim.x - 1 && by == gridDim.y - 1) asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (!PD && bx == 0 && by == 0 && tx == 0) a.ctr->t[a.par ^ 1] = __ldcg(&a.ctr->t[a.par]) + 1;
+    // One block waits for the programmatic primary (this step's IB cluster)
+    // to complete: the grid cannot complete before that block, so the grid's
+    // completion implies the step's.  The last block is scheduled last, so
+    // the wait is normally over before it starts; it waits on a kernel that
+    // was resident before any bulk block started, so there is no circular
+    // wait.
+    if (PD && bx == gridDim.x - 1 && by == gridDim.y - 1) asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -983,6 +1001,9 @@ __global__ void __launch_bounds__(kIbThreads) ib_fused(const IbArgs ia, int pass
     const int T = gridDim.x * kIbThreads;
     const int g = blockIdx.x * kIbThreads + threadIdx.x;
     const int t = step_time(ia.s);
+    // the step counter of the next step (the bulk kernel launched as this
+    // kernel's dependent does not write it; the others write the same value)
+    if (ia.s.mode == MODE_STEP && g == 0) ia.s.ctr->t[ia.s.par ^ 1] = t + 1;
     for (int n = g; n < ia.nforced; n += T) ib_node_item<S, SC>(ia, n, t);
     cluster_sync();
     for (int p = 0; p < passes; p++) {
@@ -991,7 +1012,7 @@ __global__ void __launch_bounds__(kIbThreads) ib_fused(const IbArgs ia, int pass
         for (int n = g; n < ia.nforced; n += T) ib_spread_item(ia, n);
         cluster_sync();
     }
-    if (XT && ia.s.les != 6) {
+    if (XT && (ia.s.les == 4 || ia.s.les == 5)) {
         // the corrected velocities into the gradient field (WALE and the
         // coherent model; the wall-damped closure has none), before any
         // forced node reads its neighbours'
