@@ -100,6 +100,7 @@ struct ippi_lbm {
     // learned tau: parameters (FP32 values of the BF16 weights) + statistics
     float* mlp_dev = nullptr;
     double* tau_field = nullptr;  // IPPI_LES_FIELD: [ny][nx]
+    unsigned long long* ib_bar = nullptr;  // arrival counter of the one-launch step's IB blocks
     void* mac = nullptr;          // IPPI_LES_WALE / CSM: [2][ny][nx] compute type, velocities
     double* wall_dist = nullptr;  // IPPI_LES_DYNAMIC: [ny][nx]
     // solid nodes (halfway bounce-back) and their momentum-exchange links
@@ -728,6 +729,7 @@ LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int pa
     }
     if (L.ib) {
         L.ib_args = h->ib;
+        L.ib_args.bar = h->ib_bar;
         L.ib_args.s = a;
         L.ib_nst = h->ib_nst;
         L.ib_passes = std::max(1, h->p.mdf_iters);
@@ -915,6 +917,9 @@ int ippi_create(const ippi_params* p, ippi_lbm** out)
         dalloc(&h->init_m, 3 * nn * sizeof(double)) != cudaSuccess ||
         dalloc(&h->red, 4096 * sizeof(double)) != cudaSuccess)
         return bail(fail(nullptr, IPPI_ERR_NOMEM, "device allocation failed"));
+    if (dalloc(&h->ib_bar, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMemset(h->ib_bar, 0, sizeof(unsigned long long)) != cudaSuccess)
+        return bail(fail(nullptr, IPPI_ERR_NOMEM, "device allocation failed"));
     if ((p->les_model == IPPI_LES_WALE || p->les_model == IPPI_LES_CSM) &&
         (dalloc(&h->mac, 2 * nn * h->csize) != cudaSuccess || cudaMemset(h->mac, 0, 2 * nn * h->csize) != cudaSuccess))
         return bail(fail(nullptr, IPPI_ERR_NOMEM, "velocity field for the gradient closures"));
@@ -939,6 +944,7 @@ int ippi_destroy(ippi_lbm* h)
     dfree(h->tau_field);
     dfree(h->mac);
     dfree(h->wall_dist);
+    dfree(h->ib_bar);
     dfree(h->solid_links);
     dfree(h->solid_out);
     dfree(h->ctr);
@@ -1140,6 +1146,8 @@ int ippi_step(ippi_lbm* h, int nsteps, int t0)
     h->dl_valid = false;
     CK(h, cudaMemcpyAsync(h->ctr_h, h->ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, h->st));
     CK(h, cudaStreamSynchronize(h->st));
+    if (h->ctr_h->err == 2)
+        return fail(h, IPPI_ERR_CUDA, "an immersed-boundary barrier timed out (blocks not co-resident)");
     if (h->ctr_h->err)
         return fail(h, IPPI_ERR_DIVERGED, "Simulation Error! rho left [0,10] at step %d", h->ctr_h->err_t);
     return IPPI_OK;
@@ -1192,6 +1200,8 @@ int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk, double*
     if (ms_band) *ms_band = tn / nsteps;
     if (ms_ib) *ms_ib = ti / nsteps;
     CK(h, cudaMemcpy(h->ctr_h, h->ctr, sizeof(Ctr), cudaMemcpyDeviceToHost));
+    if (h->ctr_h->err == 2)
+        return fail(h, IPPI_ERR_CUDA, "an immersed-boundary barrier timed out (blocks not co-resident)");
     if (h->ctr_h->err)
         return fail(h, IPPI_ERR_DIVERGED, "Simulation Error! rho left [0,10] at step %d", h->ctr_h->err_t);
     return IPPI_OK;

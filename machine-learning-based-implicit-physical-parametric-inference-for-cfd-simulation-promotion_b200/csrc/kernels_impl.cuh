@@ -49,30 +49,34 @@ static void launch_ib(const LaunchSet& L, cudaStream_t st)
         cudaLaunchKernelEx(&cfg, ib_fused<S, SC, CO, LRN, 4, XT>, L.ib_args, L.ib_passes);
 }
 
-// the bulk kernel of a normal step, optionally as the programmatic
-// dependent of the kernel launched before it on the stream
+// the bulk kernel of a normal step (with or without the running means)
 template <int S, int CO, int SC, bool LRN, int XT>
-static void launch_bulk(const LaunchSet& L, bool pdl)
+static void launch_bulk(const LaunchSet& L)
 {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = L.grid;
-    cfg.blockDim = dim3(kBlockX);
-    cfg.stream = L.stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = pdl ? 1 : 0;
-    if (pdl) {
+    if (L.avg_on)
+        step_fast<S, CO, SC, LRN, XT, 1><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
+    else
+        step_fast<S, CO, SC, LRN, XT, 0><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
+}
+
+// a normal step with markers as one launch: the IB blocks first, then the
+// bulk row segments (step_ib_fused)
+template <int S, int CO, int SC, bool LRN, int XT>
+static void launch_merged(const LaunchSet& L)
+{
+    const unsigned nblk = (unsigned)kIbCtas + L.grid.x * L.grid.y;
+    IbArgs ia = L.ib_args;
+    ia.s = L.step;
+    if (L.ib_nst == 16) {
         if (L.avg_on)
-            cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, LRN, XT, 1, 1>, L.step);
+            step_ib_fused<S, SC, CO, LRN, 16, XT, 1><<<nblk, kBlockX, 0, L.stream>>>(ia, L.ib_passes);
         else
-            cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, LRN, XT, 0, 1>, L.step);
+            step_ib_fused<S, SC, CO, LRN, 16, XT, 0><<<nblk, kBlockX, 0, L.stream>>>(ia, L.ib_passes);
     } else {
         if (L.avg_on)
-            cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, LRN, XT, 1, 0>, L.step);
+            step_ib_fused<S, SC, CO, LRN, 4, XT, 1><<<nblk, kBlockX, 0, L.stream>>>(ia, L.ib_passes);
         else
-            cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, LRN, XT, 0, 0>, L.step);
+            step_ib_fused<S, SC, CO, LRN, 4, XT, 0><<<nblk, kBlockX, 0, L.stream>>>(ia, L.ib_passes);
     }
 }
 
@@ -85,11 +89,9 @@ static cudaError_t launch_tpl(const LaunchSet& L)
     // kernel, in stream order; the local models (tau field, wall-damped Cs)
     // in timed launches.  Channel scene only: no boundary-net work.
     if (XT && (L.step.les == 3 || L.step.les == 6) && L.step.mode == MODE_STEP && L.ib && !L.events) {
-        // the tau field and the wall-damped closure are local: the same
-        // overlap of the IB kernel and its dependent bulk kernel as the
-        // normal step below
-        launch_ib<S, SC, CO, LRN, XT>(L, L.stream);
-        launch_bulk<S, CO, SC, LRN, XT>(L, true);
+        // the tau field and the wall-damped closure are local: one launch
+        // with the IB blocks, as the normal step below
+        launch_merged<S, CO, SC, LRN, XT>(L);
         return cudaGetLastError();
     }
     if (XT) {
@@ -103,19 +105,17 @@ static cudaError_t launch_tpl(const LaunchSet& L)
             cudaEventRecord(L.events[0], L.stream);
         }
         if (L.step.mode == MODE_STEP)
-            launch_bulk<S, CO, SC, LRN, XT>(L, false);
+            launch_bulk<S, CO, SC, LRN, XT>(L);
         else
             step_kernel<S, CO, SC, LRN, XT><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
         if (L.events) cudaEventRecord(L.events[1], L.stream);
         return cudaGetLastError();
     }
-    // Normal steps with markers and no boundary nets: IB cluster, then the
-    // bulk kernel as its programmatic dependent, both on the main stream.
-    // Timed launches (events) keep the side-stream form below, so the bulk
-    // kernel's own duration can be measured.
+    // Normal steps with markers and no boundary nets: one launch, IB blocks
+    // and bulk row segments.  Timed launches (events) keep the side-stream
+    // form below, so the bulk kernel's own duration can be measured.
     if (L.step.mode == MODE_STEP && L.ib && !L.band && L.nprep == 0 && !L.events) {
-        launch_ib<S, SC, CO, LRN>(L, L.stream);
-        launch_bulk<S, CO, SC, LRN, 0>(L, true);
+        launch_merged<S, CO, SC, LRN, 0>(L);
         return cudaGetLastError();
     }
     const bool side = L.nprep > 0 || L.band || L.ib;
@@ -135,7 +135,7 @@ static cudaError_t launch_tpl(const LaunchSet& L)
     }
     if (L.events) cudaEventRecord(L.events[0], L.stream);
     if (L.step.mode == MODE_STEP)
-        launch_bulk<S, CO, SC, LRN, 0>(L, false);
+        launch_bulk<S, CO, SC, LRN, 0>(L);
     else
         step_kernel<S, CO, SC, LRN><<<L.grid, kBlockX, 0, L.stream>>>(L.step);
     if (L.events) cudaEventRecord(L.events[1], L.stream);

@@ -550,78 +550,76 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
 // its 9 populations from one base pointer at constant plane offsets.  Edge
 // nodes take the boundary rule of the scene.
 // ---------------------------------------------------------------------------
-template <int S, int CO, int SC, bool LRN, int XT = 0, int AV = 0, int PD = 0>
-__global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step_fast(const StepArgs ap)
+// One 256-node row segment (bx, by) of a normal step: pull (or the node's
+// boundary rule), moments, relaxation time, collision, stores.  Everything
+// that is not the node's own pull, collision and stores is kept out of the
+// common instance: the flag tables are read only in rows the parameter mask
+// marks, the step counter only by the averaging instances (AV, chosen per
+// step on the host) and on the error path, the per-node relaxation-time
+// field only by the XT instances.  At 8 blocks of 256 threads per SM the
+// kernel has 32 registers, and each extra branch with its own loads cost
+// 1-3 % of the step (measured interleaved).
+template <int S, int CO, int SC, bool LRN, int XT, int AV>
+__device__ __forceinline__ void bulk_tile(const StepArgs& a, int bx, int by, int tx)
 {
-    // Everything that is not the node's own pull, collision and stores is
-    // kept out of the common instance: the flag tables are read only in rows
-    // the parameter mask marks, the step counter only by the averaging
-    // instances (AV, chosen per step on the host) and on the error path, the
-    // per-node relaxation-time field only by the XT instances.  PD: launched
-    // as the programmatic dependent of the step's IB kernel, which advances
-    // the step counter; the other instances advance it here.  At 8 blocks of
-    // 256 threads per SM the kernel has 32 registers, and each extra branch
-    // with its own loads cost 1-3 % of the step (measured interleaved).
     using C = typename Store<S>::C;
     using T = typename Store<S>::T;
-    const StepArgs& a = ap;
-    const int tx = threadIdx.x, bx = blockIdx.x, by = blockIdx.y;
     const int x = bx * kBlockX + tx, y = by;
     const int nx = a.nx, ny = a.ny;
     const int pitch = (int)a.pitch, plane = (int)a.plane;
-    if (x < nx) {
-        const int node = y * nx + x;
-        uint8_t nf = 0;
-        const int rbit = y >> a.row_shift;
-        if (((a.rowmask[rbit >> 5] >> (rbit & 31)) & 1u) && a.tile[by * a.tiles_x + bx]) nf = a.nflag[node];
-        if (!(nf & (NF_DEFER | NF_SOLID))) {
-            const C rbs = rbase<S>(a);
-            C f[9], rho, ux, uy;
-            const int cell = y * pitch + x;
-            if (nf & NF_SBND) {
-                solid_pull<S>(a, x, y, f);
-                macros<C>(f, rbs, rho, ux, uy);
-            } else if (x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
-                const T* p = reinterpret_cast<const T*>(a.f_in) + cell;
+    if (x >= nx) return;
+    const int node = y * nx + x;
+    uint8_t nf = 0;
+    const int rbit = y >> a.row_shift;
+    if (((a.rowmask[rbit >> 5] >> (rbit & 31)) & 1u) && a.tile[by * a.tiles_x + bx]) nf = a.nflag[node];
+    if (nf & (NF_DEFER | NF_SOLID)) return;
+    const C rbs = rbase<S>(a);
+    C f[9], rho, ux, uy;
+    const int cell = y * pitch + x;
+    if (nf & NF_SBND) {
+        solid_pull<S>(a, x, y, f);
+        macros<C>(f, rbs, rho, ux, uy);
+    } else if (x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
+        const T* p = reinterpret_cast<const T*>(a.f_in) + cell;
 #pragma unroll
-                for (int k = 0; k < 9; k++) f[k] = Store<S>::ld(__ldg(p + (k * plane - EY(k) * pitch - EX(k))));
-                macros<C>(f, rbs, rho, ux, uy);
-            } else if (SC == SC_REF) {
-                ref_state<S>(a, x, y, f, rho, ux, uy);
-            } else {
-                ch_state<S>(a, x, y, f, rho, ux, uy);
-            }
-            // Mesh::ErrorCatch (mesh.cpp:2103): rho outside [0, 10]; NaN too
-            const bool bad = !(rho <= C(10) && rho >= C(0));
-            const C tau = XT ? ext_tau<S>(a, x, y, f, rho, ux, uy, rbs)
-                             : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
-                                                prm<C>(a.cs, a.f_cs), a.mlp);
-            if (AV) {
-                // Mesh::ComputeAvgVelocity (mesh.cpp:1969-1971) of the post-stream
-                // moments, which the collision below overwrites in f only
-                const int t = __ldcg(&a.ctr->t[a.par]);
-                C* av = reinterpret_cast<C*>(a.avg);
-                const int pl = nx * ny;
-                const C n0 = C(t - a.avg_start), n1 = C(t - a.avg_start + 1);
-                av[node] = (av[node] * n0 + ux) / n1;
-                av[pl + node] = (av[pl + node] * n0 + uy) / n1;
-                av[2 * pl + node] = (av[2 * pl + node] * n0 + rho) / n1;
-            }
-            collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
-            T* q = reinterpret_cast<T*>(a.f_out) + cell;
-#pragma unroll
-            for (int k = 0; k < 9; k++) q[k * plane] = Store<S>::st(f[k]);
-            if (bad) flag_error(a.ctr, __ldcg(&a.ctr->t[a.par]));
-        }
+        for (int k = 0; k < 9; k++) f[k] = Store<S>::ld(__ldg(p + (k * plane - EY(k) * pitch - EX(k))));
+        macros<C>(f, rbs, rho, ux, uy);
+    } else if (SC == SC_REF) {
+        ref_state<S>(a, x, y, f, rho, ux, uy);
+    } else {
+        ch_state<S>(a, x, y, f, rho, ux, uy);
     }
-    if (!PD && bx == 0 && by == 0 && tx == 0) a.ctr->t[a.par ^ 1] = __ldcg(&a.ctr->t[a.par]) + 1;
-    // One block waits for the programmatic primary (this step's IB cluster)
-    // to complete: the grid cannot complete before that block, so the grid's
-    // completion implies the step's.  The last block is scheduled last, so
-    // the wait is normally over before it starts; it waits on a kernel that
-    // was resident before any bulk block started, so there is no circular
-    // wait.
-    if (PD && bx == gridDim.x - 1 && by == gridDim.y - 1) asm volatile("griddepcontrol.wait;" ::: "memory");
+    // Mesh::ErrorCatch (mesh.cpp:2103): rho outside [0, 10]; NaN too
+    const bool bad = !(rho <= C(10) && rho >= C(0));
+    const C tau = XT ? ext_tau<S>(a, x, y, f, rho, ux, uy, rbs)
+                     : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
+                                        prm<C>(a.cs, a.f_cs), a.mlp);
+    if (AV) {
+        // Mesh::ComputeAvgVelocity (mesh.cpp:1969-1971) of the post-stream
+        // moments, which the collision below overwrites in f only
+        const int t = __ldcg(&a.ctr->t[a.par]);
+        C* av = reinterpret_cast<C*>(a.avg);
+        const int pl = nx * ny;
+        const C n0 = C(t - a.avg_start), n1 = C(t - a.avg_start + 1);
+        av[node] = (av[node] * n0 + ux) / n1;
+        av[pl + node] = (av[pl + node] * n0 + uy) / n1;
+        av[2 * pl + node] = (av[2 * pl + node] * n0 + rho) / n1;
+    }
+    collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
+    T* q = reinterpret_cast<T*>(a.f_out) + cell;
+#pragma unroll
+    for (int k = 0; k < 9; k++) q[k * plane] = Store<S>::st(f[k]);
+    if (bad) flag_error(a.ctr, __ldcg(&a.ctr->t[a.par]));
+}
+
+// a normal step without immersed boundary work in the same launch: one
+// block per row segment; block (0, 0) advances the step counter
+template <int S, int CO, int SC, bool LRN, int XT = 0, int AV = 0>
+__global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step_fast(const StepArgs ap)
+{
+    bulk_tile<S, CO, SC, LRN, XT, AV>(ap, blockIdx.x, blockIdx.y, threadIdx.x);
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+        ap.ctr->t[ap.par ^ 1] = __ldcg(&ap.ctr->t[ap.par]) + 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -800,27 +798,24 @@ __global__ void __launch_bounds__(kBandThreads) band_kernel(const BandArgs ba)
 
 // ---------------------------------------------------------------------------
 // immersed boundary (mesh.cpp:514-832, 1244-1281 and NodeAndLattice.cpp:162-195)
-// as ONE kernel launched as a cluster of kIbCtas CTAs (the hardware
-// co-schedules a cluster, so its barriers cannot wait on an unscheduled CTA),
-// on the high-priority side stream, phases separated by cluster barriers
+// as one sequence of phases over kIbCtas blocks, separated by barriers
 // (release / acquire: global-memory writes of one phase are visible to every
-// CTA of the cluster in the next):
+// block in the next):
 //   nodes    post-stream state of every stencil node, from the previous field
 //            (the bulk kernel skips these nodes)
 //   markers  InterpolateVel + CalParticleForce: F_m = 2 (U_b - sum u delta)
 //   spread   SpreadForce + UpdateVelocity: node force, u += F / (2 rho)
 //            (markers and spread repeat for each direct-forcing pass)
-//   finish   per-body force sums (FP64 fixed-order tree, one CTA per body)
+//   finish   per-body force sums (FP64 fixed-order tree, one block per body)
 //            and the forced nodes' collision with the corrected velocity and
 //            the operator's forcing term
-// One launch instead of a chain of dependent ones.  In a normal step it runs
-// on the main stream BEFORE the bulk kernel, which is its programmatic
-// dependent: the cluster triggers the bulk launch as soon as it is resident
-// (griddepcontrol.launch_dependents), the bulk kernel fills the rest of the
-// GPU, and the bulk kernel's last block waits for the cluster's completion
-// (griddepcontrol.wait) so that the end of the bulk grid is the end of the
-// step.  Launched beside the bulk kernel on another stream instead, the
-// cluster only found free SMs once the bulk kernel drained.
+// In a normal step the phases run in the first kIbCtas blocks of the step's
+// one launch (step_ib_fused, a global-memory barrier); alone (ib_fused) they
+// run as one thread-block cluster with cluster barriers.  Launched beside the
+// bulk kernel on another stream instead, the IB work only found free SMs
+// once the bulk kernel drained; as a separate cluster kernel with the bulk
+// kernel as its programmatic dependent, the launch pair cost about 5 us per
+// step more than one launch.
 // ---------------------------------------------------------------------------
 constexpr int kIbThreads = 128;  // threads per CTA of the IB cluster
 constexpr int kIbCtas = 8;       // CTAs per cluster (portable cluster size)
@@ -851,6 +846,7 @@ struct IbArgs {
     double* force_now;          // [nbody][2]
     double* force_hist;         // [hist_cap][nbody][2]
     int hist_cap;
+    unsigned long long* bar;    // GridBar arrival counter (step_ib_fused)
     StepArgs s;
 };
 
@@ -931,20 +927,21 @@ __device__ __forceinline__ void ib_spread_item(const IbArgs& ia, int n)
 }
 
 // body force -sum F ds over the body's markers: fixed-order tree over the CTA
-__device__ __forceinline__ void ib_body_sum(const IbArgs& ia, int b, int t, double (*red)[kIbThreads])
+template <int NT>
+__device__ __forceinline__ void ib_body_sum(const IbArgs& ia, int b, int t, double (*red)[NT])
 {
     const StepArgs& a = ia.s;
     const int tid = threadIdx.x;
     const int2 mr = ia.body_m[b];
     double sx = 0.0, sy = 0.0;
-    for (int m = mr.x + tid; m < mr.y; m += kIbThreads) {
+    for (int m = mr.x + tid; m < mr.y; m += NT) {
         sx -= ia.mft[m].x * ia.ds[m];
         sy -= ia.mft[m].y * ia.ds[m];
     }
     red[0][tid] = sx;
     red[1][tid] = sy;
     __syncthreads();
-    for (int w = kIbThreads / 2; w; w >>= 1) {
+    for (int w = NT / 2; w; w >>= 1) {
         if (tid < w) {
             red[0][tid] += red[0][tid + w];
             red[1][tid] += red[1][tid + w];
@@ -991,31 +988,75 @@ __device__ __forceinline__ void ib_collide_item(const IbArgs& ia, int n)
     }
 }
 
-// launched as exactly one cluster: gridDim.x == kIbCtas
-template <int S, int SC, int CO, bool LRN, int NST, int XT = 0>
-__global__ void __launch_bounds__(kIbThreads) ib_fused(const IbArgs ia, int passes)
+// Barrier between the IB phases of the kIbCtas IB blocks.  ClusterBar: the
+// blocks form one thread-block cluster (the hardware co-schedules it).
+// GridBar: the blocks are the first kIbCtas blocks of the step kernel; a
+// monotonic 64-bit arrival counter in global memory, nbar barriers per
+// launch, so each launch starts from a multiple of kIbCtas * nbar (the first
+// barrier cannot complete before every block has read it).  The wait is
+// bounded: after kBarSpins polls the block records IPPI's barrier error
+// (Ctr::err = 2) and goes on, so a launch never hangs.  The IB blocks are
+// the lowest block indices of a launch on an otherwise idle stream and the
+// other blocks never wait on them, so they are resident long before then.
+struct ClusterBar {
+    __device__ __forceinline__ void operator()() { cluster_sync(); }
+};
+
+constexpr int kBarSpins = 1 << 24;
+
+struct GridBar {
+    unsigned long long* ctr;
+    unsigned long long base;
+    int k;
+    Ctr* err;
+    __device__ __forceinline__ void operator()()
+    {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(ctr, 1ull);
+            k++;
+            const unsigned long long target = base + (unsigned long long)k * kIbCtas;
+            int it = 0;
+            unsigned long long v;
+            do {
+                asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(ctr) : "memory");
+                if (v >= target) break;
+                __nanosleep(64);
+            } while (++it < kBarSpins);
+            if (v < target) atomicExch(&err->err, 2);
+            __threadfence();
+        } else {
+            k++;
+        }
+        __syncthreads();
+    }
+};
+
+// The IB sub-step of one launch, in nblk blocks of NT threads (block blk):
+// stencil-node states, direct-forcing passes, body sums, forced collisions.
+template <int S, int SC, int CO, bool LRN, int NST, int XT, int NT, typename Bar>
+__device__ __forceinline__ void ib_phases(const IbArgs& ia, int passes, int blk, int nblk, double (*red)[NT],
+                                          Bar& bar)
 {
-    __shared__ double red[2][kIbThreads];
-    // the dependent bulk kernel may launch now (a no-op without one)
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    const int T = gridDim.x * kIbThreads;
-    const int g = blockIdx.x * kIbThreads + threadIdx.x;
+    const int T = nblk * NT;
+    const int g = blk * NT + threadIdx.x;
     const int t = step_time(ia.s);
-    // the step counter of the next step (the bulk kernel launched as this
-    // kernel's dependent does not write it; the others write the same value)
+    // the step counter of the next step (a bulk kernel beside this one does
+    // not write it; the others write the same value)
     if (ia.s.mode == MODE_STEP && g == 0) ia.s.ctr->t[ia.s.par ^ 1] = t + 1;
     for (int n = g; n < ia.nforced; n += T) ib_node_item<S, SC>(ia, n, t);
-    cluster_sync();
+    bar();
     for (int p = 0; p < passes; p++) {
         for (int m = g; m < ia.nmark; m += T) ib_marker_item<NST>(ia, m, p == 0);
-        cluster_sync();
+        bar();
         for (int n = g; n < ia.nforced; n += T) ib_spread_item(ia, n);
-        cluster_sync();
+        bar();
     }
     if (XT && (ia.s.les == 4 || ia.s.les == 5)) {
         // the corrected velocities into the gradient field (WALE and the
-        // coherent model; the wall-damped closure has none), before any
-        // forced node reads its neighbours'
+        // coherent model; the local models have none), before any forced
+        // node reads its neighbours'
         using C = typename Store<S>::C;
         C* m = reinterpret_cast<C*>(ia.s.mac);
         const int pl = ia.s.nx * ia.s.ny;
@@ -1024,10 +1065,48 @@ __global__ void __launch_bounds__(kIbThreads) ib_fused(const IbArgs ia, int pass
             m[xy.y * ia.s.nx + xy.x] = C(ia.ucx[n]);
             m[pl + xy.y * ia.s.nx + xy.x] = C(ia.ucy[n]);
         }
-        cluster_sync();
+        bar();
     }
-    for (int b = blockIdx.x; b < ia.nbody; b += gridDim.x) ib_body_sum(ia, b, t, red);
+    for (int b = blk; b < ia.nbody; b += nblk) ib_body_sum<NT>(ia, b, t, red);
     for (int n = g; n < ia.nforced; n += T) ib_collide_item<S, CO, LRN, XT>(ia, n);
+}
+
+// the IB sub-step alone, launched as exactly one cluster (gridDim.x ==
+// kIbCtas): initialisation and download modes, timed and boundary-net steps
+template <int S, int SC, int CO, bool LRN, int NST, int XT = 0>
+__global__ void __launch_bounds__(kIbThreads) ib_fused(const IbArgs ia, int passes)
+{
+    __shared__ double red[2][kIbThreads];
+    ClusterBar bar;
+    ib_phases<S, SC, CO, LRN, NST, XT, kIbThreads>(ia, passes, blockIdx.x, gridDim.x, red, bar);
+}
+
+// A normal step with markers in ONE launch: blocks 0 .. kIbCtas-1 perform
+// the IB sub-step (GridBar between its phases), the rest are the bulk row
+// segments (block kIbCtas + by * tiles_x + bx).  The IB blocks are
+// dispatched first, so they run beside the bulk blocks from the start, and
+// the step ends when the launch does.
+template <int S, int SC, int CO, bool LRN, int NST, int XT, int AV>
+__global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step_ib_fused(const IbArgs ia, int passes)
+{
+    __shared__ double red[2][kBlockX];
+    __shared__ unsigned long long s_base;
+    if (blockIdx.x < kIbCtas) {
+        const unsigned long long nbar =
+            1ull + 2ull * (unsigned long long)passes + ((XT && (ia.s.les == 4 || ia.s.les == 5)) ? 1ull : 0ull);
+        if (threadIdx.x == 0) {
+            unsigned long long v;
+            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(ia.bar) : "memory");
+            s_base = v - v % (nbar * kIbCtas);
+        }
+        __syncthreads();
+        GridBar bar{ia.bar, s_base, 0, ia.s.ctr};
+        ib_phases<S, SC, CO, LRN, NST, XT, kBlockX>(ia, passes, blockIdx.x, kIbCtas, red, bar);
+        return;
+    }
+    const int tile = blockIdx.x - kIbCtas;
+    const int by = tile / ia.s.tiles_x, bx = tile - by * ia.s.tiles_x;
+    bulk_tile<S, CO, SC, LRN, XT, AV>(ia.s, bx, by, threadIdx.x);
 }
 
 // the post-stream velocity of every node into StepArgs::mac (closures 4, 5):
