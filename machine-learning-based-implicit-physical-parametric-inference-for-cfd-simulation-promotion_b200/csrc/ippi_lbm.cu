@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -730,6 +731,14 @@ LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int pa
     if (L.ib) {
         L.ib_args = h->ib;
         L.ib_args.bar = h->ib_bar;
+        // IPPI_TEST_IB_BARRIER_EXTRA=n (tests only): every IB barrier of the
+        // one-launch step waits for n arrivals that never come, runs out
+        // after its poll limit and reports the timeout
+        static const int bar_extra = [] {
+            const char* e = std::getenv("IPPI_TEST_IB_BARRIER_EXTRA");
+            return e ? std::max(0, std::atoi(e)) : 0;
+        }();
+        L.ib_args.bar_extra = bar_extra;
         L.ib_args.s = a;
         L.ib_nst = h->ib_nst;
         L.ib_passes = std::max(1, h->p.mdf_iters);

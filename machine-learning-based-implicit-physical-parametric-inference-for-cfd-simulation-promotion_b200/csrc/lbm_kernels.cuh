@@ -847,6 +847,8 @@ struct IbArgs {
     double* force_hist;         // [hist_cap][nbody][2]
     int hist_cap;
     unsigned long long* bar;    // GridBar arrival counter (step_ib_fused)
+    int bar_extra;              // arrivals each GridBar waits for beyond kIbCtas:
+                                // 0, or > 0 in the test that lets the wait run out
     StepArgs s;
 };
 
@@ -994,21 +996,23 @@ __device__ __forceinline__ void ib_collide_item(const IbArgs& ia, int n)
 // monotonic 64-bit arrival counter in global memory, nbar barriers per
 // launch, so each launch starts from a multiple of kIbCtas * nbar (the first
 // barrier cannot complete before every block has read it).  The wait is
-// bounded: after kBarSpins polls the block records IPPI's barrier error
-// (Ctr::err = 2) and goes on, so a launch never hangs.  The IB blocks are
+// bounded: after 1 s (or kBarSpins polls) the block records the barrier
+// error (Ctr::err = 2) and goes on, so a launch never hangs.  The IB blocks are
 // the lowest block indices of a launch on an otherwise idle stream and the
 // other blocks never wait on them, so they are resident long before then.
 struct ClusterBar {
     __device__ __forceinline__ void operator()() { cluster_sync(); }
 };
 
-constexpr int kBarSpins = 1 << 24;
+constexpr int kBarSpins = 1 << 26;                  // polls, and
+constexpr unsigned long long kBarNanos = 1000000000ull;  // 1 s of waiting at most
 
 struct GridBar {
     unsigned long long* ctr;
     unsigned long long base;
     int k;
     Ctr* err;
+    int extra;
     __device__ __forceinline__ void operator()()
     {
         __syncthreads();
@@ -1016,14 +1020,16 @@ struct GridBar {
             __threadfence();
             atomicAdd(ctr, 1ull);
             k++;
-            const unsigned long long target = base + (unsigned long long)k * kIbCtas;
+            const unsigned long long target = base + (unsigned long long)k * (kIbCtas + extra);
             int it = 0;
-            unsigned long long v;
+            unsigned long long v, t0, now;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
             do {
                 asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(ctr) : "memory");
                 if (v >= target) break;
                 __nanosleep(64);
-            } while (++it < kBarSpins);
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+            } while (++it < kBarSpins && now - t0 < kBarNanos);
             if (v < target) atomicExch(&err->err, 2);
             __threadfence();
         } else {
@@ -1100,7 +1106,7 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
             s_base = v - v % (nbar * kIbCtas);
         }
         __syncthreads();
-        GridBar bar{ia.bar, s_base, 0, ia.s.ctr};
+        GridBar bar{ia.bar, s_base, 0, ia.s.ctr, ia.bar_extra};
         ib_phases<S, SC, CO, LRN, NST, XT, kBlockX>(ia, passes, blockIdx.x, kIbCtas, red, bar);
         return;
     }
