@@ -94,6 +94,23 @@ static cudaError_t launch_tpl(const LaunchSet& L)
         launch_merged<S, CO, SC, LRN, XT>(L);
         return cudaGetLastError();
     }
+    if (XT && (L.step.les == 4 || L.step.les == 5) && L.step.mode == MODE_STEP && L.ib && !L.events) {
+        // WALE / coherent model with markers: two launches, the IB force
+        // phases beside the velocity pass, then the forced collisions beside
+        // the bulk row segments
+        IbArgs ia = L.ib_args;
+        ia.s = L.step;
+        const unsigned nblk = (unsigned)kIbCtas + L.grid.x * L.grid.y;
+        if (L.ib_nst == 16)
+            mac_ib_fused<S, SC, 16><<<nblk, kBlockX, 0, L.stream>>>(ia, L.ib_passes);
+        else
+            mac_ib_fused<S, SC, 4><<<nblk, kBlockX, 0, L.stream>>>(ia, L.ib_passes);
+        if (L.avg_on)
+            collide_ib_fused<S, SC, CO, LRN, 1><<<nblk, kBlockX, 0, L.stream>>>(ia);
+        else
+            collide_ib_fused<S, SC, CO, LRN, 0><<<nblk, kBlockX, 0, L.stream>>>(ia);
+        return cudaGetLastError();
+    }
     if (XT) {
         // timed launches: events 2-3 around the velocity pass and the IB
         // kernel, 0-1 around the bulk kernel

@@ -181,7 +181,10 @@ __device__ __forceinline__ C wale_tau(const C* g, C tau0)
     const C dxy = C(0.5) * (gxy2 + gyx2);
     const C dyy = C(0.5) * (gyy2 + gyy2) - grr2 / C(3.0);
     const C gg = dxx * dxx + dxy * dxy + dxy * dxy + dyy * dyy;
-    const C vt = C(0.45 * 0.45) * pow(gg, C(1.5)) / (pow(ss, C(2.5)) + pow(gg, C(1.25)) + C(1e-12));
+    // x^1.5 = x sqrt(x), x^2.5 = x^2 sqrt(x), x^1.25 = x sqrt(sqrt(x)): the
+    // same values to rounding, without a general power
+    const C rg = sqrt(gg), rs = sqrt(ss);
+    const C vt = C(0.45 * 0.45) * (gg * rg) / (ss * ss * rs + gg * sqrt(rg) + C(1e-12));
     return tau0 + C(3) * vt;
 }
 
@@ -200,7 +203,7 @@ __device__ __forceinline__ C csm_tau(const C* g, C pxx, C pxy, C pyy, C tau0)
     C ccsm = C(0.016);
     if (e != C(0)) {
         const C fcs = fabs(q / e);
-        ccsm = (C(1) / C(11.0)) * pow(fcs, C(1.5)) * (C(1) - fcs);
+        ccsm = (C(1) / C(11.0)) * (fcs * sqrt(fcs)) * (C(1) - fcs);
     }
     const C s2 = pxx * pxx + pxy * pxy + pxy * pxy + pyy * pyy;
     return tau0 + C(3) * (ccsm * sqrt(C(2) * s2));

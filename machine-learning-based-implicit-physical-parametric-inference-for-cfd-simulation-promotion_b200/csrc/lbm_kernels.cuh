@@ -1039,8 +1039,40 @@ struct GridBar {
     }
 };
 
+// The force part of the IB sub-step in nblk blocks of NT threads (block
+// blk): stencil-node states, direct-forcing passes, the corrected
+// velocities into the gradient field (WALE / coherent model; with a barrier
+// after them when SYNC_MAC, for collisions in the same launch), body sums.
+template <int S, int SC, int NST, int XT, int NT, bool SYNC_MAC, typename Bar>
+__device__ __forceinline__ void ib_force_phases(const IbArgs& ia, int passes, int blk, int nblk,
+                                                double (*red)[NT], Bar& bar, int t)
+{
+    const int T = nblk * NT;
+    const int g = blk * NT + threadIdx.x;
+    for (int n = g; n < ia.nforced; n += T) ib_node_item<S, SC>(ia, n, t);
+    bar();
+    for (int p = 0; p < passes; p++) {
+        for (int m = g; m < ia.nmark; m += T) ib_marker_item<NST>(ia, m, p == 0);
+        bar();
+        for (int n = g; n < ia.nforced; n += T) ib_spread_item(ia, n);
+        bar();
+    }
+    if (XT && (ia.s.les == 4 || ia.s.les == 5)) {
+        using C = typename Store<S>::C;
+        C* m = reinterpret_cast<C*>(ia.s.mac);
+        const int pl = ia.s.nx * ia.s.ny;
+        for (int n = g; n < ia.nforced; n += T) {
+            const int2 xy = ia.fn_xy[n];
+            m[xy.y * ia.s.nx + xy.x] = C(ia.ucx[n]);
+            m[pl + xy.y * ia.s.nx + xy.x] = C(ia.ucy[n]);
+        }
+        if (SYNC_MAC) bar();
+    }
+    for (int b = blk; b < ia.nbody; b += nblk) ib_body_sum<NT>(ia, b, t, red);
+}
+
 // The IB sub-step of one launch, in nblk blocks of NT threads (block blk):
-// stencil-node states, direct-forcing passes, body sums, forced collisions.
+// the force part, then the forced nodes' collisions.
 template <int S, int SC, int CO, bool LRN, int NST, int XT, int NT, typename Bar>
 __device__ __forceinline__ void ib_phases(const IbArgs& ia, int passes, int blk, int nblk, double (*red)[NT],
                                           Bar& bar)
@@ -1051,29 +1083,7 @@ __device__ __forceinline__ void ib_phases(const IbArgs& ia, int passes, int blk,
     // the step counter of the next step (a bulk kernel beside this one does
     // not write it; the others write the same value)
     if (ia.s.mode == MODE_STEP && g == 0) ia.s.ctr->t[ia.s.par ^ 1] = t + 1;
-    for (int n = g; n < ia.nforced; n += T) ib_node_item<S, SC>(ia, n, t);
-    bar();
-    for (int p = 0; p < passes; p++) {
-        for (int m = g; m < ia.nmark; m += T) ib_marker_item<NST>(ia, m, p == 0);
-        bar();
-        for (int n = g; n < ia.nforced; n += T) ib_spread_item(ia, n);
-        bar();
-    }
-    if (XT && (ia.s.les == 4 || ia.s.les == 5)) {
-        // the corrected velocities into the gradient field (WALE and the
-        // coherent model; the local models have none), before any forced
-        // node reads its neighbours'
-        using C = typename Store<S>::C;
-        C* m = reinterpret_cast<C*>(ia.s.mac);
-        const int pl = ia.s.nx * ia.s.ny;
-        for (int n = g; n < ia.nforced; n += T) {
-            const int2 xy = ia.fn_xy[n];
-            m[xy.y * ia.s.nx + xy.x] = C(ia.ucx[n]);
-            m[pl + xy.y * ia.s.nx + xy.x] = C(ia.ucy[n]);
-        }
-        bar();
-    }
-    for (int b = blk; b < ia.nbody; b += nblk) ib_body_sum<NT>(ia, b, t, red);
+    ib_force_phases<S, SC, NST, XT, NT, true>(ia, passes, blk, nblk, red, bar, t);
     for (int n = g; n < ia.nforced; n += T) ib_collide_item<S, CO, LRN, XT>(ia, n);
 }
 
@@ -1115,16 +1125,16 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
     bulk_tile<S, CO, SC, LRN, XT, AV>(ia.s, bx, by, threadIdx.x);
 }
 
-// the post-stream velocity of every node into StepArgs::mac (closures 4, 5):
-// the state the step's collision sees, before the IB correction
+// the post-stream velocity of node (x, y) into StepArgs::mac (closures 4,
+// 5): the state the step's collision sees, before the IB correction
 template <int S, int SC>
-__global__ void __launch_bounds__(kBlockX) mac_kernel(const StepArgs a)
+__device__ __forceinline__ void mac_node(const StepArgs& a, int x, int y, bool skip_forced)
 {
     using C = typename Store<S>::C;
-    const int x = blockIdx.x * kBlockX + threadIdx.x, y = blockIdx.y;
     if (x >= a.nx) return;
     const int node = y * a.nx + x, pl = a.nx * a.ny;
     const uint8_t nf = a.nflag[node];
+    if (skip_forced && (nf & NF_DEFER)) return;  // written by the IB blocks
     C f[9], rho, ux = C(0), uy = C(0);
     if (nf & NF_SOLID) {
     } else if ((nf & NF_SBND) && a.mode != MODE_INIT && a.mode != MODE_MAT_INIT) {
@@ -1136,6 +1146,55 @@ __global__ void __launch_bounds__(kBlockX) mac_kernel(const StepArgs a)
     C* m = reinterpret_cast<C*>(a.mac);
     m[node] = ux;
     m[pl + node] = uy;
+}
+
+template <int S, int SC>
+__global__ void __launch_bounds__(kBlockX) mac_kernel(const StepArgs a)
+{
+    mac_node<S, SC>(a, blockIdx.x * kBlockX + threadIdx.x, blockIdx.y, false);
+}
+
+// WALE / coherent model with markers, a normal step in two launches.  First:
+// blocks 0 .. kIbCtas-1 the force part of the IB sub-step (GridBar between
+// phases; the corrected velocities into the gradient field), the others the
+// post-stream velocities of every other node.  Second: blocks 0 ..
+// kIbCtas-1 the forced nodes' collisions, the others the bulk row segments;
+// every velocity the gradients read is final by then.
+template <int S, int SC, int NST>
+__global__ void __launch_bounds__(kBlockX, 8) mac_ib_fused(const IbArgs ia, int passes)
+{
+    __shared__ double red[2][kBlockX];
+    __shared__ unsigned long long s_base;
+    if (blockIdx.x < kIbCtas) {
+        const unsigned long long nbar = 1ull + 2ull * (unsigned long long)passes;
+        if (threadIdx.x == 0) {
+            unsigned long long v;
+            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(ia.bar) : "memory");
+            s_base = v - v % (nbar * kIbCtas);
+        }
+        __syncthreads();
+        GridBar bar{ia.bar, s_base, 0, ia.s.ctr, ia.bar_extra};
+        const int t = step_time(ia.s);
+        if (ia.s.mode == MODE_STEP && blockIdx.x == 0 && threadIdx.x == 0) ia.s.ctr->t[ia.s.par ^ 1] = t + 1;
+        ib_force_phases<S, SC, NST, 1, kBlockX, false>(ia, passes, blockIdx.x, kIbCtas, red, bar, t);
+        return;
+    }
+    const int tile = blockIdx.x - kIbCtas;
+    const int by = tile / ia.s.tiles_x, bx = tile - by * ia.s.tiles_x;
+    mac_node<S, SC>(ia.s, bx * kBlockX + threadIdx.x, by, true);
+}
+
+template <int S, int SC, int CO, bool LRN, int AV>
+__global__ void __launch_bounds__(kBlockX, 8) collide_ib_fused(const IbArgs ia)
+{
+    if (blockIdx.x < kIbCtas) {
+        for (int n = blockIdx.x * kBlockX + threadIdx.x; n < ia.nforced; n += kIbCtas * kBlockX)
+            ib_collide_item<S, CO, LRN, 1>(ia, n);
+        return;
+    }
+    const int tile = blockIdx.x - kIbCtas;
+    const int by = tile / ia.s.tiles_x, bx = tile - by * ia.s.tiles_x;
+    bulk_tile<S, CO, SC, LRN, 1, AV>(ia.s, bx, by, threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
