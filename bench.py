@@ -271,15 +271,22 @@ def run_ours(a):
     L = ip.lib()
     dump = [torch.empty((NY, NX), dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
     hist = torch.zeros((n_e2e, 1, 2), dtype=torch.float64).pin_memory().numpy()
+
+    def e2e_pass(nsteps):
+        lat.init_macros(*pin)
+        ip._lib.check(L.ippi_step(lat.handle, nsteps, 1), lat.handle)
+        n = L.ippi_force_history(lat.handle, hist.ctypes.data_as(C.POINTER(C.c_double)), nsteps)
+        for fld, buf in zip((ip.FIELD_RHO, ip.FIELD_UX, ip.FIELD_UY), dump):
+            ip._lib.check(L.ippi_download(lat.handle, fld, buf.ctypes.data_as(C.c_void_p), buf.nbytes),
+                          lat.handle)
+        return n
+
+    # one untimed pass (the download buffers are allocated on first use)
+    e2e_pass(max(a.warmup, 3))
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
-    lat.init_macros(*pin)
-    ip._lib.check(L.ippi_step(lat.handle, n_e2e, 1), lat.handle)
-    got = L.ippi_force_history(lat.handle, hist.ctypes.data_as(C.POINTER(C.c_double)), n_e2e)
-    for fld, buf in zip((ip.FIELD_RHO, ip.FIELD_UX, ip.FIELD_UY), dump):
-        ip._lib.check(L.ippi_download(lat.handle, fld, buf.ctypes.data_as(C.c_void_p), buf.nbytes),
-                      lat.handle)
+    got = e2e_pass(n_e2e)
     e2e_s = time.perf_counter() - t0
     assert got == n_e2e, got
     if dist:
