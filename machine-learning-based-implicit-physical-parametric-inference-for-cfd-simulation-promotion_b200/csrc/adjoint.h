@@ -31,6 +31,7 @@ struct AdjArgs {
     double* grad_tau;    // [nn] accumulated (tau field), or null
     double* xs;          // [nn][6] standardised features of learned nodes (else 0)
     double* up;          // [nn] dL / d softplus * out_scale of learned nodes (else 0)
+    double* lin;         // [nn][8] learned tau linearised: value, d tau / d x[6], in-range flag
     const double* dldm;  // [3][nn] loss on the post-stream moments, or null
     // immersed boundary (null when no markers)
     const IbArgs* ib;    // host copy of the forward's tables

@@ -1501,6 +1501,7 @@ int ippi_adjoint_backward(ippi_lbm* h, const double* dl_dforce, const double* dl
     double* lb = (double*)get(9 * nn * sizeof(double));
     A.lam_ft = (double*)get(9 * nn * sizeof(double));
     A.grad_tau = grad_tau ? (double*)get(nn * sizeof(double)) : nullptr;
+    A.lin = A.learned ? (double*)get(nn * 8 * sizeof(double)) : nullptr;
     double* gmlp = nullptr;
     double* part = nullptr;
     if (grad_mlp) {

@@ -232,8 +232,104 @@ __global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restric
     out[s] = softplus(z);
 }
 
+// The adjoint's weight gradient, FP64: sum over samples s of
+// Y[s] * d softplus(z(x_s)) / dw.  One sample per warp at a time, lane j =
+// neuron j of both hidden layers: row j of W2 in registers, its columns read
+// from shared memory (conflict-free), the other lanes' activations by
+// shuffle.  Lane j accumulates row j of dW2 and dW1 in registers; samples
+// with Y[s] = 0 (outside the network's range) are skipped.  Warp partials
+// are added in warp order into one partial per block, in the layout
+// mlp_reduce_kernel expects.
+__global__ void __launch_bounds__(kThreads) mlp_grad_up_f64_kernel(const double* __restrict__ X,
+                                                                   const double* __restrict__ Y, int n,
+                                                                   const float* __restrict__ W,
+                                                                   double* __restrict__ part)
+{
+    // W2 during the sample loop, the warp partials after it
+    __shared__ double smem[kWarps * kPartial];
+    __shared__ double hs[kWarps][kMlpHid], ds[kWarps][kMlpHid];  // per warp: h1, then d2
+    static_assert(kWarps * kPartial >= kMlpHid * kMlpHid, "W2 fits the partial buffer");
+    double* w2s = smem;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int p = tid; p < kMlpHid * kMlpHid; p += kThreads) w2s[p] = double(W[kMlpW2 + p]);
+    const int j = lane;
+    double w1[kMlpIn], w2r[kMlpHid];
+#pragma unroll
+    for (int i = 0; i < kMlpIn; i++) w1[i] = double(W[kMlpW1 + j * kMlpIn + i]);
+#pragma unroll
+    for (int i = 0; i < kMlpHid; i++) w2r[i] = double(W[kMlpW2 + j * kMlpHid + i]);
+    const double b1 = double(W[kMlpB1 + j]), b2 = double(W[kMlpB2 + j]), w3 = double(W[kMlpW3 + j]);
+    const double b3 = double(W[kMlpB3]);
+    __syncthreads();
+    double gW2[kMlpHid], gW1[kMlpIn];
+#pragma unroll
+    for (int i = 0; i < kMlpHid; i++) gW2[i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < kMlpIn; i++) gW1[i] = 0.0;
+    double gb1 = 0.0, gb2 = 0.0, gw3 = 0.0, gb3 = 0.0;
+    const int nw = gridDim.x * kWarps;
+    for (int s = blockIdx.x * kWarps + warp; s < n; s += nw) {
+        const double up = Y[s];
+        if (up == 0.0) continue;  // the same sample on every lane
+        double x[kMlpIn];
+#pragma unroll
+        for (int i = 0; i < kMlpIn; i++) x[i] = X[(size_t)s * kMlpIn + i];
+        double a1 = b1;
+#pragma unroll
+        for (int i = 0; i < kMlpIn; i++) a1 += w1[i] * x[i];
+        const double h1 = tanh(a1);
+        // the other lanes' values through shared memory, summed in four
+        // independent chains
+        hs[warp][j] = h1;
+        __syncwarp();
+        double p2[4] = {b2, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < kMlpHid; i++) p2[i & 3] += w2r[i] * hs[warp][i];
+        const double h2 = tanh((p2[0] + p2[1]) + (p2[2] + p2[3]));
+        double z = w3 * h2;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) z += __shfl_xor_sync(0xffffffffu, z, o);
+        z += b3;
+        const double dout = up * sigm(z);
+        const double d2 = dout * w3 * (1.0 - h2 * h2);
+        ds[warp][j] = d2;
+        __syncwarp();
+        double p1[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < kMlpHid; k++) p1[k & 3] += w2s[k * kMlpHid + j] * ds[warp][k];
+        const double d1 = ((p1[0] + p1[1]) + (p1[2] + p1[3])) * (1.0 - h1 * h1);
+#pragma unroll
+        for (int i = 0; i < kMlpHid; i++) gW2[i] += d2 * hs[warp][i];
+        __syncwarp();  // hs / ds are rewritten for the next sample
+#pragma unroll
+        for (int i = 0; i < kMlpIn; i++) gW1[i] += d1 * x[i];
+        gb2 += d2;
+        gb1 += d1;
+        gw3 += dout * h2;
+        gb3 += dout;
+    }
+    __syncthreads();  // W2 no longer read
+    double* r = smem + warp * kPartial;
+#pragma unroll
+    for (int i = 0; i < kMlpHid; i++) r[kMlpW2 + j * kMlpHid + i] = gW2[i];
+#pragma unroll
+    for (int i = 0; i < kMlpIn; i++) r[kMlpW1 + j * kMlpIn + i] = gW1[i];
+    r[kMlpB1 + j] = gb1;
+    r[kMlpB2 + j] = gb2;
+    r[kMlpW3 + j] = gw3;
+    if (j == 0) {
+        r[kMlpB3] = gb3;
+        r[kMlpParams] = 0.0;
+    }
+    __syncthreads();
+    for (int p = tid; p < kPartial; p += kThreads) {
+        double v = 0.0;
+        for (int w = 0; w < kWarps; w++) v += smem[w * kPartial + p];
+        part[(size_t)blockIdx.x * kPartial + p] = v;
+    }
+}
+
 bool g_grad_attr = false;
-bool g_grad_attr64 = false;
 
 }  // namespace
 
@@ -245,13 +341,7 @@ cudaError_t mlp_grad_upstream_f64(const double* xs, const double* up, int n, con
                                   double* grad, cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;
-    if (!g_grad_attr64) {
-        cudaError_t e = cudaFuncSetAttribute(mlp_grad_kernel<double, true>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_smem<double>());
-        if (e != cudaSuccess) return e;
-        g_grad_attr64 = true;
-    }
-    mlp_grad_kernel<double, true><<<IPPI_MLP_GRAD_BLOCKS, kThreads, grad_smem<double>(), st>>>(xs, up, n, w, part);
+    mlp_grad_up_f64_kernel<<<IPPI_MLP_GRAD_BLOCKS, kThreads, 0, st>>>(xs, up, n, w, part);
     mlp_reduce_kernel<double, true><<<(kPartial + 255) / 256, 256, 0, st>>>(part, IPPI_MLP_GRAD_BLOCKS, grad, nullptr);
     return cudaGetLastError();
 }

@@ -191,3 +191,62 @@ def test_torch_autograd_wrapper_gives_the_adjoint_gradient():
     L0, g = run_gpu(sc, p, nsteps, a, b, tau=tau0, grads=dict(tau=True))
     assert float(loss.detach()) == pytest.approx(L0, rel=1e-12)
     np.testing.assert_allclose(tau.grad.numpy(), g["tau"], rtol=1e-10, atol=1e-14)
+
+
+ADJ_CHILD = """
+import sys
+sys.path[:0] = [%r, %r]
+import numpy as np
+import ippi_lbm as ip
+import tau_mlp as tm
+from ippi_lbm import scenes
+out = []
+for les in (ip.LES_FIELD, ip.LES_LEARNED, ip.LES_SMAGORINSKY):
+    sc = scenes.cylinder_channel(64, 32, 8, 16.3, 16.1, 0.05, 60, collision=ip.MRT, storage=ip.F64)
+    p = dict(sc["params"]); p.update(les_model=les, tau0=0.56, cs=0.1)
+    g = ip.Lattice(64, 32, **p)
+    g.init_macros(*sc["init"]); g.set_markers(sc["markers"], ds=sc["ds"])
+    rng = np.random.default_rng(1)
+    if les == ip.LES_FIELD:
+        g.set_tau_field(0.56 + 0.02 * rng.random((32, 64)))
+    if les == ip.LES_LEARNED:
+        w = (tm.xavier_init(3) + rng.normal(0, 0.1, tm.NPARAM)).astype(np.float32)
+        st = np.concatenate([[1.0, 0.03, 0, 0, 0, 5e-3], [2e-3, 0.02, 0.5, 0.5, 0.5, 5e-3],
+                             [0.9, 0.0, -1, -1, -1, 0.0], [1.1, 0.2, 1, 1, 1, 0.2], [0.02]]).astype(np.float32)
+        g.load_tau_mlp_f32(w, st)
+    g.step(3, 1)
+    g.adjoint_forward(20, 4, 7)
+    a = rng.normal(0, 1, (20, 1, 2)); b = rng.normal(0, 1e-2, (3, 32, 64))
+    r = g.adjoint_backward(dl_dforce=a, dl_dmacro=b, tau=les == ip.LES_FIELD, mlp=les == ip.LES_LEARNED,
+                           f0=True)
+    out.append({k: np.asarray(v) for k, v in r.items() if v is not None})
+    g.close()
+np.savez(sys.argv[1], **{f"{i}_{k}": v for i, d in enumerate(out) for k, v in d.items()})
+"""
+
+
+def test_reverse_mode_mrt_collision_equals_dual_numbers(tmp_path):
+    """The hand-written reverse-mode MRT collision adjoint against the dual-
+    number kernel (IPPI_TEST_ADJ_DUAL=1) on the same rollouts: tau-field,
+    network-weight and initial-population gradients, learned / field /
+    Smagorinsky relaxation times, with IB markers."""
+    import os
+    import subprocess
+    import sys
+
+    from conftest import PKG_DIR, REPO
+
+    code = ADJ_CHILD % (PKG_DIR, os.path.join(REPO, "oracle"))
+    res = {}
+    for mode in ("0", "1"):
+        path = str(tmp_path / f"g{mode}.npz")
+        env = dict(os.environ, IPPI_TEST_ADJ_DUAL=mode)
+        r = subprocess.run([sys.executable, "-c", code, path], env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr[-3000:]
+        res[mode] = dict(np.load(path))
+    assert res["0"].keys() == res["1"].keys() and len(res["0"]) >= 4
+    for k in res["0"]:
+        a, b = res["0"][k], res["1"][k]
+        assert np.abs(b).max() > 0, k
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-10 * np.abs(b).max(), err_msg=k)
