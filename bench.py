@@ -353,6 +353,34 @@ def run_ncu_case(a):
     print(json.dumps({"ncu_case": WORKLOAD, "steps": a.steps}))
 
 
+def run_adjoint_ncu_case(a):
+    """The command profiled by ncu for the adjoint: the --adjoint lattice
+    (learned tau, seeded Xavier network), an --adjoint-steps rollout
+    checkpointed every 64 steps and its backward sweep with a random force
+    loss, twice."""
+    import numpy as np
+
+    import ippi_lbm as ip
+    from ippi_lbm import learned_tau as lt
+    from ippi_lbm import scenes
+
+    n = a.adjoint_steps
+    sc = scenes.cylinder_channel(1024, 256, 32, 256, 128, 0.04, 3900, collision=ip.MRT)
+    lat = ip.Lattice(1024, 256, **dict(sc["params"], les_model=ip.LES_LEARNED, storage=ip.F32))
+    lat.init_macros(*sc["init"])
+    lat.set_markers(sc["markers"], ds=sc["ds"])
+    stats = np.concatenate([[1.0, 0.04, 0, 0, 0, 1e-3], [2e-3, 0.02, 0.5, 0.5, 0.5, 1e-3],
+                            [0.9, 0.0, -1, -1, -1, 0.0], [1.1, 0.2, 1, 1, 1, 0.1],
+                            [1e-3]]).astype(np.float32)
+    lat.load_tau_mlp_f32(lt.xavier(0).astype(np.float32), stats)
+    wF = np.random.default_rng(0).normal(0, 1, (n, 1, 2))
+    for _ in range(2):
+        lat.adjoint_forward(n, 1, 64)
+        lat.adjoint_backward(dl_dforce=wF, mlp=True)
+    lat.close()
+    print(json.dumps({"adjoint_ncu_case": "channel_cylinder_1024x256_mrt_learned_tau_adjoint", "steps": n}))
+
+
 def run_learned(a):
     """The learned-tau comparison: a fine 4096 x 1024 plain-Smagorinsky run
     (the Cd reference and the data source), training on its filtered
@@ -509,11 +537,15 @@ def main():
                     help="precision studies of configs 2 and 3 instead of the MLUPS line")
     ap.add_argument("--validate-steps2", type=int, default=160000)
     ap.add_argument("--validate-steps3", type=int, default=20000)
+    ap.add_argument("--adjoint-ncu-case", action="store_true",
+                    help="short adjoint rollout and backward sweep for an ncu capture")
     ap.add_argument("--ncu-case", action="store_true",
                     help="short run of single launches for an ncu capture")
     a = ap.parse_args()
     if a.ncu_case:
         run_ncu_case(a)
+    elif a.adjoint_ncu_case:
+        run_adjoint_ncu_case(a)
     elif a.learned:
         run_learned(a)
     elif a.adjoint:
