@@ -9,6 +9,12 @@
 //                     samples (dW2[j][:] += d2[s][j] h1[s][:], ...).  Warp
 //                     sums are added in a fixed order into one partial per
 //                     block.
+//   mlp_grad_up_f64_kernel  the FP64 weight gradient of the adjoint (upstream
+//                     gradients per sample): one warp per sample and one
+//                     hidden neuron per lane, W2's row in registers, the other
+//                     lanes' activations and deltas staged in shared memory and
+//                     summed in four independent chains; samples whose
+//                     upstream gradient is zero are skipped.
 //   mlp_reduce_kernel the block partials summed in block order: gradient of
 //                     the mean squared error and the loss
 //   mlp_adam_kernel   Adam update, one thread per parameter

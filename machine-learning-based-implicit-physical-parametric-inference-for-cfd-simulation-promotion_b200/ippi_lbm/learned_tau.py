@@ -256,3 +256,126 @@ def strouhal(cl, d, u, pad=16):
         den = a - 2 * b + g
         k = k + (0.5 * (a - g) / den if den != 0 else 0.0)
     return float(k / n * d / u)
+
+
+# ---------------------------------------------------------------------------
+# the learned-tau experiment: fine plain run -> data -> training -> coarse runs
+# ---------------------------------------------------------------------------
+def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=160000,
+               avg_steps=64000, n_snap=200, max_samples=2_000_000, epochs=30, seed=0, device=0,
+               finetune_iters=0, finetune_lr=2e-3, log=None):
+    """Fine lattice (plain Smagorinsky MRT, FP32) -> `n_snap` filtered
+    snapshots over its averaging window -> training -> the coarse lattice
+    (nx/factor x ny/factor, same Re and Mach) with plain Smagorinsky and with
+    the learned tau.  Mean Cd / Cl and St over the same physical window, and
+    the device wall time of each run."""
+    from . import scenes
+
+    say = log or (lambda s: None)
+    cx, cy = nx / 4, ny / 2
+    fine = scenes.cylinder_channel(nx, ny, d, cx, cy, u, re, seed=seed)
+    first = fine_steps - avg_steps + 1
+    stride = max(avg_steps // n_snap, 1)
+    say(f"fine {nx}x{ny}: {fine_steps} steps, snapshots every {stride} from {first}")
+    rf = run_cylinder(fine, fine_steps, first, snapshot=(factor, first + stride - 1, stride, n_snap),
+                      device=device)
+    say(f"fine: Cd {rf['cd']:.5f} St {rf['st']:.4f} wall {rf['wall_s']:.2f} s")
+    mx, my, dc = nx // factor, ny // factor, d / factor
+    coarse = scenes.cylinder_channel(mx, my, dc, cx / factor, cy / factor, u, re, seed=seed)
+    tau0c = coarse["params"]["tau0"]
+    mask = cylinder_mask(mx, my, cx / factor, cy / factor, dc)
+    xs, ys = zip(*(samples_from_snapshot(s, tau0c, mask) for s in rf["snapshots"]))
+    x, y = np.concatenate(xs), np.concatenate(ys)
+    rng = np.random.default_rng(seed)
+    if x.shape[0] > max_samples:
+        sel = rng.choice(x.shape[0], max_samples, replace=False)
+        x, y = x[sel], y[sel]
+    t0 = time.perf_counter()
+    net, hist = train(x, y, epochs=epochs, seed=seed, device=device, log=log)
+    train_s = time.perf_counter() - t0
+    say(f"trained on {x.shape[0]} samples in {train_s:.1f} s, loss {hist[0]:.4g} -> {hist[-1]:.4g}")
+    csteps, cfirst = fine_steps // factor, (fine_steps - avg_steps) // factor + 1
+    rp = run_cylinder(coarse, csteps, cfirst, device=device)
+    rl = run_cylinder(coarse, csteps, cfirst, net=net, device=device)
+    say(f"coarse plain: Cd {rp['cd']:.5f}; learned: Cd {rl['cd']:.5f}")
+    tuned = None
+    if finetune_iters:
+        t1 = time.perf_counter()
+        net_ft, ft_hist = train_through_solver(net, coarse, rf["cd"], iters=finetune_iters,
+                                               spinup=cfirst - 1, lr=finetune_lr, device=device, log=log)
+        ft_s = time.perf_counter() - t1
+        rt = run_cylinder(coarse, csteps, cfirst, net=net_ft, device=device)
+        say(f"coarse learned + through-solver training: Cd {rt['cd']:.5f}")
+        tuned = dict(cd=rt["cd"], st=rt["st"], wall_s=rt["wall_s"],
+                     cd_rel_err=abs(rt["cd"] - rf["cd"]) / abs(rf["cd"]), iters=finetune_iters,
+                     train_seconds=ft_s, history=ft_hist)
+        net = net_ft
+
+    def err(r):
+        return abs(r["cd"] - rf["cd"]) / abs(rf["cd"])
+
+    return dict(
+        fine=dict(nx=nx, ny=ny, steps=fine_steps, cd=rf["cd"], cl=rf["cl"], st=rf["st"],
+                  wall_s=rf["wall_s"]),
+        coarse_plain=dict(nx=mx, ny=my, steps=csteps, cd=rp["cd"], st=rp["st"], wall_s=rp["wall_s"],
+                          cd_rel_err=err(rp)),
+        coarse_learned=dict(nx=mx, ny=my, steps=csteps, cd=rl["cd"], st=rl["st"], wall_s=rl["wall_s"],
+                            cd_rel_err=err(rl)),
+        training=dict(samples=int(x.shape[0]), epochs=epochs, loss_first=hist[0], loss_last=hist[-1],
+                      seconds=train_s),
+        coarse_learned_through_solver=tuned,
+        speedup_vs_fine=rf["wall_s"] / rl["wall_s"],
+        net=net)
+
+
+# ---------------------------------------------------------------------------
+# end-to-end training through the solver (adjoint)
+# ---------------------------------------------------------------------------
+def train_through_solver(net, sc, cd_ref, iters=8, nsteps=4000, ckpt=64, spinup=12000, lr=2e-3,
+                         device=0, log=None):
+    """Fine-tune the network so that the coarse lattice's mean drag over an
+    nsteps window (after `spinup` steps) matches cd_ref.  Loss
+    ((<Cd> - cd_ref) / cd_ref)^2; its gradient with respect to the FP32
+    weights comes from the adjoint (NetworkRollout), the update from the
+    library's Adam kernel.  Returns (net with new weights, history)."""
+    import torch
+
+    from .autograd import NetworkRollout, Rollout
+    from .lattice import Lattice
+
+    params = dict(sc["params"], les_model=L.LES_LEARNED)
+    lat = Lattice(sc["nx"], sc["ny"], device=device, **params)
+    lat.set_markers(sc["markers"], ds=sc["ds"])
+    stats = net.stats()
+    dev = torch.device("cuda", device)
+    wd = torch.from_numpy(net.w.astype(np.float32)).to(dev)
+    md, vd, gd = torch.zeros_like(wd), torch.zeros_like(wd), torch.zeros_like(wd)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    lib = L.lib()
+
+    def reset(lt_):
+        lt_.init_macros(*sc["init"])
+        lt_.load_tau_mlp_f32(wd.cpu().numpy(), stats)
+        lt_.step(spinup, 1)
+
+    roll = Rollout(lat, reset, nsteps, spinup + 1, ckpt, stats)
+    q = 0.5 * sc["u_ref"] ** 2 * sc["d"]
+    hist = []
+    for it in range(iters):
+        w = wd.cpu().clone().requires_grad_(True)
+        t0 = time.perf_counter()
+        forces, _ = NetworkRollout.apply(w, roll)
+        cd = forces[:, 0, 0].mean() / q
+        loss = ((cd - cd_ref) / cd_ref) ** 2
+        loss.backward()
+        gd.copy_(w.grad.float())
+        L.check(lib.ippi_mlp_adam(wd.data_ptr(), gd.data_ptr(), md.data_ptr(), vd.data_ptr(), it + 1, lr,
+                                  0.9, 0.999, 1e-8, stream))
+        torch.cuda.synchronize(dev)
+        hist.append(dict(cd=float(cd.detach()), loss=float(loss.detach()), seconds=time.perf_counter() - t0))
+        if log:
+            log(f"through-solver {it}: Cd {hist[-1]['cd']:.5f} loss {hist[-1]['loss']:.4g} "
+                f"({hist[-1]['seconds']:.1f} s)")
+    lat.close()
+    out = TauNet(wd.cpu().numpy(), net.mean, net.std, net.lo, net.hi, net.out_scale)
+    return out, hist

@@ -39,3 +39,18 @@ def test_seeded_cylinders_keep_their_gap():
 def test_config3_scene_bodies():
     sc = config3_scene(2048, 512, d=48, n=4)
     assert sc["bodies"].max() == 3 and len(sc["bodies"]) == len(sc["ds"]) == 4 * 151
+
+
+def test_bench_modes_resolve_their_drivers():
+    """Every driver function the bench's learned and adjoint modes call is
+    present in the package (import-level check; the runs need a GPU)."""
+    import inspect
+
+    from ippi_lbm import learned_tau as lt
+    from ippi_lbm.autograd import NetworkRollout, Rollout
+
+    assert callable(NetworkRollout.apply) and inspect.isclass(Rollout)
+    sig = inspect.signature(lt.experiment)
+    for k in ("fine_steps", "avg_steps", "device", "finetune_iters"):
+        assert k in sig.parameters, k
+    assert "iters" in inspect.signature(lt.train_through_solver).parameters

@@ -212,3 +212,20 @@ def test_pipeline_small_end_to_end():
     coarse = scenes.cylinder_channel(128, 32, 8, 32, 16, 0.05, 300, collision=ip.MRT)
     out = lt.run_cylinder(coarse, 1500, 1001, net=net)
     assert np.isfinite(out["cd"]) and out["cd"] > 0
+
+
+def test_experiment_driver_small():
+    """The learned-tau experiment driver end to end on a small channel (the
+    code path behind the bench's learned mode): fine run, filtered snapshots,
+    training, the coarse plain and learned runs and one through-solver
+    iteration, with every reported figure finite."""
+    r = lt.experiment(nx=512, ny=128, d=32, u=0.05, re=300.0, fine_steps=2000, avg_steps=800,
+                      n_snap=10, epochs=3, finetune_iters=1)
+    for k in ("fine", "coarse_plain", "coarse_learned"):
+        assert np.isfinite(r[k]["cd"]) and r[k]["cd"] > 0, k
+        assert r[k]["wall_s"] > 0, k
+    assert r["coarse_plain"]["nx"] == 128 and r["coarse_learned"]["steps"] == 500
+    assert r["speedup_vs_fine"] > 0
+    ts = r["coarse_learned_through_solver"]
+    assert ts["iters"] == 1 and len(ts["history"]) == 1 and np.isfinite(ts["cd"])
+    assert r["training"]["samples"] > 0
