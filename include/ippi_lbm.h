@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define IPPI_ABI_VERSION 2
+#define IPPI_ABI_VERSION 3
 
 /* status codes */
 #define IPPI_OK 0
@@ -98,7 +98,9 @@ extern "C" {
 #define IPPI_FIELD_AVG_V 6
 #define IPPI_FIELD_AVG_RHO 7
 #define IPPI_FIELD_FLAGS 8   /* uint8 [ny][nx]: JudgeStyle chars f i o m d u (w) */
-#define IPPI_FIELD_NNFLAG 9  /* double [ny][nx]: 1 where a boundary net sets tau */
+#define IPPI_FIELD_NNFLAG 9  /* double [ny][nx]: 1 where a boundary net sets tau;
+                                with IPPI_LES_LEARNED, 1 where the learned network
+                                set it (0: Smagorinsky fallback, solid nodes) */
 
 typedef struct ippi_lbm ippi_lbm;
 
@@ -294,6 +296,40 @@ int ippi_solid_force(ippi_lbm* h, double* force_xy);
 /* IPPI_LES_DYNAMIC: the wall distance d[ny][nx] of every node (Mesh::
  * SetNormalDis, mesh.cpp:1935-1953, computes it for the cylinder). */
 int ippi_set_wall_distance(ippi_lbm* h, const double* dist);
+
+/* No counterpart in the reference (its state is written only as Tecplot
+ * text, mesh.cpp:1180-1233).  Diagnostics of the state after the last step,
+ * for a metrics log: the largest |u| over the non-solid nodes (NaN once the
+ * state holds a NaN), and with IPPI_LES_LEARNED the number of non-solid nodes
+ * whose relaxation time the network set and the number where the features
+ * left its training range and Smagorinsky set it (both 0 for other models).
+ * Any output may be NULL.  Synchronises. */
+int ippi_diagnostics(ippi_lbm* h, double* max_u, long long* net_nodes, long long* fallback_nodes);
+
+/* No counterpart in the reference (it has no restart path).  Checkpoint and
+ * resume of the evolving state: both population buffers (the current one and
+ * the input of the last step, which downloads re-run), the running means, the
+ * flat-plate corner values, the drag/lift of the last step and the force
+ * history, and the step bookkeeping (last user step, internal step count).
+ * The configuration is not saved: the resuming handle is created and set up
+ * (parameters, markers, solid mask, wall distance, tau field or network) as
+ * the saving one was; a hash of the parameters, markers and solid mask in the
+ * checkpoint must match, and so must the FP64 mass the state gives when its
+ * last step is re-run under the resuming handle's configuration.  The buffer
+ * also carries a hash of its payload.  Layout: a fixed header then the raw
+ * device sections, native byte order.
+ *
+ * ippi_state_bytes: size of the checkpoint of this handle.
+ * ippi_save_state: write it into host[bytes] (bytes >= ippi_state_bytes);
+ *   IPPI_ERR_STATE before the handle's first step.
+ * ippi_load_state: restore from host[bytes]; *last_step (may be NULL) gets the
+ *   user step number of the saved state's last step, so stepping resumes at
+ *   *last_step + 1.  IPPI_ERR_ARG on a bad magic, version, size, hash or mass;
+ *   on a mass mismatch the handle holds the loaded state but must not be
+ *   trusted.  Synchronise. */
+int ippi_state_bytes(ippi_lbm* h, size_t* bytes);
+int ippi_save_state(ippi_lbm* h, void* host, size_t bytes);
+int ippi_load_state(ippi_lbm* h, const void* host, size_t bytes, int* last_step);
 
 /* Last error message of the handle (or of the library when h is NULL). */
 int ippi_last_error(ippi_lbm* h, char* buf, size_t n);

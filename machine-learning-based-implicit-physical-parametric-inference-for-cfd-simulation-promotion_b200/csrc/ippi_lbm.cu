@@ -832,6 +832,86 @@ int materialize(ippi_lbm* h)
     return IPPI_OK;
 }
 
+// ---------------------------------------------------------------------------
+// checkpoint layout: a fixed header, then the device sections in this order
+// ---------------------------------------------------------------------------
+constexpr char kCkpMagic[8] = {'I', 'P', 'P', 'I', 'C', 'K', 'P', '1'};
+
+struct CkpHeader {
+    char magic[8];
+    uint32_t abi, header_bytes;
+    uint64_t config_hash;
+    int32_t nx, ny, storage, nbody, hist_cap, cur;
+    int64_t kcount, last_t, hist_written;
+    uint64_t f_bytes, avg_bytes, corner_bytes, force_bytes, hist_bytes;
+    double mass;            // FP64 mass of the state (ippi_forces), re-checked on load
+    uint64_t payload_hash;  // ckp_hash of everything after the header
+};
+
+struct CkpLayout {
+    size_t f, avg, corner, force, hist, total;
+};
+
+struct CkpSection {
+    void* dev;
+    size_t bytes;
+};
+
+CkpLayout ckp_layout(const ippi_lbm* h)
+{
+    const size_t nn = (size_t)h->p.nx * h->p.ny;
+    CkpLayout L;
+    L.f = (size_t)9 * h->plane * h->tsize;
+    L.avg = 3 * nn * h->csize;
+    L.corner = 24 * (size_t)h->csize;
+    L.force = h->force_now ? (size_t)h->nbody * 2 * sizeof(double) : 0;
+    L.hist = h->force_hist ? (size_t)h->hist_cap * h->nbody * 2 * sizeof(double) : 0;
+    L.total = sizeof(CkpHeader) + 2 * L.f + L.avg + L.corner + L.force + L.hist;
+    return L;
+}
+
+std::vector<CkpSection> ckp_sections(ippi_lbm* h, const CkpLayout& L)
+{
+    return {{h->f[0], L.f},         {h->f[1], L.f},          {h->avg, L.avg},
+            {h->corner, L.corner}, {h->force_now, L.force}, {h->force_hist, L.hist}};
+}
+
+// FNV-1a over 64-bit words (bytes for the tail), each step followed by a
+// right xor-shift so that high bits reach the low ones
+uint64_t ckp_hash(const unsigned char* p, size_t n, uint64_t x = 0xcbf29ce484222325ull)
+{
+    constexpr uint64_t prime = 0x100000001b3ull;
+    size_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+        uint64_t w;
+        std::memcpy(&w, p + i, 8);
+        x = (x ^ w) * prime;
+        x ^= x >> 29;
+    }
+    for (; i < n; i++) x = (x ^ p[i]) * prime;
+    return x;
+}
+
+// what the saved state presumes of the handle: parameters (not the device),
+// markers and solid mask
+uint64_t ckp_config_hash(const ippi_lbm* h)
+{
+    const ippi_params& p = h->p;
+    uint64_t x = 0xcbf29ce484222325ull;
+    auto put = [&](const void* v, size_t n) { x = ckp_hash(static_cast<const unsigned char*>(v), n, x); };
+    const int32_t ints[] = {p.nx, p.ny, p.collision, p.storage, p.bc_set, p.les_model,
+                            p.plate_x0, p.avg_start, p.delta_kernel, p.mdf_iters, h->nbody, h->hist_cap};
+    const double dbl[] = {p.tau0, p.cs, p.u_in, p.rho0};
+    put(ints, sizeof ints);
+    put(dbl, sizeof dbl);
+    put(h->mk_xy.data(), h->mk_xy.size() * sizeof(double));
+    put(h->mk_ub.data(), h->mk_ub.size() * sizeof(double));
+    put(h->mk_ds.data(), h->mk_ds.size() * sizeof(double));
+    put(h->mk_body.data(), h->mk_body.size() * sizeof(int));
+    put(h->solid.data(), h->solid.size());
+    return x;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1324,6 +1404,119 @@ int ippi_get_stream(ippi_lbm* h, void** stream)
 {
     if (!h || !stream) return fail(h, IPPI_ERR_ARG, "null argument");
     *stream = (void*)h->st;
+    return IPPI_OK;
+}
+
+int ippi_diagnostics(ippi_lbm* h, double* max_u, long long* net_nodes, long long* fallback_nodes)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    CK(h, cudaSetDevice(h->p.device));
+    int rc = materialize(h);
+    if (rc) return rc;
+    const size_t nn = (size_t)h->p.nx * h->p.ny;
+    const int learned = h->p.les_model == IPPI_LES_LEARNED;
+    unsigned long long* out = reinterpret_cast<unsigned long long*>(h->red);
+    CK(h, cudaMemsetAsync(out, 0, 3 * sizeof(unsigned long long), h->st));
+    const unsigned nblk = (unsigned)std::min<size_t>((nn + 255) / 256, 4 * 148);
+    diag_kernel<<<nblk, 256, 0, h->st>>>(h->dl + 9 * nn, h->nflag, (long long)nn, learned, out);
+    CK(h, cudaGetLastError());
+    unsigned long long r[3];
+    CK(h, cudaMemcpyAsync(r, out, sizeof r, cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    if (max_u) std::memcpy(max_u, &r[0], sizeof(double));
+    if (net_nodes) *net_nodes = (long long)r[1];
+    if (fallback_nodes) *fallback_nodes = (long long)r[2];
+    return IPPI_OK;
+}
+
+int ippi_state_bytes(ippi_lbm* h, size_t* bytes)
+{
+    if (!h || !bytes) return fail(h, IPPI_ERR_ARG, "null argument");
+    *bytes = ckp_layout(h).total;
+    return IPPI_OK;
+}
+
+int ippi_save_state(ippi_lbm* h, void* host, size_t bytes)
+{
+    if (!h || !host) return fail(h, IPPI_ERR_ARG, "null argument");
+    const CkpLayout L = ckp_layout(h);
+    if (bytes < L.total) return fail(h, IPPI_ERR_ARG, "checkpoint needs %zu bytes, got %zu", L.total, bytes);
+    CK(h, cudaSetDevice(h->p.device));
+    if (h->pending_init) return fail(h, IPPI_ERR_STATE, "no state to save before the first step");
+    CkpHeader hd{};
+    std::memcpy(hd.magic, kCkpMagic, sizeof hd.magic);
+    hd.abi = IPPI_ABI_VERSION;
+    hd.header_bytes = sizeof(CkpHeader);
+    hd.config_hash = ckp_config_hash(h);
+    hd.nx = h->p.nx;
+    hd.ny = h->p.ny;
+    hd.storage = h->p.storage;
+    hd.nbody = h->nbody;
+    hd.hist_cap = h->hist_cap;
+    hd.cur = h->cur;
+    hd.kcount = h->kcount;
+    hd.last_t = h->last_t;
+    hd.hist_written = h->hist_written;
+    hd.f_bytes = L.f;
+    hd.avg_bytes = L.avg;
+    hd.corner_bytes = L.corner;
+    hd.force_bytes = L.force;
+    hd.hist_bytes = L.hist;
+    int rc = ippi_forces(h, nullptr, nullptr, &hd.mass);
+    if (rc) return rc;
+    CK(h, cudaStreamSynchronize(h->st));
+    unsigned char* p = static_cast<unsigned char*>(host) + sizeof(CkpHeader);
+    for (const CkpSection& s : ckp_sections(h, L)) {
+        if (s.bytes) CK(h, cudaMemcpy(p, s.dev, s.bytes, cudaMemcpyDeviceToHost));
+        p += s.bytes;
+    }
+    hd.payload_hash = ckp_hash(static_cast<unsigned char*>(host) + sizeof(CkpHeader), L.total - sizeof(CkpHeader));
+    std::memcpy(host, &hd, sizeof hd);
+    return IPPI_OK;
+}
+
+int ippi_load_state(ippi_lbm* h, const void* host, size_t bytes, int* last_step)
+{
+    if (!h || !host) return fail(h, IPPI_ERR_ARG, "null argument");
+    if (bytes < sizeof(CkpHeader)) return fail(h, IPPI_ERR_ARG, "checkpoint shorter than its header");
+    CkpHeader hd;
+    std::memcpy(&hd, host, sizeof hd);
+    if (std::memcmp(hd.magic, kCkpMagic, sizeof hd.magic) != 0) return fail(h, IPPI_ERR_ARG, "not a checkpoint");
+    if (hd.abi != IPPI_ABI_VERSION || hd.header_bytes != sizeof(CkpHeader))
+        return fail(h, IPPI_ERR_ARG, "checkpoint of ABI %u, this library is %d", hd.abi, IPPI_ABI_VERSION);
+    const CkpLayout L = ckp_layout(h);
+    if (hd.nx != h->p.nx || hd.ny != h->p.ny || hd.storage != h->p.storage || hd.nbody != h->nbody ||
+        hd.hist_cap != h->hist_cap || hd.f_bytes != L.f || hd.avg_bytes != L.avg || hd.corner_bytes != L.corner ||
+        hd.force_bytes != L.force || hd.hist_bytes != L.hist)
+        return fail(h, IPPI_ERR_ARG, "checkpoint of a %dx%d lattice (storage %d, %d bodies) does not fit this handle",
+                    hd.nx, hd.ny, hd.storage, hd.nbody);
+    if (bytes < L.total) return fail(h, IPPI_ERR_ARG, "checkpoint truncated (%zu of %zu bytes)", bytes, L.total);
+    if (hd.config_hash != ckp_config_hash(h))
+        return fail(h, IPPI_ERR_ARG, "checkpoint of another configuration (parameters, markers or solid mask)");
+    if (hd.cur != 0 && hd.cur != 1) return fail(h, IPPI_ERR_ARG, "checkpoint buffer index %d", hd.cur);
+    const unsigned char* p = static_cast<const unsigned char*>(host) + sizeof(CkpHeader);
+    if (ckp_hash(p, L.total - sizeof(CkpHeader)) != hd.payload_hash)
+        return fail(h, IPPI_ERR_ARG, "checkpoint payload hash mismatch (corrupted)");
+    CK(h, cudaSetDevice(h->p.device));
+    CK(h, cudaStreamSynchronize(h->st));
+    for (const CkpSection& s : ckp_sections(h, L)) {
+        if (s.bytes) CK(h, cudaMemcpy(s.dev, p, s.bytes, cudaMemcpyHostToDevice));
+        p += s.bytes;
+    }
+    std::memset(h->ctr_h, 0, sizeof(Ctr));
+    CK(h, cudaMemcpy(h->ctr, h->ctr_h, sizeof(Ctr), cudaMemcpyHostToDevice));
+    h->cur = hd.cur;
+    h->kcount = (int)hd.kcount;
+    h->last_t = (int)hd.last_t;
+    h->hist_written = hd.hist_written;
+    h->pending_init = false;
+    h->dl_valid = false;
+    double mass = 0.0;
+    int rc = ippi_forces(h, nullptr, nullptr, &mass);
+    if (rc) return rc;
+    if (std::memcmp(&mass, &hd.mass, sizeof mass) != 0)
+        return fail(h, IPPI_ERR_ARG, "checkpoint mass %.17g, this configuration gives %.17g", hd.mass, mass);
+    if (last_step) *last_step = h->last_t;
     return IPPI_OK;
 }
 

@@ -501,6 +501,24 @@ __device__ Dual<N> learned_tau(Dual<N> pxx, Dual<N> pxy, Dual<N> pyy, Dual<N> rh
     return t;
 }
 
+// whether a node's learned-model features lie inside the network's training
+// range (the network sets tau there, Smagorinsky outside it): the same
+// features and comparisons as learned_tau
+template <typename C>
+__device__ __forceinline__ bool learned_in_range(const C* f, C rho, C ux, C uy, C rb, C tau0,
+                                                 const float* __restrict__ w)
+{
+    C pxx, pxy, pyy, x[kMlpIn];
+    pi_neq<C>(f, rho, ux, uy, rb, pxx, pxy, pyy);
+    mlp_features<C>(pxx, pxy, pyy, rho, ux, uy, tau0, x);
+    const float* st = w + kMlpParams;
+    bool in = true;
+#pragma unroll
+    for (int i = 0; i < kMlpIn; i++)
+        in = in && x[i] >= C(__ldg(st + 2 * kMlpIn + i)) && x[i] <= C(__ldg(st + 3 * kMlpIn + i));
+    return in;
+}
+
 // relaxation time of a node's next collision: tau0, Smagorinsky, or (LRN)
 // the learned model with its Smagorinsky fallback
 template <typename C, bool LRN = false>

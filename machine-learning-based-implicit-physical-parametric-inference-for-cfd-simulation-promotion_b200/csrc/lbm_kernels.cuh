@@ -531,6 +531,9 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
                                                               prm<C>(a.cs, a.f_cs), a.mlp);
                 if (a.mode >= MODE_MAT) {
                     a.dl_tau[node] = double(tau);
+                    if (LRN)  // 1 where the network set tau, 0 where Smagorinsky did
+                        a.dl_m[3ll * a.nx * a.ny + node] =
+                            learned_in_range<C>(f, rho, ux, uy, rbs, prm<C>(a.tau0, a.f_tau0), a.mlp) ? 1.0 : 0.0;
                 } else {
                     collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
 #pragma unroll
@@ -982,6 +985,9 @@ __device__ __forceinline__ void ib_collide_item(const IbArgs& ia, int n)
                                                   prm<C>(a.cs, a.f_cs), a.mlp);
     if (a.mode >= MODE_MAT) {
         a.dl_tau[(long long)xy.y * a.nx + xy.x] = double(tau);
+        if (LRN)
+            a.dl_m[3ll * a.nx * a.ny + (long long)xy.y * a.nx + xy.x] =
+                learned_in_range<C>(f, rho, ux, uy, rbs, prm<C>(a.tau0, a.f_tau0), a.mlp) ? 1.0 : 0.0;
     } else {
         collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
         add_force<C, CO>(f, ux, uy, C(ia.fx[n]), C(ia.fy[n]), prm<C>(a.tau0, a.f_tau0), tau);
@@ -1276,6 +1282,42 @@ static __global__ void sum_partial_kernel(const double* in, long long n, double*
         __syncthreads();
     }
     if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// run diagnostics of the materialised moments m = [rho, ux, uy, net flag]
+// [ny][nx] over the non-solid nodes: out[0] = bit pattern of the largest |u|
+// (non-negative doubles order as their bit patterns, and a NaN's pattern lies
+// above every number's, so one NaN shows), out[1] / out[2] = nodes with the
+// net flag set / clear (learned model only).  out[] is zeroed by the caller.
+static __global__ void diag_kernel(const double* __restrict__ m, const uint8_t* __restrict__ nflag, long long nn,
+                                   int learned, unsigned long long* out)
+{
+    unsigned long long mx = 0, net = 0, fb = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nn;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (nflag[i] & NF_SOLID) continue;
+        const double ux = m[nn + i], uy = m[2 * nn + i];
+        const unsigned long long b = (unsigned long long)__double_as_longlong(sqrt(ux * ux + uy * uy));
+        mx = b > mx ? b : mx;
+        if (learned) {
+            if (m[3 * nn + i] != 0.0) net++;
+            else fb++;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long v = __shfl_xor_sync(0xffffffffu, mx, o);
+        mx = v > mx ? v : mx;
+        net += __shfl_xor_sync(0xffffffffu, net, o);
+        fb += __shfl_xor_sync(0xffffffffu, fb, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(out, mx);
+        if (learned) {
+            atomicAdd(out + 1, net);
+            atomicAdd(out + 2, fb);
+        }
+    }
 }
 
 }  // namespace ippi

@@ -11,6 +11,7 @@
 //             [--nets DIR] [--init FILE] [--batched] [--print N] [--device N]
 //             [--xflow DIR] [--xflow-offset N] [--xflow-init] [--xflow-abs N]
 //             [--les none|smagorinsky|wale|csm|dynamic]
+//             [--checkpoint FILE] [--resume FILE] [--metrics FILE]
 //
 //   plate    the reference's scene: flat plate, NEE inlet u = --u, Re 5e5,
 //            tau = 0.5 + 6 (Ny U / Re) (main.cpp:37-43)
@@ -38,6 +39,12 @@
 //                  --xflow-offset); --xflow-init: Mesh::ManageDataFromXflow
 //                  after step 1; --xflow-abs N: Mesh::XflowABS every N steps
 //                  (the coupling blocks of the reference's main.cpp:132-156)
+//   --checkpoint FILE  the device state (Mesh::SaveCheckpoint) at every save
+//                  point and after the last step
+//   --resume FILE  continue from such a checkpoint, set up with the same
+//                  options, at the step after the one it holds
+//   --metrics FILE a JSON line (Mesh::LogMetrics) at every --print step
+#include <chrono>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -67,6 +74,7 @@ struct Options {
     int xflow_abs = 0;
     int les = -1;
     string nets, init;
+    string checkpoint, resume, metrics;
     bool batched = false;
     int print = 1;
     int device = 0;
@@ -111,6 +119,9 @@ bool parse(int argc, char** argv, Options& o)
             if (o.les == -2) return false;
         }
         else if (a == "--cp" && need(1)) o.cp = atoi(argv[++i]);
+        else if (a == "--checkpoint" && need(1)) o.checkpoint = argv[++i];
+        else if (a == "--resume" && need(1)) o.resume = argv[++i];
+        else if (a == "--metrics" && need(1)) o.metrics = argv[++i];
         else if (a == "--nets" && need(1)) o.nets = argv[++i];
         else if (a == "--init" && need(1)) o.init = argv[++i];
         else if (a == "--batched") o.batched = true;
@@ -145,7 +156,8 @@ int main(int argc, char* argv[])
                 "                 [--avg N] [--re R] [--u U] [--cs C] [--cylinder X Y D] [--markers N]\n"
                 "                 [--solid] [--cp START] [--nets DIR] [--init FILE] [--batched]\n"
                 "                 [--print N] [--device N] [--xflow DIR] [--xflow-offset N]\n"
-                "                 [--xflow-init] [--xflow-abs N] [--les none|smagorinsky|wale|csm|dynamic]"
+                "                 [--xflow-init] [--xflow-abs N] [--les none|smagorinsky|wale|csm|dynamic]\n"
+                "                 [--checkpoint FILE] [--resume FILE] [--metrics FILE]"
              << endl;
         return 2;
     }
@@ -218,7 +230,16 @@ int main(int argc, char* argv[])
     cout << "Start Computing" << endl;
 
     const bool forces = channel && o.cylinder && !solid;
-    for (int t = 1; t <= o.steps;) {
+    int first = 1;
+    if (!o.resume.empty()) {
+        const int last = mesh.LoadCheckpoint(o.resume);
+        if (last < 0) return 1;
+        first = last + 1;
+        cout << "Resumed at step " << first << " from " << o.resume << endl;
+    }
+    auto t_mark = std::chrono::steady_clock::now();
+    int s_mark = first - 1;
+    for (int t = first; t <= o.steps;) {
         int n = 1;
         if (o.batched) {
             // up to the next save point
@@ -257,8 +278,19 @@ int main(int argc, char* argv[])
             }
         }
         mesh.ComputeAvgVelocity(last);
-        if (o.print > 0 && (last % o.print == 0 || last == o.steps))
-            cout << "Compute Step:" << " " << last << endl;
+        const bool report = o.print > 0 && (last % o.print == 0 || last == o.steps);
+        if (report) cout << "Compute Step:" << " " << last << endl;
+        if (!o.metrics.empty() && report) {
+            const auto now = std::chrono::steady_clock::now();
+            const double sec = std::chrono::duration<double>(now - t_mark).count();
+            const double mlups = sec > 0 ? (double)Nx * Ny * (last - s_mark) / sec * 1e-6 : 0.0;
+            mesh.LogMetrics(o.metrics, last, mlups, o.u, o.d);
+            t_mark = std::chrono::steady_clock::now();
+            s_mark = last;
+        }
+        if (!o.checkpoint.empty() && ((o.save > 0 && last % o.save == 0) || last == o.steps) &&
+            !mesh.SaveCheckpoint(o.checkpoint))
+            return 1;
     }
     return mesh.errorflag;
 }

@@ -718,3 +718,84 @@ void Mesh::OutputForces(int t, double U, double D)
     out.precision(12);
     out << t << " " << f[0] << " " << f[1] << " " << f[0] / q << " " << f[1] / q << "\n";
 }
+
+// ---------------------------------------------------------------------------
+// additions: checkpoint / resume and the metrics log (no reference code; the
+// reference writes Tecplot text only and has no restart path)
+// ---------------------------------------------------------------------------
+bool Mesh::SaveCheckpoint(const std::string& path)
+{
+    if (!h_) return false;
+    size_t n = 0;
+    if (!check(ippi_state_bytes(h_, &n), "ippi_state_bytes")) return false;
+    std::vector<unsigned char> buf(n);
+    if (!check(ippi_save_state(h_, buf.data(), n), "ippi_save_state")) return false;
+    const std::string tmp = path + ".tmp";
+    {
+        std::ofstream out(tmp, std::ios::binary | std::ios::trunc);
+        if (!out.write(reinterpret_cast<const char*>(buf.data()), (std::streamsize)n)) {
+            cerr << "cannot write " << tmp << endl;
+            return false;
+        }
+    }
+    if (std::rename(tmp.c_str(), path.c_str()) != 0) {
+        cerr << "cannot rename " << tmp << " to " << path << endl;
+        return false;
+    }
+    return true;
+}
+
+int Mesh::LoadCheckpoint(const std::string& path)
+{
+    if (!h_) return -1;
+    std::ifstream in(path, std::ios::binary | std::ios::ate);
+    if (!in) {
+        cerr << "cannot read " << path << endl;
+        return -1;
+    }
+    const std::streamsize n = in.tellg();
+    std::vector<unsigned char> buf((size_t)n);
+    in.seekg(0);
+    if (!in.read(reinterpret_cast<char*>(buf.data()), n)) {
+        cerr << "cannot read " << path << endl;
+        return -1;
+    }
+    int last = -1;
+    if (!check(ippi_load_state(h_, buf.data(), buf.size(), &last), "ippi_load_state")) return -1;
+    last_t_ = last;
+    synced_ = false;
+    return last;
+}
+
+void Mesh::LogMetrics(const std::string& path, int t, double mlups, double U, double D)
+{
+    if (!h_) return;
+    int nb = 0;
+    double mass = 0, f[2] = {0, 0};
+    if (!check(ippi_forces(h_, nullptr, &nb, &mass), "ippi_forces")) return;
+    if (nb > 0) BodyForces(f, 1);
+    double max_u = 0;
+    long long net = 0, fallback = 0;
+    if (!check(ippi_diagnostics(h_, &max_u, &net, &fallback), "ippi_diagnostics")) return;
+    const int bytes = Storage == IPPI_F64 ? 144 : (Storage == IPPI_F32 ? 72 : 36);
+    std::ofstream out(path, std::ios::app);
+    out.precision(17);
+    auto num = [&](double v) -> std::ostream& {
+        if (std::isfinite(v)) out << v;
+        else out << "null";
+        return out;
+    };
+    const double q = 0.5 * U * U * D;
+    out << "{\"step\": " << t << ", \"mlups\": ";
+    num(mlups) << ", \"hbm_gbs\": ";
+    num(mlups * bytes * 1e-3) << ", \"mass\": ";
+    num(mass) << ", \"cd\": ";
+    if (nb > 0 && q > 0) {
+        num(f[0] / q) << ", \"cl\": ";
+        num(f[1] / q);
+    } else {
+        out << "null, \"cl\": null";
+    }
+    out << ", \"max_u\": ";
+    num(max_u) << ", \"tau_net_nodes\": " << net << ", \"tau_fallback_nodes\": " << fallback << "}\n";
+}

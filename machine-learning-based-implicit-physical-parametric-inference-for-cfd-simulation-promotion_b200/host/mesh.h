@@ -122,6 +122,17 @@ public:
     void DragLift(double U, double D, double* cd, double* cl);
     // one line "t Fx Fy Cd Cl" appended to particle/forces.dat
     void OutputForces(int t, double U, double D);
+    // checkpoint of the device state written to `path` (ippi_save_state,
+    // through a temporary file renamed over it); false on error
+    bool SaveCheckpoint(const std::string& path);
+    // resume from a checkpoint file (ippi_load_state) into a mesh set up as
+    // the saving one was; returns the last step it holds, -1 on error
+    int LoadCheckpoint(const std::string& path);
+    // one JSON line appended to `path`: step, MLUPS and HBM GB/s of the
+    // steps since the previous line, FP64 mass, Cd / Cl of body 0 (U, D;
+    // null without markers), max |u|, and the learned tau's network /
+    // fallback node counts (ippi_diagnostics)
+    void LogMetrics(const std::string& path, int t, double mlups, double U, double D);
     ippi_lbm* Handle() { return h_; }
 
 private:

@@ -18,7 +18,7 @@ F64, F32, F16, BF16 = 0, 1, 2, 3
 BC_REF_NEE, BC_CHANNEL = 0, 1
 LES_NONE, LES_SMAGORINSKY, LES_LEARNED, LES_FIELD, LES_WALE, LES_CSM, LES_DYNAMIC = range(7)
 MLP_PARAMS, MLP_STATS, MLP_GRAD_BLOCKS = 1313, 25, 296
-ABI_VERSION = 2
+ABI_VERSION = 3
 DELTA_BILINEAR, DELTA_PESKIN4 = 0, 1
 (FIELD_F, FIELD_RHO, FIELD_UX, FIELD_UY, FIELD_TAU, FIELD_AVG_U, FIELD_AVG_V, FIELD_AVG_RHO,
  FIELD_FLAGS, FIELD_NNFLAG) = range(10)
@@ -30,7 +30,8 @@ EXPORTS = ("ippi_abi_version", "ippi_params_default", "ippi_create", "ippi_destr
            "ippi_filter_snapshot", "ippi_mlp_param_count", "ippi_mlp_scratch_floats", "ippi_mlp_grad",
            "ippi_mlp_adam", "ippi_mlp_forward", "ippi_set_tau_field", "ippi_load_tau_mlp_f32",
            "ippi_adjoint_forward", "ippi_adjoint_backward", "ippi_tau_scan", "ippi_tau_scan_state", "ippi_set_solid", "ippi_solid_force", "ippi_reequilibrate",
-           "ippi_set_wall_distance")
+           "ippi_set_wall_distance", "ippi_diagnostics", "ippi_state_bytes", "ippi_save_state",
+           "ippi_load_state")
 
 
 class Params(C.Structure):
@@ -99,6 +100,10 @@ def lib() -> C.CDLL:
         L.ippi_adjoint_backward.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
         L.ippi_reequilibrate.argtypes = [C.c_void_p, _dp, _dp, _dp]
         L.ippi_set_wall_distance.argtypes = [C.c_void_p, _dp]
+        L.ippi_diagnostics.argtypes = [C.c_void_p, _dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        L.ippi_state_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_size_t)]
+        L.ippi_save_state.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+        L.ippi_load_state.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_int)]
         L.ippi_set_solid.argtypes = [C.c_void_p, C.POINTER(C.c_uint8), C.c_size_t]
         L.ippi_solid_force.argtypes = [C.c_void_p, _dp]
         L.ippi_tau_scan.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), _dp, C.c_int, C.c_int,

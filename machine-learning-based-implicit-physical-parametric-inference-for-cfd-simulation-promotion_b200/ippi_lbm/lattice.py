@@ -2,6 +2,7 @@
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -172,6 +173,36 @@ class Lattice:
         """Wall distance per node [ny][nx] for the wall-damped closure."""
         d = _f64(dist, self.nx * self.ny)
         L.check(L.lib().ippi_set_wall_distance(self._h, _p(d)), self._h)
+
+    def diagnostics(self):
+        """dict(max_u, net_nodes, fallback_nodes) of the state after the last
+        step (ippi_diagnostics)."""
+        mu, net, fb = C.c_double(), C.c_longlong(), C.c_longlong()
+        L.check(L.lib().ippi_diagnostics(self._h, C.byref(mu), C.byref(net), C.byref(fb)), self._h)
+        return dict(max_u=mu.value, net_nodes=net.value, fallback_nodes=fb.value)
+
+    def save_state(self, path=None):
+        """Checkpoint of the evolving state (ippi_save_state) as bytes; also
+        written to `path` when given."""
+        n = C.c_size_t()
+        L.check(L.lib().ippi_state_bytes(self._h, C.byref(n)), self._h)
+        buf = np.empty(n.value, dtype=np.uint8)
+        L.check(L.lib().ippi_save_state(self._h, buf.ctypes.data_as(C.c_void_p), buf.nbytes), self._h)
+        if path is not None:
+            buf.tofile(path)
+        return buf.tobytes()
+
+    def load_state(self, data):
+        """Restore a checkpoint (bytes, or a file path); returns the user step
+        number of its last step (stepping resumes at that + 1)."""
+        if isinstance(data, (str, os.PathLike)):
+            buf = np.fromfile(data, dtype=np.uint8)
+        else:
+            buf = np.frombuffer(bytes(data), dtype=np.uint8).copy()
+        last = C.c_int()
+        L.check(L.lib().ippi_load_state(self._h, buf.ctypes.data_as(C.c_void_p), buf.nbytes, C.byref(last)),
+                self._h)
+        return last.value
 
     def set_solid(self, mask):
         """Solid nodes: mask[ny][nx] (nonzero = solid); None removes them."""

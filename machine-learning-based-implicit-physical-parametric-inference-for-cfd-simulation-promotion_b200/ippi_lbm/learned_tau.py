@@ -115,6 +115,26 @@ def samples_from_snapshot(snap, tau0, mask, min_strain=1e-7):
     return x[keep], (tau_t - tau0)[keep]
 
 
+def state_features(lat, tau0):
+    """The features the fused learned tau computes at every node of a
+    lattice's post-stream state (rho, |u|, Pi/|Pi| with Pi = sum e e (f -
+    feq), |S| = sqrt(2 S:S) with S = -3/(2 rho tau0) Pi), [ny * nx][6]."""
+    f = lat.download(L.FIELD_F)
+    rho, ux, uy = (lat.download(k) for k in (L.FIELD_RHO, L.FIELD_UX, L.FIELD_UY))
+    ex = np.array([0, 1, 0, -1, 0, 1, -1, -1, 1], dtype=np.float64)[:, None, None]
+    ey = np.array([0, 0, 1, 0, -1, 1, 1, -1, -1], dtype=np.float64)[:, None, None]
+    wk = np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4)[:, None, None]
+    eu = ex * ux + ey * uy
+    d = f - wk * rho * (1 + 3 * eu + 4.5 * eu * eu - 1.5 * (ux * ux + uy * uy))
+    pxx, pxy, pyy = (np.sum(c * d, 0) for c in (ex * ex, ex * ey, ey * ey))
+    c = -1.5 / (rho * tau0)
+    pn = np.sqrt(pxx * pxx + 2 * pxy * pxy + pyy * pyy)
+    inv = np.where(pn > 0, 1.0 / np.where(pn > 0, pn, 1.0), 0.0)
+    s = np.sqrt(2 * ((pxx * c) ** 2 + 2 * (pxy * c) ** 2 + (pyy * c) ** 2))
+    x = np.stack([rho, np.sqrt(ux * ux + uy * uy), pxx * inv, pxy * inv, pyy * inv, s], -1)
+    return x.reshape(-1, NIN)
+
+
 def cylinder_mask(nx, ny, cx, cy, d, margin=3):
     """Cells away from the lattice edges and outside the cylinder's IB band."""
     yy, xx = np.mgrid[0:ny, 0:nx]
@@ -332,18 +352,37 @@ def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=
 # end-to-end training through the solver (adjoint)
 # ---------------------------------------------------------------------------
 def train_through_solver(net, sc, cd_ref, iters=8, nsteps=4000, ckpt=64, spinup=12000, lr=2e-3,
-                         device=0, log=None):
+                         device=0, log=None, widen=False):
     """Fine-tune the network so that the coarse lattice's mean drag over an
     nsteps window (after `spinup` steps) matches cd_ref.  Loss
     ((<Cd> - cd_ref) / cd_ref)^2; its gradient with respect to the FP32
     weights comes from the adjoint (NetworkRollout), the update from the
-    library's Adam kernel.  Returns (net with new weights, history)."""
+    library's Adam kernel.  widen: first extend the network's training range
+    to the features the coarse lattice itself visits after the spin-up (the
+    solver's states become training data too), so that no node of the
+    training window falls back to Smagorinsky, where the weights get no
+    gradient.  Returns (net with new weights and range, history)."""
     import torch
 
     from .autograd import NetworkRollout, Rollout
     from .lattice import Lattice
 
     params = dict(sc["params"], les_model=L.LES_LEARNED)
+    lo, hi = net.lo.copy(), net.hi.copy()
+    if widen:
+        probe = Lattice(sc["nx"], sc["ny"], device=device, **params)
+        probe.set_markers(sc["markers"], ds=sc["ds"])
+        probe.init_macros(*sc["init"])
+        probe.load_tau_mlp_f32(net.w.astype(np.float32), net.stats())
+        probe.step(spinup, 1)
+        x = state_features(probe, params["tau0"])
+        probe.close()
+        span = x.max(0) - x.min(0)
+        lo = np.minimum(lo, x.min(0) - 0.25 * span).astype(np.float32)
+        hi = np.maximum(hi, x.max(0) + 0.25 * span).astype(np.float32)
+        if log:
+            log(f"training range widened to the solver's features: lo {lo} hi {hi}")
+    net = TauNet(net.w, net.mean, net.std, lo, hi, net.out_scale)
     lat = Lattice(sc["nx"], sc["ny"], device=device, **params)
     lat.set_markers(sc["markers"], ds=sc["ds"])
     stats = net.stats()

@@ -24,7 +24,7 @@ def test_library_exports_every_declared_symbol():
     for s in syms:
         assert hasattr(L, s), s
     assert set(_lib.EXPORTS) <= set(syms)
-    assert L.ippi_abi_version() == 2
+    assert L.ippi_abi_version() == 3
 
 
 def test_params_default_is_reference_main():

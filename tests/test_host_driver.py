@@ -140,3 +140,39 @@ def test_driver_solid_cylinder_cd_and_cp(tmp_path):
     assert front[2] > 0.5  # stagnation side
     assert cp[:, 2].min() < 0  # suction on the flanks
     g.close()
+
+
+@pytest.mark.gpu
+def test_driver_checkpoint_resume_and_metrics_log(tmp_path):
+    """--checkpoint at the save points, --resume from the one at step 30:
+    the resumed run writes the same fields and forces as the uninterrupted
+    one; --metrics writes one JSON line per --print step."""
+    import json
+    import shutil
+
+    common = ["--scene", "channel", "--nx", "200", "--ny", "64", "--u", "0.05", "--re", "100",
+              "--cs", "0.1", "--cylinder", "50.3", "32.1", "12", "--steps", "60", "--save", "30",
+              "--avg", "40", "--print", "10"]
+    a, b = tmp_path / "a", tmp_path / "b"
+    a.mkdir()
+    b.mkdir()
+    run_main(common + ["--checkpoint", "state30.ippi", "--steps", "30", "--metrics", "m.jsonl"], cwd=a)
+    shutil.copy(a / "state30.ippi", b / "state30.ippi")
+    run_main(common + ["--checkpoint", "state.ippi"], cwd=a)
+    out = run_main(common + ["--resume", "state30.ippi", "--checkpoint", "state.ippi"], cwd=b)
+    assert "Resumed at step 31" in out
+    fa = np.loadtxt(a / "particle" / "forces.dat")
+    fb = np.loadtxt(b / "particle" / "forces.dat")
+    assert fa.shape == (90, 5) and fb.shape == (30, 5)  # run a wrote 30 + 60 lines
+    np.testing.assert_array_equal(fa[-30:], fb)
+    np.testing.assert_array_equal(read_tecplot(a / "fluid" / "fluid_Merged_60.dat"),
+                                  read_tecplot(b / "fluid" / "fluid_Merged_60.dat"))
+    assert (a / "state.ippi").read_bytes() == (b / "state.ippi").read_bytes()
+    rows = [json.loads(ln) for ln in (a / "m.jsonl").read_text().splitlines()]
+    assert [r["step"] for r in rows] == [10, 20, 30]
+    for r in rows:
+        assert r["mlups"] > 0 and r["hbm_gbs"] == pytest.approx(r["mlups"] * 0.144)
+        # FP64 mass of the open channel (Zou-He inflow, NEE outflow): near rho0 per node
+        assert abs(r["mass"] / (200 * 64) - 1) < 0.01 and 0.04 < r["max_u"] < 0.2
+        assert math.isfinite(r["cd"]) and math.isfinite(r["cl"])
+        assert r["tau_net_nodes"] == 0 and r["tau_fallback_nodes"] == 0
