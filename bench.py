@@ -395,7 +395,7 @@ def run_learned(a):
     rank, local, world = env_rank()
     torch.cuda.set_device(local)
     r = lt.experiment(fine_steps=a.learned_steps, avg_steps=a.learned_steps * 2 // 5, device=local,
-                      finetune_iters=a.learned_finetune)
+                      finetune_iters=a.learned_finetune, calibrate=not a.learned_no_calibration)
     r.pop("net")
     if rank != 0:
         return
@@ -408,13 +408,17 @@ def run_learned(a):
                    "snapshots": 200, "filter": 4},
         "cd": {"fine": r["fine"]["cd"], "coarse_plain": r["coarse_plain"]["cd"],
                "coarse_learned": r["coarse_learned"]["cd"],
+               "coarse_learned_a_priori": r["coarse_learned_a_priori"]["cd"],
                "rel_err_plain": r["coarse_plain"]["cd_rel_err"],
-               "rel_err_learned": r["coarse_learned"]["cd_rel_err"]},
+               "rel_err_learned": r["coarse_learned"]["cd_rel_err"],
+               "rel_err_learned_a_priori": r["coarse_learned_a_priori"]["cd_rel_err"]},
         "st": {"fine": r["fine"]["st"], "coarse_plain": r["coarse_plain"]["st"],
                "coarse_learned": r["coarse_learned"]["st"]},
         "wall_s": {"fine": r["fine"]["wall_s"], "coarse_plain": r["coarse_plain"]["wall_s"],
                    "coarse_learned": r["coarse_learned"]["wall_s"]},
         "training": r["training"],
+        "calibration": None if r["calibration"] is None else {
+            k: v for k, v in r["calibration"].items() if k != "history"},
         "through_solver": None if r["coarse_learned_through_solver"] is None else {
             k: v for k, v in r["coarse_learned_through_solver"].items() if k != "history"},
     }
@@ -528,6 +532,8 @@ def main():
     ap.add_argument("--learned-steps", type=int, default=160000)
     ap.add_argument("--learned-finetune", type=int, default=0,
                     help="iterations of training through the solver (adjoint) after the a-priori fit")
+    ap.add_argument("--learned-no-calibration", action="store_true",
+                    help="skip fitting the network's output scale to the fine drag (forward runs)")
     ap.add_argument("--adjoint", action="store_true",
                     help="adjoint forward+backward throughput and gradient check instead of the MLUPS line")
     ap.add_argument("--adjoint-steps", type=int, default=4000)

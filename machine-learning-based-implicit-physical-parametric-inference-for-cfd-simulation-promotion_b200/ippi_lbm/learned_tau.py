@@ -283,12 +283,16 @@ def strouhal(cl, d, u, pad=16):
 # ---------------------------------------------------------------------------
 def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=160000,
                avg_steps=64000, n_snap=200, max_samples=2_000_000, epochs=30, seed=0, device=0,
-               finetune_iters=0, finetune_lr=2e-3, log=None):
+               finetune_iters=0, finetune_lr=2e-3, calibrate=True, log=None):
     """Fine lattice (plain Smagorinsky MRT, FP32) -> `n_snap` filtered
     snapshots over its averaging window -> training -> the coarse lattice
     (nx/factor x ny/factor, same Re and Mach) with plain Smagorinsky and with
-    the learned tau.  Mean Cd / Cl and St over the same physical window, and
-    the device wall time of each run."""
+    the learned tau.  calibrate: the network's output scale is then fitted
+    to the fine run's drag (calibrate_scale) on the coarse scene started
+    from another noise seed (seed + 1) than the evaluation run; finetune_iters
+    adjoint iterations (train_through_solver) may follow.  Mean Cd / Cl and
+    St over the same physical window, and the device wall time of each
+    run."""
     from . import scenes
 
     say = log or (lambda s: None)
@@ -317,7 +321,18 @@ def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=
     csteps, cfirst = fine_steps // factor, (fine_steps - avg_steps) // factor + 1
     rp = run_cylinder(coarse, csteps, cfirst, device=device)
     rl = run_cylinder(coarse, csteps, cfirst, net=net, device=device)
-    say(f"coarse plain: Cd {rp['cd']:.5f}; learned: Cd {rl['cd']:.5f}")
+    say(f"coarse plain: Cd {rp['cd']:.5f}; learned (a priori): Cd {rl['cd']:.5f}")
+    a_priori, cal = rl, None
+    if calibrate:
+        t1 = time.perf_counter()
+        other = scenes.cylinder_channel(mx, my, dc, cx / factor, cy / factor, u, re, seed=seed + 1)
+        net_c, cal_hist = calibrate_scale(net, other, rf["cd"], csteps, cfirst, device=device, log=log)
+        cal_s = time.perf_counter() - t1
+        cal = dict(scale=net_c.out_scale / net.out_scale, runs=len(cal_hist), seconds=cal_s,
+                   history=[dict(scale=a, cd=b) for a, b in cal_hist])
+        net = net_c
+        rl = run_cylinder(coarse, csteps, cfirst, net=net, device=device)
+        say(f"coarse learned, output scale x{cal['scale']:.4g}: Cd {rl['cd']:.5f}")
     tuned = None
     if finetune_iters:
         t1 = time.perf_counter()
@@ -341,11 +356,80 @@ def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=
                           cd_rel_err=err(rp)),
         coarse_learned=dict(nx=mx, ny=my, steps=csteps, cd=rl["cd"], st=rl["st"], wall_s=rl["wall_s"],
                             cd_rel_err=err(rl)),
+        coarse_learned_a_priori=dict(cd=a_priori["cd"], st=a_priori["st"], wall_s=a_priori["wall_s"],
+                                     cd_rel_err=err(a_priori)),
+        calibration=cal,
         training=dict(samples=int(x.shape[0]), epochs=epochs, loss_first=hist[0], loss_last=hist[-1],
                       seconds=train_s),
         coarse_learned_through_solver=tuned,
         speedup_vs_fine=rf["wall_s"] / rl["wall_s"],
         net=net)
+
+
+# ---------------------------------------------------------------------------
+# a posteriori calibration of the output scale (forward runs only)
+# ---------------------------------------------------------------------------
+def calibrate_scale(net, sc, cd_ref, steps, avg_from, grid=(1, 4, 16, 64, 256, 1024), iters=6,
+                    device=0, log=None):
+    """Fit the network's output scale so that the coarse lattice's mean drag
+    over steps avg_from..steps comes closest to cd_ref, by forward runs of
+    the scene `sc`: the scales of `grid` first; then, where two neighbouring
+    grid points bracket cd_ref, the Illinois variant of regula falsi on
+    log(scale) between them, else a golden-section search of |Cd - cd_ref|
+    between the best grid point's neighbours (`iters` more runs either way).
+    Mean drag over a long window is a smooth function of the eddy-viscosity
+    level even where the wake is chaotic, which its gradient over a short
+    window is not.  Returns (net with the best scale, [(scale, Cd), ...] in
+    run order)."""
+    hist = []
+
+    def f(x):
+        n = TauNet(net.w, net.mean, net.std, net.lo, net.hi, net.out_scale * math.exp(x))
+        cd = run_cylinder(sc, steps, avg_from, net=n, device=device)["cd"]
+        hist.append((math.exp(x), cd))
+        if log:
+            log(f"calibration: scale {math.exp(x):.4g} -> Cd {cd:.5f}")
+        return cd - cd_ref
+
+    xs = [math.log(g) for g in grid]
+    fs = [f(x) for x in xs]
+    brackets = [i for i in range(len(xs) - 1) if fs[i] * fs[i + 1] < 0]
+    if brackets:
+        i = min(brackets, key=lambda k: min(abs(fs[k]), abs(fs[k + 1])))
+        a, fa, b, fb = xs[i], fs[i], xs[i + 1], fs[i + 1]
+        side = 0
+        for _ in range(iters):
+            c = (a * fb - b * fa) / (fb - fa)
+            fc = f(c)
+            if fc * fb > 0:
+                b, fb = c, fc
+                if side == -1:
+                    fa /= 2
+                side = -1
+            elif fa * fc > 0:
+                a, fa = c, fc
+                if side == 1:
+                    fb /= 2
+                side = 1
+            else:
+                break
+    else:
+        k = min(range(len(xs)), key=lambda i: abs(fs[i]))
+        a, b = xs[max(k - 1, 0)], xs[min(k + 1, len(xs) - 1)]
+        r = (math.sqrt(5.0) - 1.0) / 2.0
+        c, d = b - r * (b - a), a + r * (b - a)
+        mc, md = abs(f(c)), abs(f(d))
+        for _ in range(iters - 2):
+            if mc < md:
+                b, d, md = d, c, mc
+                c = b - r * (b - a)
+                mc = abs(f(c))
+            else:
+                a, c, mc = c, d, md
+                d = a + r * (b - a)
+                md = abs(f(d))
+    best = min(hist, key=lambda h: abs(h[1] - cd_ref))
+    return TauNet(net.w, net.mean, net.std, net.lo, net.hi, net.out_scale * best[0]), hist
 
 
 # ---------------------------------------------------------------------------

@@ -54,3 +54,22 @@ def test_bench_modes_resolve_their_drivers():
     for k in ("fine_steps", "avg_steps", "device", "finetune_iters"):
         assert k in sig.parameters, k
     assert "iters" in inspect.signature(lt.train_through_solver).parameters
+
+
+def test_output_scale_calibration_finds_the_closest_drag(monkeypatch):
+    """calibrate_scale on a synthetic drag curve Cd(scale) (a bump in
+    log(scale), the shape the coarse channel shows): the target inside the
+    curve's range is met closely, one above its peak gets the peak."""
+    from ippi_lbm import learned_tau as lt
+
+    def fake_run(sc, steps, avg_from, net=None, device=0):
+        return dict(cd=0.96 + 0.47 * math.exp(-((math.log(net.out_scale) - math.log(300)) / 2.5) ** 2))
+
+    monkeypatch.setattr(lt, "run_cylinder", fake_run)
+    net = lt.TauNet(np.zeros(1313), np.zeros(6), np.ones(6), np.zeros(6), np.ones(6), 2.0)
+    best, hist = lt.calibrate_scale(net, None, 1.63, 10, 1)
+    assert len(hist) <= 6 + 6 and best.w is not None
+    assert abs(best.out_scale - 300) < 30  # the peak, 1.43
+    best, hist = lt.calibrate_scale(net, None, 1.2, 10, 1)
+    assert min(abs(c - 1.2) for _, c in hist) < 0.002
+    assert fake_run(None, 0, 0, best)["cd"] == pytest.approx(1.2, abs=0.002)
