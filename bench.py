@@ -353,6 +353,38 @@ def run_ncu_case(a):
     print(json.dumps({"ncu_case": WORKLOAD, "steps": a.steps}))
 
 
+def run_learned_ncu_case(a):
+    """The command profiled by ncu for the learned-tau step: the coarse
+    1024 x 256 channel of the learned comparison (MRT, FP32, learned tau with
+    a seeded Xavier network whose range covers every node), --steps steps
+    after 200 warm-up steps, timed on the host around the synchronising
+    ippi_step call."""
+    import numpy as np
+    import torch
+
+    import ippi_lbm as ip
+    from ippi_lbm import learned_tau as lt
+    from ippi_lbm import scenes
+
+    sc = scenes.cylinder_channel(1024, 256, 32, 256, 128, 0.04, 3900, collision=ip.MRT)
+    lat = ip.Lattice(1024, 256, **dict(sc["params"], les_model=ip.LES_LEARNED, storage=ip.F32))
+    lat.init_macros(*sc["init"])
+    lat.set_markers(sc["markers"], ds=sc["ds"])
+    stats = np.concatenate([[1.0, 0.04, 0, 0, 0, 1e-3], [2e-3, 0.02, 0.5, 0.5, 0.5, 1e-3],
+                            [-1e6] * 6, [1e6] * 6, [1e-3]]).astype(np.float32)
+    bits, _ = lt.bf16_bits(lt.xavier(0))
+    lat.load_tau_mlp(bits, stats)
+    lat.step(200, 1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lat.step(a.steps, 201)  # returns after the handle's stream has drained
+    us = (time.perf_counter() - t0) * 1e6 / a.steps
+    d = lat.diagnostics()
+    lat.close()
+    print(json.dumps({"learned_ncu_case": "channel_cylinder_1024x256_mrt_learned_tau", "steps": a.steps,
+                      "us_per_step": round(us, 2), "fallback_nodes": d["fallback_nodes"]}))
+
+
 def run_adjoint_ncu_case(a):
     """The command profiled by ncu for the adjoint: the --adjoint lattice
     (learned tau, seeded Xavier network), an --adjoint-steps rollout
@@ -543,6 +575,8 @@ def main():
                     help="precision studies of configs 2 and 3 instead of the MLUPS line")
     ap.add_argument("--validate-steps2", type=int, default=160000)
     ap.add_argument("--validate-steps3", type=int, default=20000)
+    ap.add_argument("--learned-ncu-case", action="store_true",
+                    help="learned-tau steps of the coarse channel for an ncu capture")
     ap.add_argument("--adjoint-ncu-case", action="store_true",
                     help="short adjoint rollout and backward sweep for an ncu capture")
     ap.add_argument("--ncu-case", action="store_true",
@@ -552,6 +586,8 @@ def main():
         run_ncu_case(a)
     elif a.adjoint_ncu_case:
         run_adjoint_ncu_case(a)
+    elif a.learned_ncu_case:
+        run_learned_ncu_case(a)
     elif a.learned:
         run_learned(a)
     elif a.adjoint:

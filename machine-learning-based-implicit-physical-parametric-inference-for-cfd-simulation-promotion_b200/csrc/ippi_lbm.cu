@@ -13,6 +13,7 @@
 //   side_f    [nslots][9], side_m [2][nslots][3] (compute type)
 //   avg       [3][ny][nx] running means (compute type)
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -20,6 +21,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -100,6 +102,7 @@ struct ippi_lbm {
     long long hist_written = 0;
     // learned tau: parameters (FP32 values of the BF16 weights) + statistics
     float* mlp_dev = nullptr;
+    unsigned long long mlp_version = 0;  // unique per network load (g_mlp_serial)
     double* tau_field = nullptr;  // IPPI_LES_FIELD: [ny][nx]
     unsigned long long* ib_bar = nullptr;  // arrival counter of the one-launch step's IB blocks
     void* mac = nullptr;          // IPPI_LES_WALE / CSM: [2][ny][nx] compute type, velocities
@@ -237,6 +240,64 @@ void adjoint_free(ippi_lbm* h)
         v->clear();
     }
     h->adj.ready = false;
+}
+
+// The fused learned-tau kernels read the network from their storage module's
+// constant memory (c_mlp), which holds one network per device at a time.  The
+// calls that launch those kernels hold the device's lock (MlpLock), copy the
+// handle's network there on the handle's stream when another one is loaded
+// (mlp_const_ready), and drain the stream before they let go of the lock, so
+// learned handles on one device take turns even across host threads.
+constexpr int kMaxDevices = 64;
+std::recursive_mutex g_mlp_mu[kMaxDevices];
+unsigned long long g_mlp_loaded[kMaxDevices][4] = {};  // network version in each storage module
+std::atomic<unsigned long long> g_mlp_serial{0};
+
+class MlpLock {
+public:
+    explicit MlpLock(ippi_lbm* h)
+    {
+        if (h && h->p.les_model == IPPI_LES_LEARNED && h->mlp_dev && h->p.device >= 0 &&
+            h->p.device < kMaxDevices) {
+            h_ = h;
+            g_mlp_mu[h->p.device].lock();
+        }
+    }
+    ~MlpLock()
+    {
+        if (!h_) return;
+        cudaStreamSynchronize(h_->st);
+        g_mlp_mu[h_->p.device].unlock();
+    }
+    MlpLock(const MlpLock&) = delete;
+    MlpLock& operator=(const MlpLock&) = delete;
+
+private:
+    ippi_lbm* h_ = nullptr;
+};
+
+// with the device's lock held and the device current: the handle's network
+// into the constant memory of its storage module, if another one is there
+int mlp_const_ready(ippi_lbm* h)
+{
+    if (h->p.les_model != IPPI_LES_LEARNED || !h->mlp_dev) return IPPI_OK;
+    if (h->p.device < 0 || h->p.device >= kMaxDevices)
+        return fail(h, IPPI_ERR_ARG, "learned tau on device %d (at most %d devices)", h->p.device, kMaxDevices);
+    unsigned long long& loaded = g_mlp_loaded[h->p.device][h->S];
+    if (loaded == h->mlp_version) return IPPI_OK;
+    void* dst = nullptr;
+    cudaError_t e;
+    switch (h->S) {
+    case ST_F64: e = mlp_const_addr_f64(&dst); break;
+    case ST_F32: e = mlp_const_addr_f32(&dst); break;
+    case ST_F16: e = mlp_const_addr_f16(&dst); break;
+    default: e = mlp_const_addr_bf16(&dst); break;
+    }
+    CK(h, e);
+    CK(h, cudaMemcpyAsync(dst, h->mlp_dev, (size_t)(kMlpParams + kMlpStats) * sizeof(float),
+                          cudaMemcpyDeviceToDevice, h->st));
+    loaded = h->mlp_version;
+    return IPPI_OK;
 }
 
 cudaError_t launch(const LaunchSet& L, int S)
@@ -771,6 +832,8 @@ int tau_ready(ippi_lbm* h)
 int run_init(ippi_lbm* h)
 {
     if (int rc = tau_ready(h)) return rc;
+    MlpLock lock(h);
+    if (int rc = mlp_const_ready(h)) return rc;
     std::memset(h->ctr_h, 0, sizeof(Ctr));
     CK(h, cudaMemcpyAsync(h->ctr, h->ctr_h, sizeof(Ctr), cudaMemcpyHostToDevice, h->st));
     CK(h, cudaStreamSynchronize(h->st));
@@ -816,6 +879,8 @@ int materialize(ippi_lbm* h)
 {
     if (h->dl_valid) return IPPI_OK;
     if (int rc = tau_ready(h)) return rc;
+    MlpLock lock(h);
+    if (int rc = mlp_const_ready(h)) return rc;
     const size_t nn = (size_t)h->p.nx * h->p.ny;
     if (!h->dl) CK(h, dalloc(&h->dl, 14 * nn * sizeof(double)));
     CK(h, cudaMemsetAsync(h->dl + 12 * nn, 0, nn * sizeof(double), h->st));  // net-flag plane
@@ -1206,6 +1271,8 @@ int ippi_step(ippi_lbm* h, int nsteps, int t0)
     if (nsteps < 0) return fail(h, IPPI_ERR_ARG, "negative step count");
     if (nsteps == 0) return IPPI_OK;
     CK(h, cudaSetDevice(h->p.device));
+    MlpLock lock(h);
+    if (int rc = mlp_const_ready(h)) return rc;
     if (h->pending_init) {
         int rc = run_init(h);
         if (rc) return rc;
@@ -1248,6 +1315,8 @@ int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk, double*
     if (int rc = tau_ready(h)) return rc;
     if (nsteps <= 0) return fail(h, IPPI_ERR_ARG, "nsteps must be positive");
     CK(h, cudaSetDevice(h->p.device));
+    MlpLock lock(h);
+    if (int rc = mlp_const_ready(h)) return rc;
     if (h->pending_init) {
         int rc = run_init(h);
         if (rc) return rc;
@@ -1550,6 +1619,7 @@ int ippi_load_tau_mlp(ippi_lbm* h, const uint16_t* w_bf16, size_t n, const float
     CK(h, cudaStreamSynchronize(h->st));
     if (!h->mlp_dev) CK(h, dalloc(&h->mlp_dev, blob.size() * sizeof(float)));
     CK(h, cudaMemcpy(h->mlp_dev, blob.data(), blob.size() * sizeof(float), cudaMemcpyHostToDevice));
+    h->mlp_version = ++g_mlp_serial;
     // step graphs captured before the first load hold a null network pointer
     drop_graphs(h);
     h->dl_valid = false;
@@ -1607,6 +1677,7 @@ int ippi_load_tau_mlp_f32(ippi_lbm* h, const float* w, size_t n, const float* st
     for (size_t i = 0; i < n; i++)
         if (!std::isfinite(w[i])) return fail(h, IPPI_ERR_ARG, "tau network weight %zu is not finite", i);
     CK(h, cudaMemcpy(h->mlp_dev, w, n * sizeof(float), cudaMemcpyHostToDevice));
+    h->mlp_version = ++g_mlp_serial;
     return IPPI_OK;
 }
 
@@ -1624,6 +1695,8 @@ int ippi_adjoint_forward(ippi_lbm* h, int nsteps, int t0, int ckpt_every)
         return fail(h, IPPI_ERR_ARG, "rollout longer than the force history (%d steps)", h->hist_cap);
     if (int rc = tau_ready(h)) return rc;
     CK(h, cudaSetDevice(h->p.device));
+    MlpLock lock(h);
+    if (int rc = mlp_const_ready(h)) return rc;
     adjoint_free(h);
     if (h->pending_init) {
         int rc = run_init(h);
@@ -1663,6 +1736,8 @@ int ippi_adjoint_backward(ippi_lbm* h, const double* dl_dforce, const double* dl
     if (grad_mlp && h->p.les_model != IPPI_LES_LEARNED)
         return fail(h, IPPI_ERR_STATE, "grad_mlp needs the learned model (IPPI_LES_LEARNED)");
     CK(h, cudaSetDevice(h->p.device));
+    MlpLock lock(h);
+    if (int rc = mlp_const_ready(h)) return rc;
     const int nx = h->p.nx, ny = h->p.ny, nsteps = h->adj.nsteps, K = h->adj.K;
     const size_t nn = (size_t)nx * ny;
     const size_t fbytes = (size_t)9 * h->plane * h->tsize;

@@ -3,4 +3,6 @@
 
 namespace ippi {
 cudaError_t launch_bf16(const LaunchSet& L) { return launch_store<ST_BF16>(L); }
+// device address of this module's copy of the fused network (c_mlp)
+cudaError_t mlp_const_addr_bf16(void** p) { return cudaGetSymbolAddress(p, c_mlp); }
 }  // namespace ippi

@@ -3,4 +3,6 @@
 
 namespace ippi {
 cudaError_t launch_f32(const LaunchSet& L) { return launch_store<ST_F32>(L); }
+// device address of this module's copy of the fused network (c_mlp)
+cudaError_t mlp_const_addr_f32(void** p) { return cudaGetSymbolAddress(p, c_mlp); }
 }  // namespace ippi

@@ -43,4 +43,11 @@ cudaError_t launch_f32(const LaunchSet& L);
 cudaError_t launch_f16(const LaunchSet& L);
 cudaError_t launch_bf16(const LaunchSet& L);
 
+// device address (current device) of each storage module's constant-memory
+// copy of the fused learned-tau network (c_mlp in lbm_common.cuh)
+cudaError_t mlp_const_addr_f64(void** p);
+cudaError_t mlp_const_addr_f32(void** p);
+cudaError_t mlp_const_addr_f16(void** p);
+cudaError_t mlp_const_addr_bf16(void** p);
+
 }  // namespace ippi

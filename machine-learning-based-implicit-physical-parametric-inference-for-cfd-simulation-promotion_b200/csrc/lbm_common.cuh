@@ -409,49 +409,52 @@ __device__ __forceinline__ void mlp_features(C pxx, C pxy, C pyy, C rho, C ux, C
     x[5] = sqrt(C(2) * (sxx * sxx + C(2) * sxy * sxy + syy * syy));
 }
 
+// The network of the fused step kernels, in constant memory (one copy per
+// compiled module; the host copies a handle's parameter block here on the
+// handle's stream before its step kernels run).  The layer loops below are
+// fully unrolled, so each weight is a constant-bank operand of its FMA: no
+// load instruction and no wait on one.
+static __constant__ float c_mlp[kMlpParams + kMlpStats];
+
 // network output softplus(z) for standardised inputs x
 template <typename C>
-__device__ __forceinline__ C mlp_forward(const float* __restrict__ w, const C* x)
+__device__ __forceinline__ C mlp_forward(const C* x)
 {
     C h1[kMlpHid];
 #pragma unroll
     for (int j = 0; j < kMlpHid; j++) {
-        C a = C(__ldg(w + kMlpB1 + j));
+        C a = C(c_mlp[kMlpB1 + j]);
 #pragma unroll
-        for (int i = 0; i < kMlpIn; i++) a += C(__ldg(w + kMlpW1 + j * kMlpIn + i)) * x[i];
+        for (int i = 0; i < kMlpIn; i++) a += C(c_mlp[kMlpW1 + j * kMlpIn + i]) * x[i];
         h1[j] = mlp_tanh(a);
     }
-    C z = C(__ldg(w + kMlpB3));
-#pragma unroll 4
-    for (int j = 0; j < kMlpHid; j++) {
-        C a = C(__ldg(w + kMlpB2 + j));
-        const float4* row = reinterpret_cast<const float4*>(w + kMlpW2 + j * kMlpHid);
+    C z = C(c_mlp[kMlpB3]);
 #pragma unroll
-        for (int i = 0; i < kMlpHid / 4; i++) {
-            const float4 q = __ldg(row + i);
-            a += C(q.x) * h1[4 * i] + C(q.y) * h1[4 * i + 1] + C(q.z) * h1[4 * i + 2] +
-                 C(q.w) * h1[4 * i + 3];
-        }
-        z += C(__ldg(w + kMlpW3 + j)) * mlp_tanh(a);
+    for (int j = 0; j < kMlpHid; j++) {
+        C a = C(c_mlp[kMlpB2 + j]);
+#pragma unroll
+        for (int i = 0; i < kMlpHid; i++) a += C(c_mlp[kMlpW2 + j * kMlpHid + i]) * h1[i];
+        z += C(c_mlp[kMlpW3 + j]) * mlp_tanh(a);
     }
     return softplus(z);
 }
 
+// relaxation time from the network (constant memory), Smagorinsky where a
+// feature leaves the training range
 template <typename C>
-__device__ __forceinline__ C learned_tau(C pxx, C pxy, C pyy, C rho, C ux, C uy, C tau0, C cs,
-                                         const float* __restrict__ w)
+__device__ __forceinline__ C learned_tau(C pxx, C pxy, C pyy, C rho, C ux, C uy, C tau0, C cs)
 {
-    const float* st = w + kMlpParams;
+    constexpr int st = kMlpParams;
     C x[kMlpIn];
     mlp_features<C>(pxx, pxy, pyy, rho, ux, uy, tau0, x);
     bool in = true;
 #pragma unroll
     for (int i = 0; i < kMlpIn; i++) {
-        in = in && x[i] >= C(__ldg(st + 2 * kMlpIn + i)) && x[i] <= C(__ldg(st + 3 * kMlpIn + i));
-        x[i] = (x[i] - C(__ldg(st + i))) / C(__ldg(st + kMlpIn + i));
+        in = in && x[i] >= C(c_mlp[st + 2 * kMlpIn + i]) && x[i] <= C(c_mlp[st + 3 * kMlpIn + i]);
+        x[i] = (x[i] - C(c_mlp[st + i])) / C(c_mlp[st + kMlpIn + i]);
     }
     if (!in) return les_tau<C>(pxx, pxy, pyy, rho, tau0, cs);
-    return tau0 + C(__ldg(st + 4 * kMlpIn)) * mlp_forward<C>(w, x);
+    return tau0 + C(c_mlp[st + 4 * kMlpIn]) * mlp_forward<C>(x);
 }
 
 // The learned tau on dual numbers (adjoint): features carry their partial
@@ -505,30 +508,28 @@ __device__ Dual<N> learned_tau(Dual<N> pxx, Dual<N> pxy, Dual<N> pyy, Dual<N> rh
 // range (the network sets tau there, Smagorinsky outside it): the same
 // features and comparisons as learned_tau
 template <typename C>
-__device__ __forceinline__ bool learned_in_range(const C* f, C rho, C ux, C uy, C rb, C tau0,
-                                                 const float* __restrict__ w)
+__device__ __forceinline__ bool learned_in_range(const C* f, C rho, C ux, C uy, C rb, C tau0)
 {
+    constexpr int st = kMlpParams;
     C pxx, pxy, pyy, x[kMlpIn];
     pi_neq<C>(f, rho, ux, uy, rb, pxx, pxy, pyy);
     mlp_features<C>(pxx, pxy, pyy, rho, ux, uy, tau0, x);
-    const float* st = w + kMlpParams;
     bool in = true;
 #pragma unroll
     for (int i = 0; i < kMlpIn; i++)
-        in = in && x[i] >= C(__ldg(st + 2 * kMlpIn + i)) && x[i] <= C(__ldg(st + 3 * kMlpIn + i));
+        in = in && x[i] >= C(c_mlp[st + 2 * kMlpIn + i]) && x[i] <= C(c_mlp[st + 3 * kMlpIn + i]);
     return in;
 }
 
 // relaxation time of a node's next collision: tau0, Smagorinsky, or (LRN)
 // the learned model with its Smagorinsky fallback
 template <typename C, bool LRN = false>
-__device__ __forceinline__ C node_tau(const C* f, C rho, C ux, C uy, C rb, int les, C tau0, C cs,
-                                      const float* mlp = nullptr)
+__device__ __forceinline__ C node_tau(const C* f, C rho, C ux, C uy, C rb, int les, C tau0, C cs)
 {
     if (!LRN && !les) return tau0;
     C pxx, pxy, pyy;
     pi_neq<C>(f, rho, ux, uy, rb, pxx, pxy, pyy);
-    if (LRN) return learned_tau(pxx, pxy, pyy, rho, ux, uy, tau0, cs, mlp);
+    if constexpr (LRN) return learned_tau(pxx, pxy, pyy, rho, ux, uy, tau0, cs);
     return les_tau<C>(pxx, pxy, pyy, rho, tau0, cs);
 }
 

@@ -528,12 +528,12 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
                 const C tau = XT            ? ext_tau<S>(a, x, y, f, rho, ux, uy, rbs)
                               : a.les == 3 ? C(a.tau_field[node])
                                            : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
-                                                              prm<C>(a.cs, a.f_cs), a.mlp);
+                                                              prm<C>(a.cs, a.f_cs));
                 if (a.mode >= MODE_MAT) {
                     a.dl_tau[node] = double(tau);
                     if (LRN)  // 1 where the network set tau, 0 where Smagorinsky did
                         a.dl_m[3ll * a.nx * a.ny + node] =
-                            learned_in_range<C>(f, rho, ux, uy, rbs, prm<C>(a.tau0, a.f_tau0), a.mlp) ? 1.0 : 0.0;
+                            learned_in_range<C>(f, rho, ux, uy, rbs, prm<C>(a.tau0, a.f_tau0)) ? 1.0 : 0.0;
                 } else {
                     collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
 #pragma unroll
@@ -596,7 +596,7 @@ __device__ __forceinline__ void bulk_tile(const StepArgs& a, int bx, int by, int
     const bool bad = !(rho <= C(10) && rho >= C(0));
     const C tau = XT ? ext_tau<S>(a, x, y, f, rho, ux, uy, rbs)
                      : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
-                                        prm<C>(a.cs, a.f_cs), a.mlp);
+                                        prm<C>(a.cs, a.f_cs));
     if (AV) {
         // Mesh::ComputeAvgVelocity (mesh.cpp:1969-1971) of the post-stream
         // moments, which the collision below overwrites in f only
@@ -982,12 +982,12 @@ __device__ __forceinline__ void ib_collide_item(const IbArgs& ia, int n)
     const C tau = XT            ? ext_tau<S>(a, xy.x, xy.y, f, rho, ux, uy, rbs)
                   : a.les == 3 ? C(a.tau_field[(long long)xy.y * a.nx + xy.x])
                                : node_tau<C, LRN>(f, rho, ux, uy, rbs, a.les, prm<C>(a.tau0, a.f_tau0),
-                                                  prm<C>(a.cs, a.f_cs), a.mlp);
+                                                  prm<C>(a.cs, a.f_cs));
     if (a.mode >= MODE_MAT) {
         a.dl_tau[(long long)xy.y * a.nx + xy.x] = double(tau);
         if (LRN)
             a.dl_m[3ll * a.nx * a.ny + (long long)xy.y * a.nx + xy.x] =
-                learned_in_range<C>(f, rho, ux, uy, rbs, prm<C>(a.tau0, a.f_tau0), a.mlp) ? 1.0 : 0.0;
+                learned_in_range<C>(f, rho, ux, uy, rbs, prm<C>(a.tau0, a.f_tau0)) ? 1.0 : 0.0;
     } else {
         collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
         add_force<C, CO>(f, ux, uy, C(ia.fx[n]), C(ia.fy[n]), prm<C>(a.tau0, a.f_tau0), tau);
