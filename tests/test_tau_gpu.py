@@ -229,3 +229,59 @@ def test_experiment_driver_small():
     ts = r["coarse_learned_through_solver"]
     assert ts["iters"] == 1 and len(ts["history"]) == 1 and np.isfinite(ts["cd"])
     assert r["training"]["samples"] > 0
+
+
+def _learned_lattice(seed, storage=ip.F32):
+    kw = dict(collision=ip.MRT, bc_set=ip.BC_CHANNEL, tau0=0.505, cs=0.1, u_in=0.05,
+              delta_kernel=ip.DELTA_PESKIN4, les_model=ip.LES_LEARNED, storage=storage)
+    g = ip.Lattice(160, 48, **kw)
+    rng = np.random.default_rng(seed)
+    bits, _ = lt.bf16_bits(tm.xavier_init(seed) + rng.normal(0, 0.1, tm.NPARAM))
+    stats = np.concatenate([[1.0, 0.04, 0, 0, 0, 2e-3], [1e-3, 0.02, 0.5, 0.5, 0.5, 2e-3],
+                            [-1e6] * 6, [1e6] * 6, [0.01]]).astype(np.float32)
+    g.load_tau_mlp(bits, stats)
+    sc = scenes.cylinder_channel(160, 48, 12, 40.3, 24.1, 0.05, 100, collision=ip.MRT)
+    g.set_markers(sc["markers"], ds=sc["ds"])
+    g.init_macros(*sc["init"])
+    return g
+
+
+def test_networks_of_several_handles_take_turns_in_constant_memory():
+    """The fused kernels read the network from constant memory, one network
+    per device at a time: handles with different networks, stepped and read
+    in alternation or from two host threads at once, give exactly what each
+    gives alone."""
+    import threading
+
+    solo = {}
+    for seed in (1, 2):
+        g = _learned_lattice(seed)
+        g.step(20, 1)
+        solo[seed] = (g.download(ip.FIELD_F), g.download(ip.FIELD_TAU))
+        g.close()
+    assert not np.array_equal(solo[1][1], solo[2][1])
+    a = {s: _learned_lattice(s) for s in (1, 2)}
+    for k in range(4):
+        for s in (1, 2):
+            a[s].step(5, 1 + 5 * k)
+    for s in (2, 1):  # downloads re-run the last step with the handle's network
+        assert np.array_equal(a[s].download(ip.FIELD_TAU), solo[s][1])
+        assert np.array_equal(a[s].download(ip.FIELD_F), solo[s][0])
+    b = {s: _learned_lattice(s) for s in (1, 2)}
+    errs = []
+
+    def run(s):
+        try:
+            for t in range(1, 21):
+                b[s].step(1, t)
+        except Exception as e:  # reported below
+            errs.append(e)
+
+    th = [threading.Thread(target=run, args=(s,)) for s in (1, 2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errs
+    for s in (1, 2):
+        assert np.array_equal(b[s].download(ip.FIELD_F), solo[s][0])
