@@ -52,6 +52,24 @@ def env_rank():
             int(os.environ.get("WORLD_SIZE", 1)))
 
 
+def max_over_ranks(x, dist=None, device="cuda"):
+    """The largest of the ranks' values of x (one all-reduce; x itself
+    without a process group).  Every rank must call it at the same point."""
+    if not dist:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_mlups(nodes, steps, world, seconds):
+    """Lattice updates of all ranks (each its own lattice of `nodes` nodes,
+    `steps` steps) per second of the slowest rank, in millions."""
+    return nodes * steps * world / seconds / 1e6
+
+
 def peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -238,13 +256,8 @@ def run_ours(a):
     t_next += a.steps
     barrier()
     torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    ms_max = ms
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = NX * NY * a.steps * world / (ms_max * 1e-3) / 1e6
+    ms_max = max_over_ranks(ev0.elapsed_time(ev1), dist)
+    value = whole_job_mlups(NX * NY, a.steps, world, ms_max * 1e-3)
 
     # ---- roofline: bulk kernel launch time (per-launch CUDA events) --------
     nprof = min(max(a.steps // 2, 20), 200)
@@ -289,11 +302,8 @@ def run_ours(a):
     got = e2e_pass(n_e2e)
     e2e_s = time.perf_counter() - t0
     assert got == n_e2e, got
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = NX * NY * n_e2e * world / e2e_s / 1e6
+    e2e_s = max_over_ranks(e2e_s, dist)
+    e2e = whole_job_mlups(NX * NY, n_e2e, world, e2e_s)
     h2d = (rho0.nbytes + ux0.nbytes + uy0.nbytes) / n_e2e
     d2h = (hist.nbytes + sum(b.nbytes for b in dump)) / n_e2e
 
