@@ -25,6 +25,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/ippi_lbm.h"
 #include "adjoint.h"
 #include "launch.h"
@@ -242,6 +244,16 @@ void adjoint_free(ippi_lbm* h)
     h->adj.ready = false;
 }
 
+// NVTX range over a library call: shown by profilers that record NVTX, a
+// no-op otherwise
+class Range {
+public:
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
+};
+
 // The fused learned-tau kernels read the network from their storage module's
 // constant memory (c_mlp), which holds one network per device at a time.  The
 // calls that launch those kernels hold the device's lock (MlpLock), copy the
@@ -294,6 +306,7 @@ int mlp_const_ready(ippi_lbm* h)
     default: e = mlp_const_addr_bf16(&dst); break;
     }
     CK(h, e);
+    nvtxMarkA("ippi tau network to constant memory");
     CK(h, cudaMemcpyAsync(dst, h->mlp_dev, (size_t)(kMlpParams + kMlpStats) * sizeof(float),
                           cudaMemcpyDeviceToDevice, h->st));
     loaded = h->mlp_version;
@@ -832,6 +845,7 @@ int tau_ready(ippi_lbm* h)
 int run_init(ippi_lbm* h)
 {
     if (int rc = tau_ready(h)) return rc;
+    Range range("ippi initial collision");
     MlpLock lock(h);
     if (int rc = mlp_const_ready(h)) return rc;
     std::memset(h->ctr_h, 0, sizeof(Ctr));
@@ -879,6 +893,7 @@ int materialize(ippi_lbm* h)
 {
     if (h->dl_valid) return IPPI_OK;
     if (int rc = tau_ready(h)) return rc;
+    Range range("ippi materialize (download pass)");
     MlpLock lock(h);
     if (int rc = mlp_const_ready(h)) return rc;
     const size_t nn = (size_t)h->p.nx * h->p.ny;
@@ -1271,6 +1286,7 @@ int ippi_step(ippi_lbm* h, int nsteps, int t0)
     if (nsteps < 0) return fail(h, IPPI_ERR_ARG, "negative step count");
     if (nsteps == 0) return IPPI_OK;
     CK(h, cudaSetDevice(h->p.device));
+    Range range("ippi_step");
     MlpLock lock(h);
     if (int rc = mlp_const_ready(h)) return rc;
     if (h->pending_init) {
@@ -1315,6 +1331,7 @@ int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk, double*
     if (int rc = tau_ready(h)) return rc;
     if (nsteps <= 0) return fail(h, IPPI_ERR_ARG, "nsteps must be positive");
     CK(h, cudaSetDevice(h->p.device));
+    Range range("ippi_profile_steps");
     MlpLock lock(h);
     if (int rc = mlp_const_ready(h)) return rc;
     if (h->pending_init) {
@@ -1512,6 +1529,7 @@ int ippi_save_state(ippi_lbm* h, void* host, size_t bytes)
     if (bytes < L.total) return fail(h, IPPI_ERR_ARG, "checkpoint needs %zu bytes, got %zu", L.total, bytes);
     CK(h, cudaSetDevice(h->p.device));
     if (h->pending_init) return fail(h, IPPI_ERR_STATE, "no state to save before the first step");
+    Range range("ippi_save_state");
     CkpHeader hd{};
     std::memcpy(hd.magic, kCkpMagic, sizeof hd.magic);
     hd.abi = IPPI_ABI_VERSION;
@@ -1567,6 +1585,7 @@ int ippi_load_state(ippi_lbm* h, const void* host, size_t bytes, int* last_step)
     if (ckp_hash(p, L.total - sizeof(CkpHeader)) != hd.payload_hash)
         return fail(h, IPPI_ERR_ARG, "checkpoint payload hash mismatch (corrupted)");
     CK(h, cudaSetDevice(h->p.device));
+    Range range("ippi_load_state");
     CK(h, cudaStreamSynchronize(h->st));
     for (const CkpSection& s : ckp_sections(h, L)) {
         if (s.bytes) CK(h, cudaMemcpy(s.dev, p, s.bytes, cudaMemcpyHostToDevice));
@@ -1695,6 +1714,7 @@ int ippi_adjoint_forward(ippi_lbm* h, int nsteps, int t0, int ckpt_every)
         return fail(h, IPPI_ERR_ARG, "rollout longer than the force history (%d steps)", h->hist_cap);
     if (int rc = tau_ready(h)) return rc;
     CK(h, cudaSetDevice(h->p.device));
+    Range range("ippi_adjoint_forward");
     MlpLock lock(h);
     if (int rc = mlp_const_ready(h)) return rc;
     adjoint_free(h);
@@ -1736,6 +1756,7 @@ int ippi_adjoint_backward(ippi_lbm* h, const double* dl_dforce, const double* dl
     if (grad_mlp && h->p.les_model != IPPI_LES_LEARNED)
         return fail(h, IPPI_ERR_STATE, "grad_mlp needs the learned model (IPPI_LES_LEARNED)");
     CK(h, cudaSetDevice(h->p.device));
+    Range range("ippi_adjoint_backward");
     MlpLock lock(h);
     if (int rc = mlp_const_ready(h)) return rc;
     const int nx = h->p.nx, ny = h->p.ny, nsteps = h->adj.nsteps, K = h->adj.K;
