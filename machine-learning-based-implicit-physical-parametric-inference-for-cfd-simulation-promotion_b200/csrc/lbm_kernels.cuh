@@ -58,7 +58,9 @@ struct StepArgs {
     int par;              // step parity: side-buffer half and ctr->t entry
     int fixed_t;          // step number for the MAT modes
     const double* init_m; // [3][ny][nx] initial rho, ux, uy (INIT modes)
-    const float* mlp;     // learned tau: parameters + feature statistics (LRN kernels)
+    const float* mlp;     // learned tau: parameters + feature statistics in device memory (the
+                          // adjoint reads them here; the LRN step kernels read the copy in
+                          // constant memory, c_mlp)
     const double* tau_field; // les == 3: relaxation time per node [ny][nx]
     void* mac;            // les 4, 5: [2][ny][nx] compute type, ux and uy of this step's
                           // post-stream (and IB-corrected) state, for the velocity gradient
