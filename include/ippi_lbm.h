@@ -201,7 +201,12 @@ int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk,
  * outside [lo, hi] take the Smagorinsky tau.
  * w_bf16[1313]: BF16 bit patterns of W1[32][6] b1[32] W2[32][32] b2[32]
  * w3[32] b3 (row-major, out x in).  stats[25]: mean[6] std[6] lo[6] hi[6]
- * out_scale. */
+ * out_scale.
+ * The step kernels read the network from the device's constant memory, which
+ * holds one network at a time: calls that run them for a learned-model
+ * handle hold a per-device lock until their stream has drained, and copy
+ * the handle's network in when another one is there.  Learned-model handles
+ * on one device therefore take turns, also across host threads. */
 #define IPPI_MLP_PARAMS 1313
 #define IPPI_MLP_STATS 25
 int ippi_load_tau_mlp(ippi_lbm* h, const uint16_t* w_bf16, size_t n, const float* stats,

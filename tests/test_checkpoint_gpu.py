@@ -181,3 +181,29 @@ def test_learned_network_and_fallback_counts_match_the_features():
     lat3, _ = _learned(lo=np.full(6, -1e6), hi=np.full(6, 1e6))
     lat3.step(5, 1)
     assert lat3.diagnostics()["fallback_nodes"] == 0
+
+
+def test_learned_model_resume_and_bf16_storage():
+    """A learned-tau lattice resumed by a handle that loaded the same network
+    (another network was used in between) and a BF16 lattice resumed: both
+    bit-identical to the uninterrupted runs."""
+    a, _ = _learned()
+    a.step(40, 1)
+    blob = a.save_state()
+    a.step(30, 41)
+    other, _ = _learned(lo=np.full(6, -1e6), hi=np.full(6, 1e6))  # constant memory used by another net
+    other.step(5, 1)
+    b, _ = _learned()
+    assert b.load_state(blob) == 40
+    b.step(30, 41)
+    for k in (ip.FIELD_F, ip.FIELD_TAU, ip.FIELD_NNFLAG):
+        assert np.array_equal(a.download(k), b.download(k)), k
+
+    c = _channel(ip.BF16, ip.MRT)
+    c.step(80, 1)
+    blob = c.save_state()
+    c.step(80, 81)
+    d = _channel(ip.BF16, ip.MRT)
+    d.load_state(blob)
+    d.step(80, 81)
+    _same(_snapshot(c), _snapshot(d))
