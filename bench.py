@@ -395,6 +395,33 @@ def run_learned_ncu_case(a):
                       "us_per_step": round(us, 2), "fallback_nodes": d["fallback_nodes"]}))
 
 
+def run_config3_rate(a):
+    """Step rate of the precision-sweep lattice: 16384 x 4096 (67 M nodes),
+    64 seeded IB cylinders (D = 48, about 9,700 markers), MRT + Smagorinsky,
+    Re 1000, for each population storage: --steps steps after 50 warm-up
+    steps, timed on the host around the synchronising ippi_step call.  One
+    JSON line per storage (GLUPS and HBM GB/s at the storage's bytes per
+    node)."""
+    import ippi_lbm as ip
+    from ippi_lbm.validation import config3_scene
+
+    for name, st, bpn in (("f32", ip.F32, 72), ("f16", ip.F16, 36), ("bf16", ip.BF16, 36)):
+        sc = config3_scene(storage=st)
+        nx, ny = sc["nx"], sc["ny"]
+        lat = ip.Lattice(nx, ny, **sc["params"])
+        lat.init_macros(*sc["init"])
+        lat.set_markers(sc["markers"], ds=sc["ds"], body=sc["bodies"])
+        lat.step(50, 1)
+        t0 = time.perf_counter()
+        lat.step(a.steps, 51)
+        s = time.perf_counter() - t0
+        lat.close()
+        glups = nx * ny * a.steps / s / 1e9
+        print(json.dumps({"config3_rate": f"channel_64_cylinders_{nx}x{ny}_mrt_{name}", "steps": a.steps,
+                          "markers": int(len(sc["ds"])), "us_per_step": round(s / a.steps * 1e6, 1),
+                          "glups": round(glups, 2), "hbm_gbs": round(glups * bpn, 1)}), flush=True)
+
+
 def run_adjoint_ncu_case(a):
     """The command profiled by ncu for the adjoint: the --adjoint lattice
     (learned tau, seeded Xavier network), an --adjoint-steps rollout
@@ -585,6 +612,8 @@ def main():
                     help="precision studies of configs 2 and 3 instead of the MLUPS line")
     ap.add_argument("--validate-steps2", type=int, default=160000)
     ap.add_argument("--validate-steps3", type=int, default=20000)
+    ap.add_argument("--config3-rate", action="store_true",
+                    help="step rate of the 64-cylinder 16384x4096 lattice per storage")
     ap.add_argument("--learned-ncu-case", action="store_true",
                     help="learned-tau steps of the coarse channel for an ncu capture")
     ap.add_argument("--adjoint-ncu-case", action="store_true",
@@ -598,6 +627,8 @@ def main():
         run_adjoint_ncu_case(a)
     elif a.learned_ncu_case:
         run_learned_ncu_case(a)
+    elif a.config3_rate:
+        run_config3_rate(a)
     elif a.learned:
         run_learned(a)
     elif a.adjoint:

@@ -711,6 +711,12 @@ int rebuild(ippi_lbm* h)
         I.force_now = (double*)up(nullptr, (size_t)nb * 2 * sizeof(double));
         I.force_hist = (double*)up(nullptr, (size_t)h->hist_cap * nb * 2 * sizeof(double));
         I.hist_cap = h->hist_cap;
+        // IB blocks of the one-launch step: one per kIbNodesPerBlock forced
+        // nodes, kIbCtas .. kIbMaxBlocks; the barrier counter restarts at 0,
+        // a multiple of every launch's arrivals
+        I.nib = (int)std::min<long long>(kIbMaxBlocks, std::max<long long>(kIbCtas, (nf + kIbNodesPerBlock - 1) /
+                                                                                      kIbNodesPerBlock));
+        CK(h, cudaMemset(h->ib_bar, 0, sizeof(unsigned long long)));
         for (auto& b : h->ib_bufs)
             if (!b.p) return fail(h, IPPI_ERR_NOMEM, "IB table allocation failed");
         h->force_now = I.force_now;

@@ -64,7 +64,7 @@ static void launch_bulk(const LaunchSet& L)
 template <int S, int CO, int SC, bool LRN, int XT>
 static void launch_merged(const LaunchSet& L)
 {
-    const unsigned nblk = (unsigned)kIbCtas + L.grid.x * L.grid.y;
+    const unsigned nblk = (unsigned)L.ib_args.nib + L.grid.x * L.grid.y;
     IbArgs ia = L.ib_args;
     ia.s = L.step;
     if (L.ib_nst == 16) {

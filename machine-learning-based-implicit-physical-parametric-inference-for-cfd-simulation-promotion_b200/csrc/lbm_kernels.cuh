@@ -814,8 +814,11 @@ __global__ void __launch_bounds__(kBandThreads) band_kernel(const BandArgs ba)
 //   finish   per-body force sums (FP64 fixed-order tree, one block per body)
 //            and the forced nodes' collision with the corrected velocity and
 //            the operator's forcing term
-// In a normal step the phases run in the first kIbCtas blocks of the step's
-// one launch (step_ib_fused, a global-memory barrier); alone (ib_fused) they
+// In a normal step the phases run in the first IbArgs::nib blocks of the
+// step's one launch (step_ib_fused, a global-memory barrier): kIbCtas, or
+// more where there are many forced nodes (one block per kIbNodesPerBlock of
+// them, at most one per SM, all of them in the launch's first wave); alone
+// (ib_fused) they
 // run as one thread-block cluster with cluster barriers.  Launched beside the
 // bulk kernel on another stream instead, the IB work only found free SMs
 // once the bulk kernel drained; as a separate cluster kernel with the bulk
@@ -824,6 +827,8 @@ __global__ void __launch_bounds__(kBandThreads) band_kernel(const BandArgs ba)
 // ---------------------------------------------------------------------------
 constexpr int kIbThreads = 128;  // threads per CTA of the IB cluster
 constexpr int kIbCtas = 8;       // CTAs per cluster (portable cluster size)
+constexpr int kIbNodesPerBlock = 512;  // forced nodes per IB block of step_ib_fused
+constexpr int kIbMaxBlocks = 148;      // IB blocks of step_ib_fused at most (one per SM)
 
 struct IbArgs {
     int nmark, nforced, nbody;
@@ -852,8 +857,9 @@ struct IbArgs {
     double* force_hist;         // [hist_cap][nbody][2]
     int hist_cap;
     unsigned long long* bar;    // GridBar arrival counter (step_ib_fused)
-    int bar_extra;              // arrivals each GridBar waits for beyond kIbCtas:
+    int bar_extra;              // arrivals each GridBar waits for beyond its blocks:
                                 // 0, or > 0 in the test that lets the wait run out
+    int nib;                    // IB blocks of step_ib_fused (kIbCtas .. kIbMaxBlocks)
     StepArgs s;
 };
 
@@ -998,12 +1004,13 @@ __device__ __forceinline__ void ib_collide_item(const IbArgs& ia, int n)
     }
 }
 
-// Barrier between the IB phases of the kIbCtas IB blocks.  ClusterBar: the
+// Barrier between the IB phases of the IB blocks.  ClusterBar: the kIbCtas
 // blocks form one thread-block cluster (the hardware co-schedules it).
-// GridBar: the blocks are the first kIbCtas blocks of the step kernel; a
+// GridBar: the blocks are the first nblk blocks of the step kernel; a
 // monotonic 64-bit arrival counter in global memory, nbar barriers per
-// launch, so each launch starts from a multiple of kIbCtas * nbar (the first
-// barrier cannot complete before every block has read it).  The wait is
+// launch, so each launch starts from a multiple of nblk * nbar (the first
+// barrier cannot complete before every block has read it; the host zeroes
+// the counter whenever a handle's nblk changes).  The wait is
 // bounded: after 1 s (or kBarSpins polls) the block records the barrier
 // error (Ctr::err = 2) and goes on, so a launch never hangs.  The IB blocks are
 // the lowest block indices of a launch on an otherwise idle stream and the
@@ -1021,6 +1028,7 @@ struct GridBar {
     int k;
     Ctr* err;
     int extra;
+    int nblk;
     __device__ __forceinline__ void operator()()
     {
         __syncthreads();
@@ -1028,7 +1036,7 @@ struct GridBar {
             __threadfence();
             atomicAdd(ctr, 1ull);
             k++;
-            const unsigned long long target = base + (unsigned long long)k * (kIbCtas + extra);
+            const unsigned long long target = base + (unsigned long long)k * (nblk + extra);
             int it = 0;
             unsigned long long v, t0, now;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
@@ -1105,9 +1113,9 @@ __global__ void __launch_bounds__(kIbThreads) ib_fused(const IbArgs ia, int pass
     ib_phases<S, SC, CO, LRN, NST, XT, kIbThreads>(ia, passes, blockIdx.x, gridDim.x, red, bar);
 }
 
-// A normal step with markers in ONE launch: blocks 0 .. kIbCtas-1 perform
-// the IB sub-step (GridBar between its phases), the rest are the bulk row
-// segments (block kIbCtas + by * tiles_x + bx).  The IB blocks are
+// A normal step with markers in ONE launch: blocks 0 .. nib-1 perform the
+// IB sub-step (GridBar between its phases), the rest are the bulk row
+// segments (block nib + by * tiles_x + bx).  The IB blocks are
 // dispatched first, so they run beside the bulk blocks from the start, and
 // the step ends when the launch does.
 template <int S, int SC, int CO, bool LRN, int NST, int XT, int AV>
@@ -1115,20 +1123,21 @@ __global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step
 {
     __shared__ double red[2][kBlockX];
     __shared__ unsigned long long s_base;
-    if (blockIdx.x < kIbCtas) {
+    const int nib = ia.nib;
+    if ((int)blockIdx.x < nib) {
         const unsigned long long nbar =
             1ull + 2ull * (unsigned long long)passes + ((XT && (ia.s.les == 4 || ia.s.les == 5)) ? 1ull : 0ull);
         if (threadIdx.x == 0) {
             unsigned long long v;
             asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(ia.bar) : "memory");
-            s_base = v - v % (nbar * kIbCtas);
+            s_base = v - v % (nbar * (unsigned long long)nib);
         }
         __syncthreads();
-        GridBar bar{ia.bar, s_base, 0, ia.s.ctr, ia.bar_extra};
-        ib_phases<S, SC, CO, LRN, NST, XT, kBlockX>(ia, passes, blockIdx.x, kIbCtas, red, bar);
+        GridBar bar{ia.bar, s_base, 0, ia.s.ctr, ia.bar_extra, nib};
+        ib_phases<S, SC, CO, LRN, NST, XT, kBlockX>(ia, passes, blockIdx.x, nib, red, bar);
         return;
     }
-    const int tile = blockIdx.x - kIbCtas;
+    const int tile = blockIdx.x - nib;
     const int by = tile / ia.s.tiles_x, bx = tile - by * ia.s.tiles_x;
     bulk_tile<S, CO, SC, LRN, XT, AV>(ia.s, bx, by, threadIdx.x);
 }
@@ -1181,7 +1190,7 @@ __global__ void __launch_bounds__(kBlockX, 8) mac_ib_fused(const IbArgs ia, int 
             s_base = v - v % (nbar * kIbCtas);
         }
         __syncthreads();
-        GridBar bar{ia.bar, s_base, 0, ia.s.ctr, ia.bar_extra};
+        GridBar bar{ia.bar, s_base, 0, ia.s.ctr, ia.bar_extra, kIbCtas};
         const int t = step_time(ia.s);
         if (ia.s.mode == MODE_STEP && blockIdx.x == 0 && threadIdx.x == 0) ia.s.ctr->t[ia.s.par ^ 1] = t + 1;
         ib_force_phases<S, SC, NST, 1, kBlockX, false>(ia, passes, blockIdx.x, kIbCtas, red, bar, t);

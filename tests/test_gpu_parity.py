@@ -198,3 +198,40 @@ def test_bad_arguments_are_rejected():
         g.init_macros(None, ux)
     g.init_macros()  # defaults are valid; the handle still steps
     g.step(2, 1)
+
+
+def test_many_cylinders_fp64_matches_oracle():
+    """24 cylinders (1,224 markers): enough forced nodes that the one-launch
+    step runs its IB sub-step in more than the minimum 8 blocks.  Fields and
+    per-body forces against the oracle."""
+    from ippi_lbm.validation import seeded_cylinders
+
+    nx, ny, d = 640, 320, 16
+    o, g = pair(nx, ny, collision=ip.MRT, bc_set=ip.BC_CHANNEL, u_in=0.05, tau0=0.56, cs=0.1,
+                delta_kernel=ip.DELTA_PESKIN4, mdf_iters=2)
+    cs = seeded_cylinders(nx, ny, d, 24, d, seed=3)
+    nm = int(np.ceil(np.pi * d))
+    xy = np.concatenate([cylinder_markers(cx, cy, d / 2, nm) for cx, cy in cs])
+    body = np.repeat(np.arange(len(cs), dtype=np.int32), nm)
+    ds = np.full(len(body), np.pi * d / nm)
+    # forced nodes: every node within the 4 x 4 Peskin support of a marker
+    forced = set()
+    for x, y in xy:
+        for i in range(int(np.floor(x)) - 1, int(np.floor(x)) + 3):
+            for j in range(int(np.floor(y)) - 1, int(np.floor(y)) + 3):
+                forced.add((i, j))
+    assert len(forced) > 8 * 512
+    o.set_markers(xy, body=body, ds=ds)
+    g.set_markers(xy, body=body, ds=ds)
+    y = np.arange(ny) + 0.5
+    ux = np.tile((4 * 0.05 * y * (ny - y) / ny ** 2)[:, None], (1, nx))
+    ux = ux + np.random.default_rng(1).uniform(-1e-4, 1e-4, ux.shape)
+    o.init_macros(np.ones((ny, nx)), ux, np.zeros((ny, nx)))
+    g.init_macros(np.ones((ny, nx)), ux, np.zeros((ny, nx)))
+    for n, t0 in ((1, 1), (24, 2)):
+        o.step(n, t0)
+        g.step(n, t0)
+        compare(o, g, 1e-11)
+        fo, _ = o.forces()
+        fg = g.forces()
+        np.testing.assert_allclose(np.asarray(fg).reshape(-1), np.asarray(fo).reshape(-1), rtol=1e-9, atol=1e-14)
