@@ -1168,7 +1168,7 @@ static void next_tau(orc* s, double* tau_out, unsigned char* flag_out)
     memcpy(fxs, s->fxn, n * sizeof(double));
     memcpy(fys, s->fyn, n * sizeof(double));
     double* bfs = (double*)malloc(2 * (s->nbody + 1) * sizeof(double));
-    memcpy(bfs, s->body_force, 2 * s->nbody * sizeof(double));
+    if (s->nbody) memcpy(bfs, s->body_force, 2 * s->nbody * sizeof(double));
     ib_substep(s);
     if (s->p.collision == COLL_BGK) nn_band(s);
     for (int i = 1; i < s->NX - 1; i++)
@@ -1202,7 +1202,7 @@ static void next_tau(orc* s, double* tau_out, unsigned char* flag_out)
     memcpy(s->uy, uys, n * sizeof(double));
     memcpy(s->fxn, fxs, n * sizeof(double));
     memcpy(s->fyn, fys, n * sizeof(double));
-    memcpy(s->body_force, bfs, 2 * s->nbody * sizeof(double));
+    if (s->nbody) memcpy(s->body_force, bfs, 2 * s->nbody * sizeof(double));
     free(tsave); free(fsave); free(uxs); free(uys); free(fxs); free(fys); free(bfs);
 }
 

@@ -228,3 +228,24 @@ def test_mrt_and_bgk_agree_on_conserved_and_shear_moments(oracle):
         # and the other moments do differ (the MRT is not BGK in disguise)
         q = e[:, 0] ** 2 + e[:, 1] ** 2
         assert abs((out[0] * q).sum() - (out[1] * q).sum()) > 1e-9
+
+
+def test_oracle_runs_clean_under_address_and_undefined_behaviour_sanitizers(tmp_path):
+    """The oracle's C code, built with -fsanitize=address,undefined, through
+    its plate, channel, IB, solid and closure paths (tests/oracle_sanitize.c)."""
+    import shutil
+    import subprocess
+
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no gcc")
+    here = os.path.dirname(os.path.abspath(__file__))
+    odir = os.path.join(os.path.dirname(here), "oracle")
+    exe = str(tmp_path / "oracle_sanitize")
+    r = subprocess.run([gcc, "-std=gnu11", "-O1", "-g", "-fno-omit-frame-pointer", "-fsanitize=address,undefined",
+                        "-fno-sanitize-recover=undefined", "-I", odir, os.path.join(here, "oracle_sanitize.c"),
+                        os.path.join(odir, "ippi_oracle.c"), "-lm", "-o", exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300,
+                       env=dict(os.environ, ASAN_OPTIONS="detect_leaks=1"))
+    assert r.returncode == 0 and "ok" in r.stdout, (r.stdout + r.stderr)[-3000:]
