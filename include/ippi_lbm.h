@@ -138,6 +138,12 @@ int ippi_destroy(ippi_lbm* h);
 /* Set rho/u on every node and the populations to their equilibrium
  * (InitialLatticeFeq).  NULL arrays mean rho = 1 / u = 0.  Resets averages. */
 int ippi_init_macros(ippi_lbm* h, const double* rho, const double* ux, const double* uy);
+
+/* ippi_init_macros for FP32 host arrays: the Lattice fields of the
+ * reference's SINGLE build (Parameter.h REAL = float) that InitialLatticeFeq
+ * reads (NodeAndLattice.cpp:69-123).  The values are widened to FP64 on the
+ * device; half the bytes cross the bus. */
+int ippi_init_macros_f32(ippi_lbm* h, const float* rho, const float* ux, const float* uy);
 /* Lattice::InitialLatticeFeq on every node in the middle of a run (the
  * reference's ManageDataFromXflow / XflowABS, mesh.cpp:2391-2398, 2615-2620):
  * populations replaced by the equilibrium of the given moments (NULL: rho 1,
@@ -165,8 +171,22 @@ int ippi_load_band_net(ippi_lbm* h, int type, const float* w, size_t n);
  * NaN in any of them.  Synchronises the handle's stream. */
 int ippi_step(ippi_lbm* h, int nsteps, int t0);
 
+/* No counterpart in the reference (measurement): ippi_step with device
+ * timing.  The steps are queued behind a short hold on the handle's stream
+ * (about 0.5 ms of GPU time), so they run back to back however slowly the host
+ * issues them, and *ms receives the milliseconds between CUDA events recorded
+ * on that stream just before the first step and just after the last.  A
+ * pending initial collision runs before the timed region. */
+int ippi_step_timed(ippi_lbm* h, int nsteps, int t0, double* ms);
+
 /* Copy a field to host memory; bytes must equal the field's size. */
 int ippi_download(ippi_lbm* h, int field, void* host, size_t bytes);
+
+/* ippi_download into FP32 host memory, the LatMesh fields WriteDatFluid reads
+ * under the reference's SINGLE build (mesh.cpp:1180-1243 with REAL = float):
+ * any field but IPPI_FIELD_FLAGS, rounded to FP32 on the device; bytes must
+ * equal the field's element count times 4. */
+int ippi_download_f32(ippi_lbm* h, int field, float* host, size_t bytes);
 
 /* Force on each body (lattice units, FP64, computed by the IB sub-step on the
  * current velocity field): force_xy[2 * nbody] = (Fx, Fy); *nbody receives

@@ -77,6 +77,7 @@ struct ippi_lbm {
     void* corner = nullptr;
     void* avg = nullptr;
     double* init_m = nullptr;
+    float* io32 = nullptr;    // [9][ny][nx] staging of the FP32 host-buffer calls
     bool pending_init = true;
     int last_t = 0;     // user step number of the last executed step
     int kcount = 0;     // internal steps executed (init counts as k = 0)
@@ -221,6 +222,13 @@ cudaError_t dalloc(P** p, size_t bytes)
 void dfree(void* p)
 {
     if (p) cudaFree(p);
+}
+
+// grid of the grid-stride conversion kernels: 256-thread blocks, at most
+// 32 per SM of a 148-SM device
+unsigned convert_blocks(size_t n)
+{
+    return (unsigned)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 32));
 }
 
 void drop_graphs(ippi_lbm* h)
@@ -1132,6 +1140,7 @@ int ippi_destroy(ippi_lbm* h)
     dfree(h->corner);
     dfree(h->avg);
     dfree(h->init_m);
+    dfree(h->io32);
     dfree(h->dl);
     dfree(h->dl_flags);
     dfree(h->red);
@@ -1150,6 +1159,12 @@ int ippi_destroy(ippi_lbm* h)
 
 namespace {
 int init_macros(ippi_lbm* h, const double* rho, const double* ux, const double* uy, bool keep_means);
+int init_macros_f32(ippi_lbm* h, const float* rho, const float* ux, const float* uy);
+}
+
+int ippi_init_macros_f32(ippi_lbm* h, const float* rho, const float* ux, const float* uy)
+{
+    return init_macros_f32(h, rho, ux, uy);
 }
 
 int ippi_init_macros(ippi_lbm* h, const double* rho, const double* ux, const double* uy)
@@ -1164,23 +1179,15 @@ int ippi_reequilibrate(ippi_lbm* h, const double* rho, const double* ux, const d
 }
 
 namespace {
-int init_macros(ippi_lbm* h, const double* rho, const double* ux, const double* uy, bool keep_means)
+// Defaults for the fields the caller did not give, the validity check and
+// the pending initial collision, once the given fields are in init_m.
+int init_macros_finish(ippi_lbm* h, bool has_rho, bool has_ux, bool has_uy, bool keep_means)
 {
-    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
-    CK(h, cudaSetDevice(h->p.device));
     const size_t nn = (size_t)h->p.nx * h->p.ny;
-    if (!h->init_m) CK(h, dalloc(&h->init_m, 3 * nn * sizeof(double)));
-    // host fields straight into the device table (fast from pinned memory),
-    // defaults and the validity check on the device
-    const double* src[3] = {rho, ux, uy};
-    for (int q = 0; q < 3; q++)
-        if (src[q])
-            CK(h, cudaMemcpyAsync(h->init_m + q * nn, src[q], nn * sizeof(double),
-                                  cudaMemcpyHostToDevice, h->st));
     unsigned long long* bad = reinterpret_cast<unsigned long long*>(h->red);
     CK(h, cudaMemsetAsync(bad, 0xff, sizeof *bad, h->st));
     init_fields_kernel<<<std::min<size_t>((nn + 255) / 256, 4096), 256, 0, h->st>>>(
-        h->init_m, (long long)nn, rho != nullptr, ux != nullptr, uy != nullptr, bad);
+        h->init_m, (long long)nn, has_rho, has_ux, has_uy, bad);
     CK(h, cudaGetLastError());
     if (!keep_means) CK(h, cudaMemsetAsync(h->avg, 0, 3 * nn * h->csize, h->st));
     unsigned long long first_bad = 0;
@@ -1194,6 +1201,42 @@ int init_macros(ippi_lbm* h, const double* rho, const double* ux, const double* 
     h->dl_valid = false;
     if (!keep_means) h->hist_written = 0;
     return IPPI_OK;
+}
+
+int init_macros(ippi_lbm* h, const double* rho, const double* ux, const double* uy, bool keep_means)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    CK(h, cudaSetDevice(h->p.device));
+    const size_t nn = (size_t)h->p.nx * h->p.ny;
+    if (!h->init_m) CK(h, dalloc(&h->init_m, 3 * nn * sizeof(double)));
+    // host fields straight into the device table (fast from pinned memory),
+    // defaults and the validity check on the device
+    const double* src[3] = {rho, ux, uy};
+    for (int q = 0; q < 3; q++)
+        if (src[q])
+            CK(h, cudaMemcpyAsync(h->init_m + q * nn, src[q], nn * sizeof(double),
+                                  cudaMemcpyHostToDevice, h->st));
+    return init_macros_finish(h, rho != nullptr, ux != nullptr, uy != nullptr, keep_means);
+}
+
+int init_macros_f32(ippi_lbm* h, const float* rho, const float* ux, const float* uy)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    CK(h, cudaSetDevice(h->p.device));
+    const size_t nn = (size_t)h->p.nx * h->p.ny;
+    if (!h->init_m) CK(h, dalloc(&h->init_m, 3 * nn * sizeof(double)));
+    if (!h->io32) CK(h, dalloc(&h->io32, 9 * nn * sizeof(float)));
+    // FP32 host fields into the staging planes, widened on the device
+    const float* src[3] = {rho, ux, uy};
+    for (int q = 0; q < 3; q++)
+        if (src[q]) {
+            CK(h, cudaMemcpyAsync(h->io32 + q * nn, src[q], nn * sizeof(float), cudaMemcpyHostToDevice,
+                                  h->st));
+            convert_kernel<float, double><<<convert_blocks(nn), 256, 0, h->st>>>(
+                h->io32 + q * nn, h->init_m + q * nn, (long long)nn);
+            CK(h, cudaGetLastError());
+        }
+    return init_macros_finish(h, rho != nullptr, ux != nullptr, uy != nullptr, false);
 }
 }  // namespace
 
@@ -1285,16 +1328,11 @@ int ippi_load_band_net(ippi_lbm* h, int type, const float* w, size_t n)
     return rebuild(h);
 }
 
-int ippi_step(ippi_lbm* h, int nsteps, int t0)
+namespace {
+// Queue nsteps steps numbered t0.. on the handle's stream (graph launches
+// only; nothing waits).  The caller holds the network lock.
+int enqueue_steps(ippi_lbm* h, int nsteps, int t0)
 {
-    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
-    if (int rc = tau_ready(h)) return rc;
-    if (nsteps < 0) return fail(h, IPPI_ERR_ARG, "negative step count");
-    if (nsteps == 0) return IPPI_OK;
-    CK(h, cudaSetDevice(h->p.device));
-    Range range("ippi_step");
-    MlpLock lock(h);
-    if (int rc = mlp_const_ready(h)) return rc;
     if (h->pending_init) {
         int rc = run_init(h);
         if (rc) return rc;
@@ -1322,6 +1360,12 @@ int ippi_step(ippi_lbm* h, int nsteps, int t0)
     h->last_t = t0 + nsteps - 1;
     h->hist_written += nsteps;
     h->dl_valid = false;
+    return IPPI_OK;
+}
+
+// Drain the stream after queued steps and report their status word.
+int finish_steps(ippi_lbm* h)
+{
     CK(h, cudaMemcpyAsync(h->ctr_h, h->ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, h->st));
     CK(h, cudaStreamSynchronize(h->st));
     if (h->ctr_h->err == 2)
@@ -1329,6 +1373,74 @@ int ippi_step(ippi_lbm* h, int nsteps, int t0)
     if (h->ctr_h->err)
         return fail(h, IPPI_ERR_DIVERGED, "Simulation Error! rho left [0,10] at step %d", h->ctr_h->err_t);
     return IPPI_OK;
+}
+
+// Holds the stream for about `ns` nanoseconds of %globaltimer (at most 2^22
+// polls), so that work queued behind it starts back to back.
+__global__ void hold_kernel(long long ns)
+{
+    long long t0, t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (int i = 0; i < (1 << 22); i++) {
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 >= ns) break;
+        __nanosleep(1000);
+    }
+}
+}  // namespace
+
+int ippi_step(ippi_lbm* h, int nsteps, int t0)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (int rc = tau_ready(h)) return rc;
+    if (nsteps < 0) return fail(h, IPPI_ERR_ARG, "negative step count");
+    if (nsteps == 0) return IPPI_OK;
+    CK(h, cudaSetDevice(h->p.device));
+    Range range("ippi_step");
+    MlpLock lock(h);
+    if (int rc = mlp_const_ready(h)) return rc;
+    if (int rc = enqueue_steps(h, nsteps, t0)) return rc;
+    return finish_steps(h);
+}
+
+int ippi_step_timed(ippi_lbm* h, int nsteps, int t0, double* ms)
+{
+    if (!h || !ms) return fail(h, IPPI_ERR_ARG, "null argument");
+    if (int rc = tau_ready(h)) return rc;
+    if (nsteps <= 0) return fail(h, IPPI_ERR_ARG, "nsteps must be positive");
+    CK(h, cudaSetDevice(h->p.device));
+    Range range("ippi_step_timed");
+    MlpLock lock(h);
+    if (int rc = mlp_const_ready(h)) return rc;
+    if (h->pending_init) {
+        // the initial collision is not part of the timed steps
+        if (int rc = run_init(h)) return rc;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(h, cudaEventCreate(&e0));
+    cudaError_t ce = cudaEventCreate(&e1);
+    if (ce != cudaSuccess) {
+        cudaEventDestroy(e0);
+        CK(h, ce);
+    }
+    hold_kernel<<<1, 1, 0, h->st>>>(500000);
+    int rc = IPPI_OK;
+    ce = cudaGetLastError();
+    if (ce == cudaSuccess) ce = cudaEventRecord(e0, h->st);
+    if (ce == cudaSuccess) rc = enqueue_steps(h, nsteps, t0);
+    if (ce == cudaSuccess && rc == IPPI_OK) ce = cudaEventRecord(e1, h->st);
+    if (ce != cudaSuccess) rc = fail(h, IPPI_ERR_CUDA, "timed step: %s", cudaGetErrorString(ce));
+    const int rf = finish_steps(h);
+    if (rc == IPPI_OK) rc = rf;
+    if (rc == IPPI_OK) {
+        float f = 0.f;
+        ce = cudaEventElapsedTime(&f, e0, e1);
+        if (ce != cudaSuccess) rc = fail(h, IPPI_ERR_CUDA, "timed step: %s", cudaGetErrorString(ce));
+        *ms = f;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
 }
 
 int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk, double* ms_band, double* ms_ib)
@@ -1439,6 +1551,45 @@ int ippi_download(ippi_lbm* h, int field, void* host, size_t bytes)
     default: src = h->dl + 13 * nn; break;  // TAU
     }
     CK(h, cudaMemcpy(host, src, need, cudaMemcpyDeviceToHost));
+    return IPPI_OK;
+}
+
+int ippi_download_f32(ippi_lbm* h, int field, float* host, size_t bytes)
+{
+    if (!h || !host) return fail(h, IPPI_ERR_ARG, "null argument");
+    CK(h, cudaSetDevice(h->p.device));
+    if (field < 0 || field > 9 || field == IPPI_FIELD_FLAGS)
+        return fail(h, IPPI_ERR_ARG, "bad field %d for an FP32 download", field);
+    const size_t nn = (size_t)h->p.nx * h->p.ny;
+    const size_t n = field == IPPI_FIELD_F ? 9 * nn : nn;
+    if (bytes != n * sizeof(float))
+        return fail(h, IPPI_ERR_ARG, "field %d needs %zu bytes, got %zu", field, n * sizeof(float), bytes);
+    if (!h->io32) CK(h, dalloc(&h->io32, 9 * nn * sizeof(float)));
+    const float* src = h->io32;
+    if (field >= IPPI_FIELD_AVG_U && field <= IPPI_FIELD_AVG_RHO) {
+        const size_t off = (size_t)(field - IPPI_FIELD_AVG_U) * nn;
+        if (h->csize == 4) {
+            src = (const float*)h->avg + off;
+        } else {
+            convert_kernel<double, float><<<convert_blocks(nn), 256, 0, h->st>>>((const double*)h->avg + off,
+                                                                                h->io32, (long long)nn);
+            CK(h, cudaGetLastError());
+        }
+    } else {
+        int rc = materialize(h);
+        if (rc) return rc;
+        const size_t plane = field == IPPI_FIELD_F      ? 0
+                             : field == IPPI_FIELD_RHO  ? 9
+                             : field == IPPI_FIELD_UX   ? 10
+                             : field == IPPI_FIELD_UY   ? 11
+                             : field == IPPI_FIELD_NNFLAG ? 12
+                                                        : 13;  // TAU
+        convert_kernel<double, float><<<convert_blocks(n), 256, 0, h->st>>>(h->dl + plane * nn, h->io32,
+                                                                           (long long)n);
+        CK(h, cudaGetLastError());
+    }
+    CK(h, cudaMemcpyAsync(host, src, bytes, cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
     return IPPI_OK;
 }
 

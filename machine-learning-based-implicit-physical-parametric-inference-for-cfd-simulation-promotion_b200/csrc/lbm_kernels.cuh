@@ -1279,6 +1279,15 @@ __global__ void to_double_kernel(const C* in, double* out, long long n)
     if (i < n) out[i] = double(in[i]);
 }
 
+// element-wise type conversion (grid-stride), for the FP32 host-buffer calls
+template <typename A, typename B>
+__global__ void convert_kernel(const A* __restrict__ in, B* __restrict__ out, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = B(in[i]);
+}
+
 // deterministic FP64 sum: per-block partial sums, then one block
 static __global__ void sum_partial_kernel(const double* in, long long n, double* part)
 {

@@ -65,6 +65,30 @@ class Lattice:
         rho, ux, uy = _f64(rho, n), _f64(ux, n), _f64(uy, n)
         L.check(L.lib().ippi_init_macros(self._h, _p(rho), _p(ux), _p(uy)), self._h)
 
+    def init_macros_f32(self, rho=None, ux=None, uy=None):
+        """init_macros from FP32 arrays (ippi_init_macros_f32); float32
+        C-contiguous arrays are passed without a copy."""
+        n = self.nx * self.ny
+
+        def f32(a):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float32)
+            if a.size != n:
+                raise ValueError(f"expected {n} values, got {a.size}")
+            return a
+        rho, ux, uy = f32(rho), f32(ux), f32(uy)
+        L.check(L.lib().ippi_init_macros_f32(self._h, _p(rho, C.c_float), _p(ux, C.c_float),
+                                             _p(uy, C.c_float)), self._h)
+
+    def download_f32(self, field, out=None):
+        """A field rounded to FP32 (ippi_download_f32), into `out` when given."""
+        shape = (9, self.ny, self.nx) if field == L.FIELD_F else (self.ny, self.nx)
+        if out is None:
+            out = np.zeros(shape, np.float32)
+        L.check(L.lib().ippi_download_f32(self._h, field, _p(out, C.c_float), out.nbytes), self._h)
+        return out
+
     def reequilibrate(self, rho=None, ux=None, uy=None):
         """Populations at the equilibrium of the given moments, keeping the
         running means and the force history (a step must have been taken)."""
@@ -88,6 +112,14 @@ class Lattice:
 
     def step(self, n=1, t0=1):
         L.check(L.lib().ippi_step(self._h, n, t0), self._h)
+
+    def step_timed(self, n, t0=1):
+        """step() with device timing: milliseconds between CUDA events on the
+        handle's stream around the n steps, queued behind a short hold so
+        they run back to back (ippi_step_timed)."""
+        ms = C.c_double()
+        L.check(L.lib().ippi_step_timed(self._h, n, t0, C.byref(ms)), self._h)
+        return ms.value
 
     def profile_steps(self, n, t0=1):
         b, nb, ib = C.c_double(), C.c_double(), C.c_double()

@@ -106,6 +106,40 @@ def config3_scene(nx=16384, ny=4096, d=48, n=64, re=1000.0, u=0.04, seed=0, coll
     return sc
 
 
+def config3_crop_window(nx=16384, ny=4096, d=48, n=64, seed=0, cw=2048, ch=512, step=64):
+    """The cw x ch window of the precision-sweep layout that holds the most
+    whole cylinders with the scene's margins (3 d from its inlet and outlet,
+    2 d from its walls), scanning x0, y0 on a `step` grid in order; returns
+    (x0, y0, centres relative to the window)."""
+    c = seeded_cylinders(nx, ny, d, n, 2 * d, seed)
+    best = None
+    for x0 in range(0, nx - cw + 1, step):
+        for y0 in range(0, ny - ch + 1, step):
+            r = c - np.array([x0, y0], dtype=np.float64)
+            ok = ((r[:, 0] >= 3 * d) & (r[:, 0] <= cw - 3 * d) & (r[:, 1] >= 2 * d) & (r[:, 1] <= ch - 2 * d))
+            if best is None or int(ok.sum()) > best[0]:
+                best = (int(ok.sum()), x0, y0, r[ok])
+    return best[1], best[2], best[3]
+
+
+def config3_crop_scene(storage=L.F32, cw=2048, ch=512, d=48, re=1000.0, u=0.04, seed=0):
+    """A 2048 x 512 crop of the precision-sweep geometry: the cylinders of
+    config3_crop_window at their positions in the window, as a channel of
+    its own (inlet, outlet and walls at the window's edges), MRT +
+    Smagorinsky, Re 1000, the same seeded initial fields as every scene."""
+    x0, y0, centres = config3_crop_window(d=d, seed=seed, cw=cw, ch=ch)
+    sc = scenes.cylinder_channel(cw, ch, d, centres[0, 0], centres[0, 1], u, re, storage=storage, seed=seed)
+    xs, dss, bodies = [], [], []
+    for b, (cx, cy) in enumerate(centres):
+        xy, ds = scenes.cylinder_markers(cx, cy, d)
+        xs.append(xy)
+        dss.append(ds)
+        bodies.append(np.full(len(ds), b, dtype=np.int32))
+    sc.update(markers=np.concatenate(xs), ds=np.concatenate(dss), bodies=np.concatenate(bodies),
+              centres=centres, window=(x0, y0))
+    return sc
+
+
 def config3_precision(nx=16384, ny=4096, steps=20000, avg=10000, storages=("f64", "f32", "f16", "bf16"),
                       log=None):
     st_of = {"f64": L.F64, "f32": L.F32, "f16": L.F16, "bf16": L.BF16}

@@ -12,6 +12,9 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 /* D2Q9 velocity order of the reference: NodeAndLattice.cpp:3-13, mesh.cpp:3-13 */
 static const int E[9][2] = {{0, 0}, {1, 0}, {0, 1}, {-1, 0}, {0, -1},
@@ -336,6 +339,15 @@ static void build_mrt(double tm[9][9], double tminv[9][9])
 static double g_tm[9][9], g_tminv[9][9];
 static int g_mrt_ready = 0;
 
+/* The MRT matrices, built once before any threaded loop reads them. */
+static void mrt_tables(void)
+{
+    if (!g_mrt_ready) {
+        build_mrt(g_tm, g_tminv);
+        g_mrt_ready = 1;
+    }
+}
+
 static void collide_bgk(const double* fnew, const double* feq, double tau, double* fcol)
 {
     /* Lattice::ComputeBGKCollision, NodeAndLattice.cpp:150-161 */
@@ -646,6 +658,15 @@ orc* orc_create(const orc_params* p)
     return s;
 }
 
+int orc_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
 void orc_destroy(orc* s)
 {
     if (!s) return;
@@ -875,6 +896,7 @@ static void ib_substep(orc* s)
             }
         }
         /* UpdateVelocity for one rank: local i = 2 .. NX-2 (mesh.cpp:1250-1256) */
+#pragma omp parallel for schedule(static)
         for (int i = 2; i < s->NX - 1; i++)
             for (int j = 0; j < s->NY; j++) {
                 size_t id = ID(s, i, j);
@@ -900,6 +922,11 @@ static int collide_all(orc* s)
 {
     int err = 0;
     int coll = s->p.collision;
+    mrt_tables();
+    /* every node's collision reads only its own state (and, for the gradient
+     * closures, neighbour velocities nothing here writes): the columns run in
+     * parallel with the same arithmetic per node */
+#pragma omp parallel for schedule(static) reduction(min : err)
     for (int i = 1; i < s->NX - 1; ++i)
         for (int j = 0; j < s->NY; ++j) {
             size_t id = ID(s, i, j);
@@ -951,6 +978,7 @@ static void halo_exchange(orc* s)
 /* Mesh::Streaming (mesh.cpp:192-226). */
 static void streaming_ref(orc* s)
 {
+#pragma omp parallel for schedule(static)
     for (int i = 1; i < s->NX - 1; i++)
         for (int j = 1; j < s->NY - 1; j++) {
             if (s->style[ID(s, i, j)] != 'f') continue;
@@ -1042,6 +1070,7 @@ static double inlet_profile(const orc* s, int y)
 static void streaming_channel(orc* s)
 {
     int nx = s->p.nx, ny = s->p.ny;
+#pragma omp parallel for schedule(static)
     for (int x = 0; x < nx - 1; x++)
         for (int y = 0; y < ny; y++) {
             int i = x + 1;
@@ -1108,6 +1137,7 @@ static void average(orc* s, int t)
     if (t < s->p.avg_start) return;
     double a = (double)(t - s->p.avg_start), b = (double)(t - s->p.avg_start + 1);
     size_t n = (size_t)s->NX * s->NY;
+#pragma omp parallel for schedule(static)
     for (size_t id = 0; id < n; id++) {
         if (s->solid && s->solid[id]) continue;
         s->avg_u[id] = (s->avg_u[id] * a + s->ux[id]) / b;

@@ -29,7 +29,7 @@
  * Parity pin: the flat-plate step (flags, BGK/MRT/RR + Smagorinsky, NEE and
  * specular boundaries, averages, IB primitives) is pinned against the
  * reference sources compiled by oracle/build_ref.sh (tests/golden fixtures
- * and tests/test_oracle_vs_ref.py); the boundary networks are pinned against
+ * and tests/test_oracle.py); the boundary networks are pinned against
  * outputs of the shipped TorchScript nets (tests/golden/band_net_golden.npz).
  * The channel scene is pinned only by analytic known-answer tests.
  */
@@ -42,6 +42,11 @@ extern "C" {
 #endif
 
 typedef struct orc orc;
+
+/* Threads of the per-node loops (collision, streaming, averages, velocity
+ * update): OpenMP over columns, with each node's arithmetic unchanged, so
+ * results do not depend on the count.  1 when built without OpenMP. */
+int orc_threads(void);
 
 typedef struct {
     int nx, ny;          /* global lattice (reference Nx, Ny)                    */

@@ -55,6 +55,7 @@ def lib() -> C.CDLL:
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.POINTER(OrcParams)]
         L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_threads.restype = C.c_int
         L.orc_init_macros.argtypes = [C.c_void_p, _dp, _dp, _dp]
         L.orc_set_markers.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.POINTER(C.c_int), _dp]
         L.orc_load_band_net.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.c_size_t]
@@ -194,6 +195,12 @@ class Oracle:
 # --------------------------------------------------------------------------
 
 REF_VARIANTS = ("srt", "srt_peskin", "mrt", "rr", "srt_f32", "mrt_f32")
+
+
+def threads() -> int:
+    """Threads of the oracle's per-node loops (OpenMP; results do not depend
+    on the count)."""
+    return int(lib().orc_threads())
 
 
 def ref_available(variant="srt") -> bool:

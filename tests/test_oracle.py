@@ -249,3 +249,44 @@ def test_oracle_runs_clean_under_address_and_undefined_behaviour_sanitizers(tmp_
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300,
                        env=dict(os.environ, ASAN_OPTIONS="detect_leaks=1"))
     assert r.returncode == 0 and "ok" in r.stdout, (r.stdout + r.stderr)[-3000:]
+
+
+_THREAD_CHECK = r"""
+import hashlib, sys
+sys.path[:0] = sys.argv[1:3]
+import pyoracle as po
+from ippi_lbm import scenes
+sc = scenes.cylinder_channel(256, 96, 24, 80, 48, 0.04, 3900)
+p = dict(sc["params"]); p.pop("storage")
+o = po.Oracle(256, 96, **p)
+o.init_macros(*sc["init"])
+o.set_markers(sc["markers"], ds=sc["ds"])
+o.step(8, 1)
+h = hashlib.sha256()
+for f in (po.F, po.RHO, po.UX, po.UY, po.TAU):
+    h.update(o.get(f).tobytes())
+h.update(o.forces()[0].tobytes())
+print(po.threads(), h.hexdigest())
+"""
+
+
+def test_threaded_loops_give_the_same_bytes(oracle):
+    """The oracle's per-node loops run on OpenMP threads; every node's
+    arithmetic is the same whatever the thread count, so an MRT +
+    Smagorinsky channel with an IB cylinder gives identical bytes on 1 and 4
+    threads."""
+    import subprocess
+    import sys
+
+    from conftest import PKG_DIR, REPO
+
+    out = {}
+    for n in (1, 4):
+        env = dict(os.environ, OMP_NUM_THREADS=str(n))
+        r = subprocess.run([sys.executable, "-c", _THREAD_CHECK, os.path.join(REPO, "oracle"), PKG_DIR],
+                           env=env, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        threads, digest = r.stdout.split()
+        assert int(threads) == n
+        out[n] = digest
+    assert out[1] == out[4]
