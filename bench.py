@@ -647,6 +647,101 @@ def run_validate(a):
         print(json.dumps({"metric": "precision_study", "config2": c2, "config3": c3}), flush=True)
 
 
+PLATE_NX, PLATE_NY = 2401, 501
+
+
+def plate_nets():
+    """The four shipped boundary nets (AutoT01/03/05/07, TorchScript parameter
+    order, exported once as raw FP32 under tests/golden/band_nets)."""
+    import numpy as np
+
+    d = os.path.join(REPO, "tests", "golden", "band_nets")
+    return {t: np.fromfile(os.path.join(d, f"AutoT0{t}.f32"), dtype=np.float32) for t in (1, 3, 5, 7)}
+
+
+def run_plate(a):
+    """The reference's own shipped workload: the 2401 x 501 flat plate of
+    main.cpp:20-45 (BGK + Smagorinsky Cs 0.173, NEE inlet u 0.1, specular
+    bottom before x 400, no-slip after it) with the four boundary nets on
+    (mesh.cpp:357-380), FP64 (the reference's default REAL) and FP32 storage.
+    Per storage one JSON line: the step rate with nets (ippi_step_timed over
+    --steps steps), the per-launch CUDA-event times of the bulk kernel and of
+    the side-stream chain (boundary-net inputs + nets + band collisions) that
+    runs beside it, the step rate with the nets off, and the reference's own
+    CPU step with the nets on (libtorch build when present), all host cores,
+    a bounded sample."""
+    import numpy as np  # noqa: F401
+    import torch
+
+    import ippi_lbm as ip
+
+    torch.cuda.set_device(0)
+    nets = plate_nets()
+    nn = PLATE_NX * PLATE_NY
+    for name, st, bpn in (("f64", ip.F64, 144), ("f32", ip.F32, 72)):
+        res = {}
+        for with_nets in (True, False):
+            lat = ip.Lattice(PLATE_NX, PLATE_NY, storage=st)
+            if with_nets:
+                for t, w in nets.items():
+                    lat.load_band_net(t, w)
+            lat.step(max(a.warmup, 3), 1)
+            ms = lat.step_timed(a.steps, max(a.warmup, 3) + 1)
+            prof = lat.profile_steps(min(max(a.steps, 20), 200), max(a.warmup, 3) + 1 + a.steps)
+            res[with_nets] = (ms / a.steps, prof)
+            tau0 = lat.params.tau0
+            lat.close()
+        ms_step, (ms_bulk, ms_band, _) = res[True]
+        line = {"plate": f"flat_plate_{PLATE_NX}x{PLATE_NY}_bgk_smagorinsky_nets_{name}", "steps": a.steps,
+                "ms_per_step": round(ms_step, 5), "mlups": round(nn / ms_step / 1e3, 1),
+                "bulk_kernel_ms": round(ms_bulk, 5),
+                "bulk_kernel_gbs": round(nn * bpn / ms_bulk / 1e6, 1),
+                "side_chain_ms": round(ms_band, 5),
+                "band_nodes": 2 * (PLATE_NX - 2) + 2 * (PLATE_NY - 2),
+                "ms_per_step_nets_off": round(res[False][0], 5),
+                "mlups_nets_off": round(nn / res[False][0] / 1e3, 1)}
+        if not a.no_cpu:
+            sys.path.insert(0, os.path.join(REPO, "oracle"))
+            import pyoracle as po
+
+            variant = ("srt_torch" if name == "f64" else "srt_f32_torch")
+            if not po.ref_available(variant):
+                variant = "srt" if name == "f64" else "srt_f32"
+                os.environ.setdefault("IPPI_REF_NN_DIR", os.path.join(REPO, "tests", "golden", "band_nets"))
+            cores = os.cpu_count() or 1
+            with quiet_stdout():
+                sim = po.RefSim(PLATE_NX, PLATE_NY, tau=tau0, ranks=cores, variant=variant)
+                sim.step(1, 1)
+                t0 = time.perf_counter()
+                done = 0
+                while done < a.cpu_steps and (done < 2 or time.perf_counter() - t0 < 30):
+                    sim.step(1, 2 + done)
+                    done += 1
+                dt = time.perf_counter() - t0
+                del sim
+            line["cpu_reference"] = {
+                "mlups": round(nn * done / dt / 1e6, 3), "ms_per_step": round(dt / done * 1e3, 1),
+                "cores": cores, "kind": "reference",
+                "nets": "libtorch on the shipped archives" if variant.endswith("torch")
+                        else "the nets' FP32 forward restated (stand-in build)",
+                "sample": f"{done} steps, {cores} thread-ranks"}
+        print(json.dumps(line), flush=True)
+
+
+def run_plate_ncu_case(a):
+    """The command profiled by ncu for the boundary nets: the flat plate with
+    the four nets, FP32 storage, --steps single steps."""
+    import ippi_lbm as ip
+
+    lat = ip.Lattice(PLATE_NX, PLATE_NY, storage=ip.F32)
+    for t, w in plate_nets().items():
+        lat.load_band_net(t, w)
+    for s in range(a.steps):
+        lat.step(1, s + 1)
+    lat.close()
+    print(json.dumps({"plate_ncu_case": f"flat_plate_{PLATE_NX}x{PLATE_NY}_nets_f32", "steps": a.steps}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -679,9 +774,17 @@ def main():
                     help="short adjoint rollout and backward sweep for an ncu capture")
     ap.add_argument("--ncu-case", action="store_true",
                     help="short run of single launches for an ncu capture")
+    ap.add_argument("--plate", action="store_true",
+                    help="the reference's flat plate with its boundary nets (FP64 and FP32) and its CPU step")
+    ap.add_argument("--plate-ncu-case", action="store_true",
+                    help="flat-plate steps with the boundary nets for an ncu capture")
     a = ap.parse_args()
     if a.ncu_case:
         run_ncu_case(a)
+    elif a.plate:
+        run_plate(a)
+    elif a.plate_ncu_case:
+        run_plate_ncu_case(a)
     elif a.adjoint_ncu_case:
         run_adjoint_ncu_case(a)
     elif a.learned_ncu_case:

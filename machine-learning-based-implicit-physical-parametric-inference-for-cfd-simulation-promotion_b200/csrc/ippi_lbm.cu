@@ -617,6 +617,11 @@ int rebuild(ippi_lbm* h)
         CK(h, cudaMemcpy(h->band_work_d, work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice));
         CK(h, cudaMemcpy(h->band_type_d, wtype.data(), wtype.size() * sizeof(int), cudaMemcpyHostToDevice));
         h->band_blocks = (int)work.size();
+        const int st = h->p.storage;
+        CK(h, st == IPPI_F64   ? band_setup_f64()
+              : st == IPPI_F32 ? band_setup_f32()
+              : st == IPPI_F16 ? band_setup_f16()
+                               : band_setup_bf16());
     }
 
     // immersed-boundary tables
@@ -1370,6 +1375,8 @@ int finish_steps(ippi_lbm* h)
     CK(h, cudaStreamSynchronize(h->st));
     if (h->ctr_h->err == 2)
         return fail(h, IPPI_ERR_CUDA, "an immersed-boundary barrier timed out (blocks not co-resident)");
+    if (h->ctr_h->err == 3)
+        return fail(h, IPPI_ERR_CUDA, "a boundary-net weight copy did not complete in time");
     if (h->ctr_h->err)
         return fail(h, IPPI_ERR_DIVERGED, "Simulation Error! rho left [0,10] at step %d", h->ctr_h->err_t);
     return IPPI_OK;
@@ -1495,6 +1502,8 @@ int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk, double*
     CK(h, cudaMemcpy(h->ctr_h, h->ctr, sizeof(Ctr), cudaMemcpyDeviceToHost));
     if (h->ctr_h->err == 2)
         return fail(h, IPPI_ERR_CUDA, "an immersed-boundary barrier timed out (blocks not co-resident)");
+    if (h->ctr_h->err == 3)
+        return fail(h, IPPI_ERR_CUDA, "a boundary-net weight copy did not complete in time");
     if (h->ctr_h->err)
         return fail(h, IPPI_ERR_DIVERGED, "Simulation Error! rho left [0,10] at step %d", h->ctr_h->err_t);
     return IPPI_OK;

@@ -143,9 +143,21 @@ static cudaError_t launch_tpl(const LaunchSet& L)
         if (L.nprep > 0)
             launch_prio(prep_kernel<S, SC>, (L.nprep + 255) / 256, 256, L.side, L.side_prio, L.step,
                         L.prep, L.nprep);
-        if (L.band)
-            launch_prio(band_kernel<S, CO>, L.band_blocks, kBandThreads, L.side, L.side_prio,
-                        L.band_args);
+        if (L.band) {
+            // dynamic shared memory (two hidden-layer weight buffers and the
+            // activations), allowed once per device by band_setup
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(L.band_blocks);
+            cfg.blockDim = dim3(kBandThreads);
+            cfg.dynamicSmemBytes = kBandSmemBytes;
+            cfg.stream = L.side;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributePriority;
+            attr[0].val.priority = L.side_prio;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            cudaLaunchKernelEx(&cfg, band_kernel<S, CO>, L.band_args);
+        }
         if (L.ib) launch_ib<S, SC, CO, LRN>(L, L.side);
         if (L.events) cudaEventRecord(L.events[3], L.side);
         cudaEventRecord(L.join, L.side);
@@ -158,6 +170,21 @@ static cudaError_t launch_tpl(const LaunchSet& L)
     if (L.events) cudaEventRecord(L.events[1], L.stream);
     if (side) cudaStreamWaitEvent(L.stream, L.join, 0);
     return cudaGetLastError();
+}
+
+// the boundary-net kernels' dynamic shared memory above the 48 KB default
+// (current device; outside any stream capture)
+template <int S>
+static cudaError_t band_setup()
+{
+    for (cudaError_t e : {cudaFuncSetAttribute(band_kernel<S, CO_BGK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)kBandSmemBytes),
+                          cudaFuncSetAttribute(band_kernel<S, CO_MRT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)kBandSmemBytes),
+                          cudaFuncSetAttribute(band_kernel<S, CO_RR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)kBandSmemBytes)})
+        if (e != cudaSuccess) return e;
+    return cudaSuccess;
 }
 
 template <int S>

@@ -43,6 +43,12 @@ cudaError_t launch_f32(const LaunchSet& L);
 cudaError_t launch_f16(const LaunchSet& L);
 cudaError_t launch_bf16(const LaunchSet& L);
 
+// allow band_kernel's dynamic shared memory (current device), per storage
+cudaError_t band_setup_f64();
+cudaError_t band_setup_f32();
+cudaError_t band_setup_f16();
+cudaError_t band_setup_bf16();
+
 // device address (current device) of each storage module's constant-memory
 // copy of the fused learned-tau network (c_mlp in lbm_common.cuh)
 cudaError_t mlp_const_addr_f64(void** p);

@@ -31,6 +31,16 @@ enum : uint8_t { NF_EXPORT = 1, NF_DEFER = 2, NF_IB = 4, NF_SOLID = 8, NF_SBND =
 // step kernel modes
 enum { MODE_STEP = 0, MODE_INIT = 1, MODE_MAT = 2, MODE_MAT_INIT = 3 };
 
+// Resident 256-thread blocks per SM the step kernels are compiled for: 8 in
+// FP32 arithmetic (32 registers), 4 in FP64 (64 registers: at 32 the FP64
+// instances spilled 0.5-2.7 KB per thread), fewer with the learned network's
+// hidden layer in registers.
+template <int S, bool LRN>
+constexpr int step_min_blocks()
+{
+    return LRN ? (S == ST_F64 ? 2 : 3) : (S == ST_F64 ? 4 : 8);
+}
+
 // D2Q9 velocity order of the reference (NodeAndLattice.cpp:3-13):
 // 0 rest, 1 E, 2 N, 3 W, 4 S, 5 NE, 6 NW, 7 SW, 8 SE.
 __host__ __device__ constexpr int EX(int k)
@@ -60,7 +70,8 @@ __host__ __device__ constexpr C WK(int k)
 // next step, so concurrent kernels of one step never see a changing value.
 struct Ctr {
     int t[2];         // user time step (feeds the averages), by step parity
-    int err;          // 1 once rho left [0,10] or became NaN
+    int err;          // 1 once rho left [0,10] or became NaN; 2 an IB barrier wait ran
+                      // out; 3 a boundary-net weight copy wait ran out
     int err_t;        // first step where that happened
 };
 

@@ -496,7 +496,7 @@ __device__ __forceinline__ void node_epilogue(const StepArgs& a, long long node,
 // (the learned-tau variant keeps the network's hidden layer in registers:
 // fewer resident blocks)
 template <int S, int CO, int SC, bool LRN, int XT = 0>
-__global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step_kernel(const StepArgs a)
+__global__ void __launch_bounds__(kBlockX, (step_min_blocks<S, LRN>())) step_kernel(const StepArgs a)
 {
     using C = typename Store<S>::C;
     const int x = blockIdx.x * kBlockX + threadIdx.x;
@@ -620,7 +620,7 @@ __device__ __forceinline__ void bulk_tile(const StepArgs& a, int bx, int by, int
 // a normal step without immersed boundary work in the same launch: one
 // block per row segment; block (0, 0) advances the step counter
 template <int S, int CO, int SC, bool LRN, int XT = 0, int AV = 0>
-__global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step_fast(const StepArgs ap)
+__global__ void __launch_bounds__(kBlockX, (step_min_blocks<S, LRN>())) step_fast(const StepArgs ap)
 {
     bulk_tile<S, CO, SC, LRN, XT, AV>(ap, blockIdx.x, blockIdx.y, threadIdx.x);
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
@@ -638,7 +638,7 @@ struct PrepNode {
 };
 
 template <int S, int SC>
-__global__ void __launch_bounds__(256, 8) prep_kernel(const StepArgs a, const PrepNode* nodes, int n)
+__global__ void __launch_bounds__(256, (step_min_blocks<S, false>())) prep_kernel(const StepArgs a, const PrepNode* nodes, int n)
 {
     using C = typename Store<S>::C;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -661,10 +661,34 @@ __global__ void __launch_bounds__(256, 8) prep_kernel(const StepArgs a, const Pr
 
 // ---------------------------------------------------------------------------
 // boundary nets (Mesh::NNmodel_Type00..07, mesh.cpp:2767-3259)
+//
+// One block evaluates one net (Linear(nin,128)+ReLU, 6 x (Linear(128,128)+
+// ReLU), Linear(128,1)) on up to kBandNodes band nodes in FP32, as libtorch
+// does on the CPU.  Each hidden layer's 128 x 128 weight matrix (64 KB) is
+// brought into shared memory once per block by a TMA bulk copy
+// (cp.async.bulk, completion on an mbarrier), two layer buffers deep, so the
+// next layer's weights arrive while this layer computes.  Thread (warp w,
+// lane l) holds a 5-node x 4-output register tile: nodes 5w..5w+4, outputs
+// 4l..4l+3; per 4 inputs it reads 5 broadcast float4 activations and 4 float4
+// weight rows from shared memory for 80 FMAs.  kBandNodes = 40 puts the
+// 5,796 band nodes of the 2401 x 501 plate in 146 blocks, one wave.
 // ---------------------------------------------------------------------------
-constexpr int kBandNodes = 32;     // band nodes per block
-constexpr int kBandThreads = 256;  // 128 neurons x 2 node halves
+constexpr int kBandWarpNodes = 5;                          // nodes per warp
+constexpr int kBandWarps = 8;
+constexpr int kBandNodes = kBandWarpNodes * kBandWarps;    // band nodes per block
+constexpr int kBandThreads = 32 * kBandWarps;
 constexpr int kHidden = 128;
+constexpr int kBandIn = 16;                                // input width, zero-padded
+constexpr int kBandAct = kHidden + 4;                      // floats per activation row
+// dynamic shared memory of band_kernel: two hidden-layer weight buffers,
+// activations, the first layer's weights, outputs, two mbarriers
+constexpr int kBandSmemW = 2 * kHidden * kHidden;
+constexpr int kBandSmemAct = kBandNodes * kBandAct;
+constexpr int kBandSmemW1 = kBandIn * kHidden;
+constexpr size_t kBandSmemBytes =
+    (size_t)(kBandSmemW + kBandSmemAct + kBandSmemW1 + kBandNodes) * sizeof(float) + 2 * sizeof(uint64_t);
+static_assert(kBandSmemBytes <= 227 * 1024, "band_kernel shared memory");
+static_assert(((kBandSmemW + kBandSmemAct + kBandSmemW1 + kBandNodes) * 4) % 8 == 0, "mbarrier alignment");
 
 struct BandNode {
     int x, y, slot, nin;   // nin = 15 or 9
@@ -672,10 +696,10 @@ struct BandNode {
     int nb_stale;          // bit q: neighbour q reads the previous step's moments
 };
 
-struct BandNet {            // weights transposed to [in][out] for coalesced reads
+struct BandNet {            // weights transposed to [in][out]
     const float* w1t;       // [nin][128]
     const float* b1;        // [128]
-    const float* wht;       // [6][128][128]
+    const float* wht;       // [6][128][128], each layer 16-byte aligned and contiguous
     const float* bh;        // [6][128]
     const float* wo;        // [128]
     float bo;
@@ -683,29 +707,120 @@ struct BandNet {            // weights transposed to [in][out] for coalesced rea
 
 struct BandArgs {
     const BandNode* nodes;
-    const int2* work;       // per block: (first node, count); all of one net type
+    const int2* work;       // per block: (first node, count <= kBandNodes); all of one net type
     const int* work_type;
     BandNet net[8];
     StepArgs s;
 };
 
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// one layer's weights (64 KB, this GPU's global memory) into shared memory by
+// the TMA engine; the mbarrier completes when all bytes have landed
+__device__ __forceinline__ void band_weights_async(float* dst, const float* src, uint64_t* bar)
+{
+    constexpr uint32_t bytes = kHidden * kHidden * sizeof(float);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// wait for phase `parity` of an mbarrier, at most 2^22 polls (each poll may
+// suspend the thread for a while); false when the limit ran out
+__device__ __forceinline__ bool band_wait(uint64_t* bar, uint32_t parity)
+{
+    const uint32_t a = smem_u32(bar);
+    for (int i = 0; i < (1 << 22); i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// acc[j][i] += sum over k < K of act[node 5w+j][k] * wt[k][4l+i]
+template <int K>
+__device__ __forceinline__ void band_layer(const float* __restrict__ act, const float* __restrict__ wt,
+                                           int warp, int lane, float (&acc)[kBandWarpNodes][4])
+{
+    const float* arow = act + warp * kBandWarpNodes * kBandAct;
+#pragma unroll 2
+    for (int k = 0; k < K; k += 4) {
+        float4 x[kBandWarpNodes];
+#pragma unroll
+        for (int j = 0; j < kBandWarpNodes; j++) x[j] = *reinterpret_cast<const float4*>(arow + j * kBandAct + k);
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+            const float4 w = *reinterpret_cast<const float4*>(wt + (k + kk) * kHidden + 4 * lane);
+#pragma unroll
+            for (int j = 0; j < kBandWarpNodes; j++) {
+                const float xv = kk == 0 ? x[j].x : kk == 1 ? x[j].y : kk == 2 ? x[j].z : x[j].w;
+                acc[j][0] = fmaf(xv, w.x, acc[j][0]);
+                acc[j][1] = fmaf(xv, w.y, acc[j][1]);
+                acc[j][2] = fmaf(xv, w.z, acc[j][2]);
+                acc[j][3] = fmaf(xv, w.w, acc[j][3]);
+            }
+        }
+    }
+}
+
+// ReLU of the register tile into the activation rows (after every thread has
+// finished reading them)
+__device__ __forceinline__ void band_store(float* act, int warp, int lane, const float (&acc)[kBandWarpNodes][4])
+{
+#pragma unroll
+    for (int j = 0; j < kBandWarpNodes; j++)
+        *reinterpret_cast<float4*>(act + (warp * kBandWarpNodes + j) * kBandAct + 4 * lane) =
+            make_float4(fmaxf(acc[j][0], 0.f), fmaxf(acc[j][1], 0.f), fmaxf(acc[j][2], 0.f),
+                        fmaxf(acc[j][3], 0.f));
+}
+
 template <int S, int CO>
-__global__ void __launch_bounds__(kBandThreads) band_kernel(const BandArgs ba)
+__global__ void __launch_bounds__(kBandThreads, 1) band_kernel(const BandArgs ba)
 {
     using C = typename Store<S>::C;
     const StepArgs& a = ba.s;
-    __shared__ __align__(16) float act[2][kBandNodes][kHidden];
-    __shared__ float out[kBandNodes];
+    extern __shared__ __align__(128) float band_smem[];
+    float* wbuf = band_smem;                  // [2][128][128]
+    float* act = wbuf + kBandSmemW;           // [kBandNodes][kBandAct]
+    float* w1 = act + kBandSmemAct;           // [16][128]
+    float* outv = w1 + kBandSmemW1;           // [kBandNodes]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(outv + kBandNodes);  // [2]
     const int2 w = ba.work[blockIdx.x];
     const BandNet& net = ba.net[ba.work_type[blockIdx.x]];
     const C* sm_cur = reinterpret_cast<const C*>(a.side_m) + (long long)a.par * a.nslots * 3;
     const C* sm_old = reinterpret_cast<const C*>(a.side_m) + (long long)(a.par ^ 1) * a.nslots * 3;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nin = ba.nodes[w.x].nin;
 
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        band_weights_async(wbuf, net.wht, &bar[0]);
+        band_weights_async(wbuf + kHidden * kHidden, net.wht + kHidden * kHidden, &bar[1]);
+    }
+    // first layer's weights, zero rows beyond nin
+    for (int i = tid; i < kBandIn * kHidden; i += kBandThreads)
+        w1[i] = i / kHidden < nin ? net.w1t[i] : 0.f;
     // inputs: (u_x, u_y, rho) of each neighbour cast to float (mesh.cpp:2805-2808)
-    for (int i = tid; i < kBandNodes * 15; i += kBandThreads) {
-        const int n = i / 15, q = i % 15;
+    for (int i = tid; i < kBandNodes * kBandIn; i += kBandThreads) {
+        const int n = i / kBandIn, q = i % kBandIn;
         float v = 0.f;
         if (n < w.y && q < nin) {
             const BandNode& bn = ba.nodes[w.x + n];
@@ -714,61 +829,55 @@ __global__ void __launch_bounds__(kBandThreads) band_kernel(const BandArgs ba)
             const C* mm = m + (long long)bn.nb_slot[nb] * 3;
             v = float(comp == 0 ? mm[1] : (comp == 1 ? mm[2] : mm[0]));
         }
-        act[0][n][q] = v;
+        act[n * kBandAct + q] = v;
     }
     __syncthreads();
 
-    const int o = tid & (kHidden - 1);
-    const int half = tid >> 7;  // nodes half*16 .. half*16+15
-    float acc[16];
+    float acc[kBandWarpNodes][4];
     // layer 1: Linear(nin, 128) + ReLU
 #pragma unroll
-    for (int n = 0; n < 16; n++) acc[n] = net.b1[o];
-    for (int i = 0; i < nin; i++) {
-        const float wv = net.w1t[i * kHidden + o];
+    for (int j = 0; j < kBandWarpNodes; j++)
 #pragma unroll
-        for (int n = 0; n < 16; n++) acc[n] = fmaf(wv, act[0][half * 16 + n][i], acc[n]);
-    }
+        for (int i = 0; i < 4; i++) acc[j][i] = net.b1[4 * lane + i];
+    band_layer<kBandIn>(act, w1, warp, lane, acc);
     __syncthreads();
-#pragma unroll
-    for (int n = 0; n < 16; n++) act[1][half * 16 + n][o] = fmaxf(acc[n], 0.f);
+    band_store(act, warp, lane, acc);
     __syncthreads();
-    // hidden layers 2..7: Linear(128, 128) + ReLU
-    int cur = 1;
+    // hidden layers 2..7: Linear(128, 128) + ReLU, weights from shared memory
+    bool ok = true;
     for (int l = 0; l < 6; l++) {
-        const float* wt = net.wht + (long long)l * kHidden * kHidden;
+        const int b = l & 1;
 #pragma unroll
-        for (int n = 0; n < 16; n++) acc[n] = net.bh[l * kHidden + o];
-        for (int i = 0; i < kHidden; i += 4) {
-            const float w0 = wt[(i + 0) * kHidden + o];
-            const float w1 = wt[(i + 1) * kHidden + o];
-            const float w2 = wt[(i + 2) * kHidden + o];
-            const float w3 = wt[(i + 3) * kHidden + o];
+        for (int j = 0; j < kBandWarpNodes; j++)
 #pragma unroll
-            for (int n = 0; n < 16; n++) {
-                const float4 x4 = *reinterpret_cast<const float4*>(&act[cur][half * 16 + n][i]);
-                acc[n] = fmaf(w0, x4.x, acc[n]);
-                acc[n] = fmaf(w1, x4.y, acc[n]);
-                acc[n] = fmaf(w2, x4.z, acc[n]);
-                acc[n] = fmaf(w3, x4.w, acc[n]);
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int n = 0; n < 16; n++) act[cur ^ 1][half * 16 + n][o] = fmaxf(acc[n], 0.f);
-        cur ^= 1;
+            for (int i = 0; i < 4; i++) acc[j][i] = net.bh[l * kHidden + 4 * lane + i];
+        ok = band_wait(&bar[b], (l >> 1) & 1) && ok;
+        band_layer<kHidden>(act, wbuf + b * kHidden * kHidden, warp, lane, acc);
+        __syncthreads();  // this layer's weights and inputs are read
+        if (tid == 0 && l + 2 < 6)
+            band_weights_async(wbuf + b * kHidden * kHidden, net.wht + (size_t)(l + 2) * kHidden * kHidden, &bar[b]);
+        band_store(act, warp, lane, acc);
         __syncthreads();
     }
-    // output layer: Linear(128, 1), one warp per 4 nodes
-    {
-        const int warp = tid >> 5, lane = tid & 31;
-        for (int n = warp; n < kBandNodes; n += kBandThreads / 32) {
-            float v = 0.f;
-            for (int i = lane; i < kHidden; i += 32) v = fmaf(net.wo[i], act[cur][n][i], v);
+    if (!ok) {
+        // a weight copy did not land in time: report it, and give the copies
+        // still in flight one more bounded wait before the block exits
+        if (tid == 0) atomicExch(&a.ctr->err, 3);
+        band_wait(&bar[0], 0);
+        band_wait(&bar[1], 0);
+    }
+    // output layer: Linear(128, 1)
 #pragma unroll
-            for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-            if (lane == 0) out[n] = v + net.bo;
-        }
+    for (int j = 0; j < kBandWarpNodes; j++) {
+        const int n = warp * kBandWarpNodes + j;
+        const float4 x = *reinterpret_cast<const float4*>(act + n * kBandAct + 4 * lane);
+        float v = x.x * net.wo[4 * lane];
+        v = fmaf(x.y, net.wo[4 * lane + 1], v);
+        v = fmaf(x.z, net.wo[4 * lane + 2], v);
+        v = fmaf(x.w, net.wo[4 * lane + 3], v);
+#pragma unroll
+        for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == 0) outv[n] = v + net.bo;
     }
     __syncthreads();
 
@@ -776,7 +885,7 @@ __global__ void __launch_bounds__(kBandThreads) band_kernel(const BandArgs ba)
     // 392-396) and the collision of the band node
     if (tid < w.y) {
         const BandNode& bn = ba.nodes[w.x + tid];
-        const double nn_tau = (double)out[tid];
+        const double nn_tau = (double)outv[tid];
         const C* sf = reinterpret_cast<const C*>(a.side_f) + (long long)bn.slot * 9;
         const C* mm = sm_cur + (long long)bn.slot * 3;
         C f[9];
@@ -1119,7 +1228,7 @@ __global__ void __launch_bounds__(kIbThreads) ib_fused(const IbArgs ia, int pass
 // dispatched first, so they run beside the bulk blocks from the start, and
 // the step ends when the launch does.
 template <int S, int SC, int CO, bool LRN, int NST, int XT, int AV>
-__global__ void __launch_bounds__(kBlockX, LRN ? (S == ST_F64 ? 2 : 3) : 8) step_ib_fused(const IbArgs ia, int passes)
+__global__ void __launch_bounds__(kBlockX, (step_min_blocks<S, LRN>())) step_ib_fused(const IbArgs ia, int passes)
 {
     __shared__ double red[2][kBlockX];
     __shared__ unsigned long long s_base;
@@ -1178,7 +1287,7 @@ __global__ void __launch_bounds__(kBlockX) mac_kernel(const StepArgs a)
 // kIbCtas-1 the forced nodes' collisions, the others the bulk row segments;
 // every velocity the gradients read is final by then.
 template <int S, int SC, int NST>
-__global__ void __launch_bounds__(kBlockX, 8) mac_ib_fused(const IbArgs ia, int passes)
+__global__ void __launch_bounds__(kBlockX, (step_min_blocks<S, false>())) mac_ib_fused(const IbArgs ia, int passes)
 {
     __shared__ double red[2][kBlockX];
     __shared__ unsigned long long s_base;
@@ -1202,7 +1311,7 @@ __global__ void __launch_bounds__(kBlockX, 8) mac_ib_fused(const IbArgs ia, int 
 }
 
 template <int S, int SC, int CO, bool LRN, int AV>
-__global__ void __launch_bounds__(kBlockX, 8) collide_ib_fused(const IbArgs ia)
+__global__ void __launch_bounds__(kBlockX, (step_min_blocks<S, LRN>())) collide_ib_fused(const IbArgs ia)
 {
     if (blockIdx.x < kIbCtas) {
         for (int n = blockIdx.x * kBlockX + threadIdx.x; n < ia.nforced; n += kIbCtas * kBlockX)

@@ -240,6 +240,9 @@ class RefSim:
     def __init__(self, nx, ny, tau, cs=0.173, u_in=0.1, avg_start=30000, ranks=1,
                  variant="srt"):
         self.nx, self.ny, self.variant = nx, ny, variant
+        if variant.endswith("_torch"):
+            # the libtorch build loads the shipped archives copied next to it
+            os.environ.setdefault("IPPI_REF_PT_DIR", os.path.join(REF_DIR, "nn"))
         self._L = ref_lib(variant)
         self._h = self._L.ref_create(nx, ny, tau, cs, u_in, avg_start, ranks)
 

@@ -12,7 +12,9 @@
  *   - JudgeStyle writes LatMesh[i][Ny].u (mesh.cpp:1438), one element past
  *     each column; the columns are given spare capacity first so that write
  *     lands in owned memory and corrupts nothing (the value is never read);
- *   - the boundary nets are served by the torch stand-in (ref_shim/torch).
+ *   - the boundary nets are served by the torch stand-in (ref_shim/torch),
+ *     or, in the libtorch build (ref_torch/), by libtorch itself loading the
+ *     shipped TorchScript archives.
  */
 #include "mesh.h"
 
@@ -45,6 +47,10 @@ void* rank_main(void* p)
 {
     RankJob* j = (RankJob*)p;
     ippi_mpi_enter(&j->s->world, j->r);
+    // one intra-op thread per rank, as the reference's ranks run under
+    // OMP_NUM_THREADS=1 (its own at::set_num_threads(1) is commented out,
+    // mesh.cpp:2776); with libtorch each net call is pinned to the rank's core
+    at::set_num_threads(1);
     try {
         (*j->fn)(j->r);
     } catch (const ippi_mpi_abort&) {

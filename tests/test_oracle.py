@@ -290,3 +290,23 @@ def test_threaded_loops_give_the_same_bytes(oracle):
         assert int(threads) == n
         out[n] = digest
     assert out[1] == out[4]
+
+
+def test_reference_on_libtorch_matches_the_stand_in_build(oracle, monkeypatch):
+    """The reference compiled against libtorch (its boundary nets run by
+    libtorch on the shipped TorchScript archives) and the stand-in build (the
+    nets' forward restated in FP32) give the same plate with the nets on:
+    populations and moments to FP32 rounding of the net output, identical
+    net flags."""
+    if not oracle.ref_available("srt_torch") or not oracle.ref_available("srt"):
+        pytest.skip("reference builds absent (oracle/build_ref.sh)")
+    monkeypatch.setenv("IPPI_REF_NN_DIR", os.path.join(GOLDEN, "band_nets"))
+    a = oracle.RefSim(416, 12, tau=0.52, variant="srt_torch")
+    b = oracle.RefSim(416, 12, tau=0.52, variant="srt")
+    a.step(10, 1)
+    b.step(10, 1)
+    assert np.array_equal(a.get(oracle.NNFLAG), b.get(oracle.NNFLAG))
+    assert a.get(oracle.NNFLAG).sum() > 0
+    for f in (oracle.F, oracle.RHO, oracle.UX, oracle.UY):
+        assert np.abs(a.get(f) - b.get(f)).max() < 1e-7
+    assert np.abs(a.get(oracle.TAU) - b.get(oracle.TAU)).max() < 1e-6
