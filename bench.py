@@ -454,12 +454,33 @@ def run_learned_ncu_case(a):
                       "us_per_step": round(us, 2), "fallback_nodes": d["fallback_nodes"]}))
 
 
+def run_config3_ncu_case(a):
+    """The command profiled by ncu for one storage of the precision sweep: the
+    64-cylinder 16384 x 4096 lattice (MRT + Smagorinsky, 90 IB blocks) with
+    --storage populations, 3 warm-up steps, then --steps single steps (one
+    step_ib_fused launch each)."""
+    import ippi_lbm as ip
+    from ippi_lbm.validation import config3_scene
+
+    st = {"f32": ip.F32, "f16": ip.F16, "bf16": ip.BF16}[a.storage]
+    sc = config3_scene(storage=st)
+    lat = ip.Lattice(sc["nx"], sc["ny"], **sc["params"])
+    lat.init_macros(*sc["init"])
+    lat.set_markers(sc["markers"], ds=sc["ds"], body=sc["bodies"])
+    lat.step(3, 1)
+    for s_ in range(a.steps):
+        lat.step(1, 4 + s_)
+    lat.close()
+    print(json.dumps({"config3_ncu_case": f"channel_64_cylinders_{sc['nx']}x{sc['ny']}_mrt_{a.storage}",
+                      "steps": a.steps}))
+
+
 def run_config3_rate(a):
     """Step rate of the precision-sweep lattice: 16384 x 4096 (67 M nodes),
     64 seeded IB cylinders (D = 48, about 9,700 markers), MRT + Smagorinsky,
     Re 1000, for each population storage: --steps steps after 50 warm-up
-    steps, timed on the host around the synchronising ippi_step call.  One
-    JSON line per storage (GLUPS and HBM GB/s at the storage's bytes per
+    steps, device-timed (ippi_step_timed: CUDA events around the queued
+    steps).  One JSON line per storage (GLUPS and HBM GB/s at the storage's bytes per
     node)."""
     import ippi_lbm as ip
     from ippi_lbm.validation import config3_scene
@@ -471,9 +492,7 @@ def run_config3_rate(a):
         lat.init_macros(*sc["init"])
         lat.set_markers(sc["markers"], ds=sc["ds"], body=sc["bodies"])
         lat.step(50, 1)
-        t0 = time.perf_counter()
-        lat.step(a.steps, 51)
-        s = time.perf_counter() - t0
+        s = lat.step_timed(a.steps, 51) * 1e-3
         lat.close()
         glups = nx * ny * a.steps / s / 1e9
         print(json.dumps({"config3_rate": f"channel_64_cylinders_{nx}x{ny}_mrt_{name}", "steps": a.steps,
@@ -774,6 +793,9 @@ def main():
                     help="short adjoint rollout and backward sweep for an ncu capture")
     ap.add_argument("--ncu-case", action="store_true",
                     help="short run of single launches for an ncu capture")
+    ap.add_argument("--config3-ncu-case", action="store_true",
+                    help="precision-sweep steps of one storage (--storage) for an ncu capture")
+    ap.add_argument("--storage", default="f16", choices=["f32", "f16", "bf16"])
     ap.add_argument("--plate", action="store_true",
                     help="the reference's flat plate with its boundary nets (FP64 and FP32) and its CPU step")
     ap.add_argument("--plate-ncu-case", action="store_true",
@@ -783,6 +805,8 @@ def main():
         run_ncu_case(a)
     elif a.plate:
         run_plate(a)
+    elif a.config3_ncu_case:
+        run_config3_ncu_case(a)
     elif a.plate_ncu_case:
         run_plate_ncu_case(a)
     elif a.adjoint_ncu_case:

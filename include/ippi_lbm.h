@@ -179,6 +179,11 @@ int ippi_step(ippi_lbm* h, int nsteps, int t0);
  * pending initial collision runs before the timed region. */
 int ippi_step_timed(ippi_lbm* h, int nsteps, int t0, double* ms);
 
+/* The Smagorinsky constant of the following steps: the Cs argument of
+ * Mesh::OneLBMStep, passed on to Mesh::CaculateLESTau each step (mesh.cpp
+ * 357, 852-911).  cs >= 0; changing it rebuilds the step graphs. */
+int ippi_set_les_cs(ippi_lbm* h, double cs);
+
 /* Copy a field to host memory; bytes must equal the field's size. */
 int ippi_download(ippi_lbm* h, int field, void* host, size_t bytes);
 
@@ -226,7 +231,9 @@ int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk,
  * holds one network at a time: calls that run them for a learned-model
  * handle hold a per-device lock until their stream has drained, and copy
  * the handle's network in when another one is there.  Learned-model handles
- * on one device therefore take turns, also across host threads. */
+ * on one device therefore take turns, also across host threads.  The record
+ * of which network the constant memory holds assumes the device's primary
+ * context lives as long as the process (no cudaDeviceReset between calls). */
 #define IPPI_MLP_PARAMS 1313
 #define IPPI_MLP_STATS 25
 int ippi_load_tau_mlp(ippi_lbm* h, const uint16_t* w_bf16, size_t n, const float* stats,
@@ -363,13 +370,18 @@ int ippi_last_error(ippi_lbm* h, char* buf, size_t n);
  * field rho[ny][nx] (device memory) into *mass (device memory), enqueued on
  * `stream` (a cudaStream_t, NULL = default stream), without allocating any
  * device memory: for callers that cannot call cudaMalloc where they need the
- * mass checksum (inside stream capture, under another allocator's ownership
- * of device memory, in loops that forbid allocation after start-up).  Its
- * scratch is a fixed device array of IPPI_NOALLOC_MAX_ROWS row sums that the
- * library keeps on every GPU it is loaded on; ny beyond that is rejected
- * with IPPI_ERR_ARG.  The first call on a device looks up that array's
- * device address, so make it before any stream capture.  Calls share the
- * array: calls that overlap on the GPU race. */
+ * mass checksum (device memory owned by another allocator, such as a
+ * framework's caching allocator or a fixed arena reserved at start-up, and
+ * loops that forbid allocation after start-up).  Its scratch is a fixed
+ * device array of IPPI_NOALLOC_MAX_ROWS row sums that the library keeps on
+ * every GPU it is loaded on until the process exits; ny beyond that is
+ * rejected with IPPI_ERR_ARG.  The first call on a device looks up that
+ * array's device address and keeps it, so make that first call before any
+ * stream capture; the kept address assumes the device's primary context
+ * lives as long as the process (no cudaDeviceReset between calls).  Calls
+ * share the array: calls that overlap on the GPU race.  A launch error
+ * already pending from the caller's earlier work is left pending (not
+ * cleared) and makes the call return IPPI_ERR_CUDA. */
 #define IPPI_NOALLOC_MAX_ROWS 16384
 int ippi_mass_noalloc(const double* rho, int nx, int ny, double* mass, void* stream);
 

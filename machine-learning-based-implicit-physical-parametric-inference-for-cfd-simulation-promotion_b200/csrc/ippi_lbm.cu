@@ -110,6 +110,10 @@ struct ippi_lbm {
     unsigned long long* ib_bar = nullptr;  // arrival counter of the one-launch step's IB blocks
     void* mac = nullptr;          // IPPI_LES_WALE / CSM: [2][ny][nx] compute type, velocities
     double* wall_dist = nullptr;  // IPPI_LES_DYNAMIC: [ny][nx]
+    // hashes of the inputs a checkpoint presumes besides the parameters: the
+    // tau field, the learned network (weights and statistics), the wall
+    // distance (0 = never set)
+    uint64_t tau_field_hash = 0, mlp_hash = 0, wall_hash = 0;
     // solid nodes (halfway bounce-back) and their momentum-exchange links
     std::vector<uint8_t> solid;   // [ny][nx] or empty
     int2* solid_links = nullptr;  // (fluid node, direction into the solid)
@@ -267,7 +271,10 @@ public:
 // calls that launch those kernels hold the device's lock (MlpLock), copy the
 // handle's network there on the handle's stream when another one is loaded
 // (mlp_const_ready), and drain the stream before they let go of the lock, so
-// learned handles on one device take turns even across host threads.
+// learned handles on one device take turns even across host threads.  The
+// record of which network each module holds assumes the device's primary
+// context (and with it the constant memory) lives as long as the process: a
+// cudaDeviceReset between calls is not supported.
 constexpr int kMaxDevices = 64;
 std::recursive_mutex g_mlp_mu[kMaxDevices];
 unsigned long long g_mlp_loaded[kMaxDevices][4] = {};  // network version in each storage module
@@ -992,7 +999,8 @@ uint64_t ckp_hash(const unsigned char* p, size_t n, uint64_t x = 0xcbf29ce484222
 }
 
 // what the saved state presumes of the handle: parameters (not the device),
-// markers and solid mask
+// markers, solid mask, and what sets the relaxation times -- the tau field,
+// the learned network, the wall distance and the boundary nets
 uint64_t ckp_config_hash(const ippi_lbm* h)
 {
     const ippi_params& p = h->p;
@@ -1008,6 +1016,13 @@ uint64_t ckp_config_hash(const ippi_lbm* h)
     put(h->mk_ds.data(), h->mk_ds.size() * sizeof(double));
     put(h->mk_body.data(), h->mk_body.size() * sizeof(int));
     put(h->solid.data(), h->solid.size());
+    const uint64_t tau_inputs[] = {h->tau_field_hash, h->mlp_hash, h->wall_hash};
+    put(tau_inputs, sizeof tau_inputs);
+    for (int t = 0; t < 8; t++) {
+        if (!h->nets[t].loaded) continue;
+        put(&t, sizeof t);
+        put(h->nets[t].w.data(), h->nets[t].w.size() * sizeof(float));
+    }
     return x;
 }
 
@@ -1805,6 +1820,8 @@ int ippi_load_tau_mlp(ippi_lbm* h, const uint16_t* w_bf16, size_t n, const float
     if (!h->mlp_dev) CK(h, dalloc(&h->mlp_dev, blob.size() * sizeof(float)));
     CK(h, cudaMemcpy(h->mlp_dev, blob.data(), blob.size() * sizeof(float), cudaMemcpyHostToDevice));
     h->mlp_version = ++g_mlp_serial;
+    h->mlp_hash = ckp_hash(reinterpret_cast<const unsigned char*>(blob.data()), blob.size() * sizeof(float),
+                           0x6d6c70ull);
     // step graphs captured before the first load hold a null network pointer
     drop_graphs(h);
     h->dl_valid = false;
@@ -1844,6 +1861,7 @@ int ippi_set_tau_field(ippi_lbm* h, const double* tau)
     CK(h, cudaStreamSynchronize(h->st));
     if (!h->tau_field) CK(h, dalloc(&h->tau_field, nn * sizeof(double)));
     CK(h, cudaMemcpy(h->tau_field, tau, nn * sizeof(double), cudaMemcpyHostToDevice));
+    h->tau_field_hash = ckp_hash(reinterpret_cast<const unsigned char*>(tau), nn * sizeof(double), 0x746175ull);
     drop_graphs(h);
     h->dl_valid = false;
     return IPPI_OK;
@@ -1863,6 +1881,8 @@ int ippi_load_tau_mlp_f32(ippi_lbm* h, const float* w, size_t n, const float* st
         if (!std::isfinite(w[i])) return fail(h, IPPI_ERR_ARG, "tau network weight %zu is not finite", i);
     CK(h, cudaMemcpy(h->mlp_dev, w, n * sizeof(float), cudaMemcpyHostToDevice));
     h->mlp_version = ++g_mlp_serial;
+    h->mlp_hash = ckp_hash(reinterpret_cast<const unsigned char*>(stats), nstats * sizeof(float),
+                           ckp_hash(reinterpret_cast<const unsigned char*>(w), n * sizeof(float), 0x6d6c7033ull));
     return IPPI_OK;
 }
 
@@ -2134,6 +2154,19 @@ int ippi_solid_force(ippi_lbm* h, double* force_xy)
     return IPPI_OK;
 }
 
+int ippi_set_les_cs(ippi_lbm* h, double cs)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (!(cs >= 0) || !std::isfinite(cs)) return fail(h, IPPI_ERR_ARG, "Cs must be finite and >= 0");
+    if (cs == h->p.cs) return IPPI_OK;
+    CK(h, cudaSetDevice(h->p.device));
+    CK(h, cudaStreamSynchronize(h->st));
+    h->p.cs = cs;
+    drop_graphs(h);  // the step graphs hold the constant as a kernel parameter
+    h->dl_valid = false;
+    return IPPI_OK;
+}
+
 int ippi_set_wall_distance(ippi_lbm* h, const double* dist)
 {
     if (!h || !dist) return fail(h, IPPI_ERR_ARG, "null argument");
@@ -2144,6 +2177,7 @@ int ippi_set_wall_distance(ippi_lbm* h, const double* dist)
     CK(h, cudaStreamSynchronize(h->st));
     if (!h->wall_dist) CK(h, dalloc(&h->wall_dist, nn * sizeof(double)));
     CK(h, cudaMemcpy(h->wall_dist, dist, nn * sizeof(double), cudaMemcpyHostToDevice));
+    h->wall_hash = ckp_hash(reinterpret_cast<const unsigned char*>(dist), nn * sizeof(double), 0x77616c6cull);
     drop_graphs(h);
     h->dl_valid = false;
     return IPPI_OK;

@@ -756,7 +756,9 @@ __device__ __forceinline__ void band_layer(const float* __restrict__ act, const 
                                            int warp, int lane, float (&acc)[kBandWarpNodes][4])
 {
     const float* arow = act + warp * kBandWarpNodes * kBandAct;
-#pragma unroll 2
+    // fully unrolled: one block per SM leaves the whole register file to its
+    // 256 threads, so the shared-memory loads can run well ahead of the FMAs
+#pragma unroll
     for (int k = 0; k < K; k += 4) {
         float4 x[kBandWarpNodes];
 #pragma unroll

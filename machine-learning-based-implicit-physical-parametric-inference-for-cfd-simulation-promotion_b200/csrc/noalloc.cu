@@ -2,12 +2,11 @@
 // density field without any device allocation.
 //
 // Who needs it: callers that may not allocate device memory at the point
-// where they want the checksum -- code running while a CUDA stream is being
-// captured into a graph (cudaMalloc is not allowed there), hosts whose device
-// memory is owned by another allocator (a framework's caching allocator, a
-// fixed arena set up at start-up) and real-time loops that forbid allocation
-// after initialisation.  ippi_forces() computes the same sum but needs a
-// lattice handle, which allocates its own reduction scratch.
+// where they want the checksum -- hosts whose device memory is owned by
+// another allocator (a framework's caching allocator, a fixed arena set up
+// at start-up) and real-time loops that forbid allocation after
+// initialisation.  ippi_forces() computes the same sum but needs a lattice
+// handle, which allocates its own reduction scratch.
 //
 // The scratch is a file-scope __device__ array of kMaxRows doubles (128 KiB):
 // one partial sum per lattice row.  Every GPU that loads the library holds it
@@ -31,7 +30,9 @@ constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_row_partials[kMaxRows];
 
-// per-device address of g_row_partials, looked up once per device
+// per-device address of g_row_partials, looked up once per device and kept:
+// valid while the device's primary context lives, which this library
+// assumes is the whole process (no cudaDeviceReset between calls)
 double* g_scratch[kMaxDevices] = {};
 std::mutex g_mu;
 
@@ -93,7 +94,18 @@ extern "C" int ippi_mass_noalloc(const double* rho, int nx, int ny, double* mass
         part = g_scratch[dev];
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // an error pending from the caller's earlier launches is theirs: leave
+    // it pending, and do not launch behind it
+    if (cudaPeekAtLastError() != cudaSuccess) return IPPI_ERR_CUDA;
     row_sums<<<ny, kThreads, 0, st>>>(rho, nx, part);
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        cudaGetLastError();  // this call's launch failed: clear its error
+        return IPPI_ERR_CUDA;
+    }
     final_sum<<<1, kThreads, 0, st>>>(part, ny, mass);
-    return cudaGetLastError() == cudaSuccess ? IPPI_OK : IPPI_ERR_CUDA;
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        cudaGetLastError();
+        return IPPI_ERR_CUDA;
+    }
+    return IPPI_OK;
 }

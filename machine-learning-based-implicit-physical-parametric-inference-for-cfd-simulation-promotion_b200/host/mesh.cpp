@@ -73,6 +73,8 @@ void Mesh::InitialLatMesh(int Nx_P, int Ny, double tau, Point2D StartVel, double
     if (h_) ippi_destroy(h_);
     h_ = nullptr;
     if (!check(ippi_create(&p, &h_), "ippi_create")) return;
+    cs_ = p.cs;
+    for (bool& b : net_loaded_) b = false;
     nx_ = nx;
     ny_ = Ny;
     LatmeshSizeNx = nx;
@@ -98,19 +100,22 @@ void Mesh::InitialLatMesh(int Nx_P, int Ny, double tau, Point2D StartVel, double
             L.u = {0, 0};
             L.InitialLatticeFeq();
         }
-    synced_ = false;
+    synced_ = synced_f_ = false;
 }
 
 void Mesh::SetInitialField(const double* rho, const double* ux, const double* uy)
 {
     if (!h_) return;
     check(ippi_init_macros(h_, rho, ux, uy), "ippi_init_macros");
-    synced_ = false;
+    synced_ = synced_f_ = false;
 }
 
 bool Mesh::LoadBandNet(int type, const float* w, size_t n)
 {
-    return h_ && check(ippi_load_band_net(h_, type, w, n), "ippi_load_band_net");
+    if (!h_ || !check(ippi_load_band_net(h_, type, w, n), "ippi_load_band_net")) return false;
+    net_loaded_[type] = true;
+    synced_ = synced_f_ = false;
+    return true;
 }
 
 // Mesh::InitialIBParticle (mesh.cpp:173-191): NumNodes markers on the circle,
@@ -138,6 +143,7 @@ void Mesh::InitialIBParticle(int NumNodes, double Radius, double ParticlePositio
     }
     center = {(REAL)ParticlePositionX, (REAL)ParticlePositionY};
     radius = Radius;
+    marker_ds_ = ds;
     if (h_) check(ippi_set_markers(h_, NumNodes, xy.data(), ub.data(), nullptr, ds.data()), "ippi_set_markers");
 }
 
@@ -171,8 +177,12 @@ void Mesh::OneLBMStep(int RankID, int CoreNum, REAL Cs, REAL Pr, int t)
 {
     (void)RankID;
     (void)CoreNum;
-    (void)Cs;
-    (void)Pr;
+    (void)Pr;  // unused by the reference's active closure too (mesh.cpp:852-911)
+    // the per-call Smagorinsky constant, as CaculateLESTau receives it
+    if (h_ && (double)Cs != cs_) {
+        if (!check(ippi_set_les_cs(h_, (double)Cs), "ippi_set_les_cs")) return;
+        cs_ = (double)Cs;
+    }
     RunSteps(t, 1);
 }
 
@@ -181,7 +191,7 @@ void Mesh::RunSteps(int t0, int n)
     if (!h_ || n <= 0) return;
     check(ippi_step(h_, n, t0), "ippi_step");
     last_t_ = t0 + n - 1;
-    synced_ = false;
+    synced_ = synced_f_ = false;
 }
 
 // Mesh::ComputeAvgVelocity (mesh.cpp:1954-1974): the running means of u, v
@@ -213,6 +223,7 @@ void Mesh::Sync(bool with_f)
                 for (int y = 0; y < ny_; y++)
                     for (int x = 0; x < nx_; x++)
                         LatMesh[x + 1][y].fnew[k] = (REAL)f[k * nn + (size_t)y * nx_ + x];
+        synced_f_ = true;
     }
     synced_ = true;
 }
@@ -556,7 +567,7 @@ void Mesh::reequilibrate_mirror()
         check(ippi_reequilibrate(h_, m.data(), m.data() + nn, m.data() + 2 * nn), "ippi_reequilibrate");
     else
         check(ippi_init_macros(h_, m.data(), m.data() + nn, m.data() + 2 * nn), "ippi_init_macros");
-    synced_ = false;
+    synced_ = synced_f_ = false;
 }
 
 // Mesh::ManageDataFromXflow (mesh.cpp:2189-2399): the imported rho, u and
@@ -763,7 +774,7 @@ int Mesh::LoadCheckpoint(const std::string& path)
     int last = -1;
     if (!check(ippi_load_state(h_, buf.data(), buf.size(), &last), "ippi_load_state")) return -1;
     last_t_ = last;
-    synced_ = false;
+    synced_ = synced_f_ = false;
     return last;
 }
 
@@ -799,3 +810,201 @@ void Mesh::LogMetrics(const std::string& path, int t, double mlups, double U, do
     out << ", \"max_u\": ";
     num(max_u) << ", \"tau_net_nodes\": " << net << ", \"tau_fallback_nodes\": " << fallback << "}\n";
 }
+
+// ---------------------------------------------------------------------------
+// sub-steps of the fused GPU step
+// ---------------------------------------------------------------------------
+void Mesh::fused_only(const char* what, const char* why)
+{
+    cerr << "Mesh::" << what << ": " << why << "; nothing was changed" << endl;
+    errorflag = 1;
+}
+
+static const char* kFused =
+    "runs inside OneLBMStep, whose one GPU launch pulls the populations, applies the boundary "
+    "rules, the immersed-boundary forcing and the collision together, so it cannot run on its own";
+
+void Mesh::Streaming(int RankID, int CoreNum)
+{
+    (void)RankID;
+    (void)CoreNum;
+    fused_only("Streaming", kFused);
+}
+void Mesh::BoundaryCondition(int RankID, int CoreNum)
+{
+    (void)RankID;
+    (void)CoreNum;
+    fused_only("BoundaryCondition", kFused);
+}
+void Mesh::SpreadForce(int RankID, int CoreNum, int Nx_P)
+{
+    (void)RankID;
+    (void)CoreNum;
+    (void)Nx_P;
+    fused_only("SpreadForce", kFused);
+}
+void Mesh::UpdateVelocity(int RankID, int CoreNum)
+{
+    (void)RankID;
+    (void)CoreNum;
+    fused_only("UpdateVelocity", kFused);
+}
+void Mesh::XflowBoundary(int t)
+{
+    (void)t;
+    fused_only("XflowBoundary",
+               "it overwrites the stored rho and u of non-fluid nodes, which the GPU step does not keep "
+               "(every step derives them from the populations)");
+}
+
+// ---------------------------------------------------------------------------
+// read-side IB and LES steps on the mirror
+// ---------------------------------------------------------------------------
+// Mesh::DiracDelta (mesh.cpp:1354-1385): Peskin's 4-point kernel
+REAL Mesh::DiracDelta(REAL x)
+{
+    const double a = std::fabs((double)x);
+    if (a < 1.0) return (REAL)((3.0 - 2.0 * a + std::sqrt(1.0 + 4.0 * a - 4.0 * a * a)) / 8.0);
+    if (a < 2.0) return (REAL)((5.0 - 2.0 * a - std::sqrt(-7.0 + 12.0 * a - 4.0 * a * a)) / 8.0);
+    return (REAL)0;
+}
+REAL Mesh::DiracDeltaD2Q9(REAL x, REAL y) { return DiracDelta(x) * DiracDelta(y); }
+REAL Mesh::GetDis2D(REAL x1, REAL y1, REAL x2, REAL y2)
+{
+    const double dx = (double)x2 - x1, dy = (double)y2 - y1;
+    return (REAL)std::sqrt(dx * dx + dy * dy);
+}
+double Mesh::ComputeDistance(double x0, double y0, double x1, double y1)
+{
+    const double dx = x1 - x0, dy = y1 - y0;
+    const double ex = x0 - center.x, ey = y0 - center.y;
+    const double len = std::sqrt(dx * dx + dy * dy);
+    if (len == 0.0) return std::sqrt(ex * ex + ey * ey);
+    return std::fabs(dx * ey - dy * ex) / len;
+}
+void Mesh::FilterLBM(int i, int j)
+{
+    (void)i;
+    (void)j;
+}
+bool Mesh::isAvailable(int i, int j)
+{
+    if (LatMesh.empty() || i < 0 || i >= (int)LatMesh.size() || j < 0 || j >= (int)LatMesh[0].size()) return false;
+    return LatMesh[i][j].style != 's';
+}
+
+// Mesh::InterpolateVel (mesh.cpp:552-655) for one rank: markers outside
+// [x of column 1, x of the last halo column) get 0; the stencil around
+// column (int)x + 1, row (int)y is 4 x 4 with Peskin's kernel or 2 x 2
+// bilinear
+void Mesh::InterpolateVel(int RankID, int CoreNum, int Nx_P)
+{
+    (void)RankID;
+    (void)CoreNum;
+    (void)Nx_P;
+    if (!h_ || LatMesh.empty()) return;
+    ensure_synced();
+    const int NX = (int)LatMesh.size(), NY = (int)LatMesh[0].size();
+    for (Particlenode& P : IBParticle) {
+        P.vel_ref = {0, 0};
+        if (P.position.x < LatMesh[1][0].pos.x || P.position.x >= LatMesh[NX - 1][0].pos.x) continue;
+        const int xi = (int)P.position.x + 1, yi = (int)P.position.y;
+        const bool peskin = DeltaKernel == IPPI_DELTA_PESKIN4;
+        const int lo = peskin ? -1 : 0, hi = peskin ? 2 : 1;
+        for (int X = xi + lo; X <= xi + hi; X++)
+            for (int Y = yi + lo; Y <= yi + hi; Y++) {
+                if (X < 0 || X >= NX || Y < 0 || Y >= NY) continue;
+                const Lattice& L = LatMesh[X][Y];
+                const REAL dx = P.position.x - L.pos.x, dy = P.position.y - L.pos.y;
+                const REAL w = peskin ? DiracDeltaD2Q9(dx, dy) : (REAL)((1 - std::fabs(dx)) * (1 - std::fabs(dy)));
+                P.vel_ref.x += L.u.x * w;
+                P.vel_ref.y += L.u.y * w;
+            }
+    }
+}
+
+// Mesh::CalParticleForce (mesh.cpp:514-531, direct forcing): F = 2 (U_b - U*),
+// without the area factor, as the reference
+void Mesh::CalParticleForce(int Radius)
+{
+    (void)Radius;
+    for (Particlenode& P : IBParticle) {
+        P.force.x = 2 * (P.vel.x - P.vel_ref.x);
+        P.force.y = 2 * (P.vel.y - P.vel_ref.y);
+    }
+}
+
+// Mesh::CaculateLESTau's active closure (SmagorinskyByHybrid, mesh.cpp
+// 852-911) for node (i, j) of the mirror: Pi = sum e e (fnew - feq),
+// S = -3 / (2 rho tau0) Pi, Q = sqrt(2 S:S),
+// tau = (sqrt(tau0^2 + 18 Cs^2 Q / rho) + tau0) / 2 with tau0 = startTau
+void Mesh::CaculateLESTau(int i, int j, REAL Cs, REAL Pr, int RankID, int CoreNum)
+{
+    (void)Pr;
+    (void)RankID;
+    (void)CoreNum;
+    if (!h_ || !isAvailable(i, j)) return;
+    if (!synced_f_) Sync(true);
+    Lattice& L = LatMesh[i][j];
+    const double rho = L.rho, ux = L.u.x, uy = L.u.y;
+    static const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1}, ey[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+    static const double w[9] = {4. / 9, 1. / 9, 1. / 9, 1. / 9, 1. / 9, 1. / 36, 1. / 36, 1. / 36, 1. / 36};
+    double pxx = 0, pxy = 0, pyy = 0;
+    for (int k = 0; k < 9; k++) {
+        const double eu = ex[k] * ux + ey[k] * uy;
+        const double feq = w[k] * rho * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * (ux * ux + uy * uy));
+        const double d = (double)L.fnew[k] - feq;
+        pxx += ex[k] * ex[k] * d;
+        pxy += ex[k] * ey[k] * d;
+        pyy += ey[k] * ey[k] * d;
+    }
+    const double tau0 = startTau > 0 ? startTau : (double)L.TauAtBeginning;
+    const double c = -3.0 / (2.0 * rho * tau0);
+    const double sxx = c * pxx, sxy = c * pxy, syy = c * pyy;
+    const double q = std::sqrt(2.0 * (sxx * sxx + 2.0 * sxy * sxy + syy * syy));
+    L.tau = (REAL)((std::sqrt(tau0 * tau0 + 18.0 * (double)Cs * Cs * q / rho) + tau0) / 2.0);
+}
+
+// Mesh::UpdateBoundary (mesh.cpp:1527-1534): each marker moves by its
+// interpolated velocity; the GPU step takes the new positions
+void Mesh::UpdateBoundary()
+{
+    if (IBParticle.empty()) return;
+    const int n = (int)IBParticle.size();
+    std::vector<double> xy(2 * (size_t)n), ub(2 * (size_t)n);
+    for (int m = 0; m < n; m++) {
+        Particlenode& P = IBParticle[m];
+        P.position.x += P.vel_ref.x;
+        P.position.y += P.vel_ref.y;
+        xy[2 * m] = P.position.x;
+        xy[2 * m + 1] = P.position.y;
+        ub[2 * m] = P.vel.x;
+        ub[2 * m + 1] = P.vel.y;
+    }
+    if (h_)
+        check(ippi_set_markers(h_, n, xy.data(), ub.data(), nullptr,
+                               marker_ds_.size() == (size_t)n ? marker_ds_.data() : nullptr),
+              "ippi_set_markers");
+}
+
+// ---------------------------------------------------------------------------
+// boundary nets: evaluated inside every step once loaded
+// ---------------------------------------------------------------------------
+int Mesh::nn_model(int type)
+{
+    if (!h_ || !net_loaded_[type]) {
+        cerr << "Mesh::NNmodel_Type0" << type << ": net AutoT0" << type
+             << " has no weights (LoadBandNet); its nodes use the Smagorinsky tau" << endl;
+        return -1;
+    }
+    Sync(false);  // tau and NNflag the next collision uses, nets included
+    return 0;
+}
+int Mesh::NNmodel_Type00(int t) { (void)t; return nn_model(0); }
+int Mesh::NNmodel_Type01(int t) { (void)t; return nn_model(1); }
+int Mesh::NNmodel_Type02(int t) { (void)t; return nn_model(2); }
+int Mesh::NNmodel_Type03(int t) { (void)t; return nn_model(3); }
+int Mesh::NNmodel_Type04(int t) { (void)t; return nn_model(4); }
+int Mesh::NNmodel_Type05(int t) { (void)t; return nn_model(5); }
+int Mesh::NNmodel_Type06(int t) { (void)t; return nn_model(6); }
+int Mesh::NNmodel_Type07(int t) { (void)t; return nn_model(7); }

@@ -100,6 +100,48 @@ public:
     void XflowABS(int t);
     void FindAndWriteTau(int i, int j, int t);
     void ChangeTauFromXflow(int t);
+    // The step's sub-steps (mesh.cpp:192-356, 656-832, 1244-1281, 2548-2584).
+    // OneLBMStep performs them in one fused launch on the GPU, so they cannot
+    // run on their own: each prints why on stderr, sets errorflag and
+    // changes nothing.
+    void Streaming(int RankID, int CoreNum);
+    void BoundaryCondition(int RankID, int CoreNum);
+    void SpreadForce(int RankID, int CoreNum, int Nx_P);
+    void UpdateVelocity(int RankID, int CoreNum);
+    void XflowBoundary(int t);
+    // Read-side IB and LES steps on the host mirror (the GPU step runs its
+    // own each step): InterpolateVel fills IBParticle[m].vel_ref from the
+    // current velocity field (Peskin 4-point or bilinear, as DeltaKernel),
+    // CalParticleForce sets IBParticle[m].force = 2 (vel - vel_ref), and
+    // CaculateLESTau sets LatMesh[i][j].tau to the Smagorinsky tau of the
+    // node's populations with the given Cs (mesh.cpp:514-655, 852-911)
+    void InterpolateVel(int RankID, int CoreNum, int Nx_P);
+    void CalParticleForce(int Radius);
+    void CaculateLESTau(int i, int j, REAL Cs, REAL Pr, int RankID, int CoreNum);
+    // moves each marker by its vel_ref and hands the new positions to the
+    // GPU step (mesh.cpp:1527-1534)
+    void UpdateBoundary();
+    // the Peskin 4-point kernel phi(x) and phi(x) phi(y) (mesh.cpp:1354-1389)
+    REAL DiracDelta(REAL x);
+    REAL DiracDeltaD2Q9(REAL x, REAL y);
+    REAL GetDis2D(REAL x1, REAL y1, REAL x2, REAL y2);
+    // distance from `center` to the line through (x0, y0) and (x1, y1); the
+    // reference's body (mesh.cpp:1536-1550) is unfinished and returns nothing
+    double ComputeDistance(double x0, double y0, double x1, double y1);
+    void FilterLBM(int i, int j);  // empty in the reference (mesh.cpp:2166-2169)
+    bool isAvailable(int i, int j);
+    // The boundary nets run inside every OneLBMStep once their weights are
+    // loaded (LoadBandNet).  NNmodel_Type0<n>(t) refreshes LatMesh's tau and
+    // NNflag from the GPU (the values the next collision uses) and returns
+    // 0, or returns -1 with a message when net n has no weights.
+    int NNmodel_Type00(int t);
+    int NNmodel_Type01(int t);
+    int NNmodel_Type02(int t);
+    int NNmodel_Type03(int t);
+    int NNmodel_Type04(int t);
+    int NNmodel_Type05(int t);
+    int NNmodel_Type06(int t);
+    int NNmodel_Type07(int t);
 
     // ---- additions ----------------------------------------------------
     // JudgeStyle marks the nodes within Radius of CylinderCenter1 as solid
@@ -143,6 +185,12 @@ private:
     std::vector<double> init_rho_, init_ux_, init_uy_;
     int cp_start_ = -1;
     std::vector<double> tau_field_;  // the tau-field model's tau[Ny][Nx]
+    std::vector<double> marker_ds_;  // arc length per marker (ippi_set_markers)
+    bool net_loaded_[8] = {};
+    bool synced_f_ = false;           // LatMesh fnew is current too
+    double cs_ = -1;                  // Smagorinsky constant on the device
+    void fused_only(const char* what, const char* why);
+    int nn_model(int type);
     void reequilibrate_mirror();
     void set_tau_node(int x, int y, double tau);
     void upload_tau_field();

@@ -113,6 +113,11 @@ class Lattice:
     def step(self, n=1, t0=1):
         L.check(L.lib().ippi_step(self._h, n, t0), self._h)
 
+    def set_les_cs(self, cs):
+        """Smagorinsky constant of the following steps (ippi_set_les_cs)."""
+        L.check(L.lib().ippi_set_les_cs(self._h, float(cs)), self._h)
+        self.params.cs = float(cs)
+
     def step_timed(self, n, t0=1):
         """step() with device timing: milliseconds between CUDA events on the
         handle's stream around the n steps, queued behind a short hold so

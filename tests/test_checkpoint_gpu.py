@@ -207,3 +207,68 @@ def test_learned_model_resume_and_bf16_storage():
     d.load_state(blob)
     d.step(80, 81)
     _same(_snapshot(c), _snapshot(d))
+
+
+def test_checkpoint_of_another_relaxation_time_setup_is_rejected():
+    """What sets the relaxation times is part of the configuration a
+    checkpoint presumes: a resume into a handle with another learned network
+    (statistics), another tau field, another wall distance or other boundary
+    nets is refused with IPPI_ERR_ARG, and the same setup is accepted."""
+    def rejected(lat, blob):
+        with pytest.raises(ip.IppiError, match="another configuration") as e:
+            lat.load_state(blob)
+        assert e.value.code == -1
+
+    a, _ = _learned()
+    a.step(10, 1)
+    blob = a.save_state()
+    rejected(_learned(lo=np.full(6, -1e6), hi=np.full(6, 1e6))[0], blob)
+    assert _learned()[0].load_state(blob) == 10
+
+    sc = scenes.cylinder_channel(NX, NY, 12, 40.3, 32.1, 0.05, 100, collision=ip.MRT, storage=ip.F64)
+    rng = np.random.default_rng(3)
+    t1 = 0.52 + 0.01 * rng.random((NY, NX))
+
+    def field(tau):
+        lat = ip.Lattice(NX, NY, **dict(sc["params"], les_model=ip.LES_FIELD))
+        lat.set_tau_field(tau)
+        lat.init_macros(*sc["init"])
+        return lat
+
+    f = field(t1)
+    f.step(10, 1)
+    blob = f.save_state()
+    rejected(field(t1 + 1e-3), blob)
+    assert field(t1).load_state(blob) == 10
+
+    d1 = np.tile(np.minimum(np.arange(NY) + 0.5, NY - np.arange(NY) - 0.5)[:, None], (1, NX))
+
+    def walled(d):
+        lat = ip.Lattice(NX, NY, **dict(sc["params"], les_model=ip.LES_DYNAMIC))
+        lat.set_wall_distance(d)
+        lat.init_macros(*sc["init"])
+        return lat
+
+    w = walled(d1)
+    w.step(10, 1)
+    blob = w.save_state()
+    rejected(walled(d1 * 1.5), blob)
+    assert walled(d1).load_state(blob) == 10
+
+    from conftest import GOLDEN
+    import os
+
+    net = np.fromfile(os.path.join(GOLDEN, "band_nets", "AutoT03.f32"), dtype=np.float32)
+
+    def plate(weights):
+        lat = ip.Lattice(416, 24, storage=ip.F64, tau0=0.52)
+        if weights is not None:
+            lat.load_band_net(3, weights)
+        return lat
+
+    p = plate(net)
+    p.step(5, 1)
+    blob = p.save_state()
+    rejected(plate(None), blob)
+    rejected(plate(net * np.float32(1.001)), blob)
+    assert plate(net).load_state(blob) == 5

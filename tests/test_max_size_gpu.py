@@ -3,7 +3,9 @@
 near the top-right corner (outlet and top wall) evolves for 20 steps; its
 neighbourhood must equal, bit for bit, the same bump in a 256 x 128 lattice,
 because every node runs the same arithmetic and nothing else reaches that
-corner in 20 steps.  One node more per row than the limit is refused."""
+corner in 20 steps.  At 16384 nodes per row the limit is 14563 rows
+(9 x 16384 x 14563 < 2^31 <= 9 x 16384 x 14564): that lattice is accepted
+and one row more is refused."""
 import numpy as np
 import pytest
 
@@ -36,5 +38,7 @@ def test_max_offset_lattice_matches_small_lattice_at_the_far_corner():
 
 
 def test_lattice_beyond_offset_limit_is_refused():
+    assert 9 * 16384 * 14563 < 2 ** 31 <= 9 * 16384 * 14564
     with pytest.raises(ip.IppiError, match="too large"):
-        ip.Lattice(16384, 14600, **P)  # 9 x 16384 x 14600 > 2^31
+        ip.Lattice(16384, 14564, **P)
+    ip.Lattice(16384, 14563, **P).close()

@@ -1,6 +1,6 @@
 """ippi_mass_noalloc: the mass checksum for callers that cannot allocate
-device memory (inside stream capture, under another allocator's ownership
-of the GPU's memory, in allocation-free loops).  It must give the mass that
+device memory (under another allocator's ownership of the GPU's memory, in
+allocation-free loops).  It must give the mass that
 ippi_forces() gives through a lattice handle, on two calls in a row (the
 second call reuses the library's fixed scratch array), and refuse fields
 taller than its scratch.
