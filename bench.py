@@ -761,6 +761,21 @@ def run_plate_ncu_case(a):
     print(json.dumps({"plate_ncu_case": f"flat_plate_{PLATE_NX}x{PLATE_NY}_nets_f32", "steps": a.steps}))
 
 
+def run_config2_seeds(a):
+    """Configuration 2 in FP32 and FP64 from --seeds noise seeds (MRT,
+    --validate-steps2 steps, statistics over the last 5/6 of them): one JSON
+    line with per-seed Cd, Cl, Cl rms and St and their spread."""
+    import torch
+
+    from ippi_lbm import validation as val
+
+    torch.cuda.set_device(0)
+    log = (lambda s_: print(s_, file=sys.stderr, flush=True))
+    steps = a.validate_steps2
+    r = val.config2_seeds(seeds=tuple(range(a.seeds)), steps=steps, avg=steps * 5 // 6, log=log)
+    print(json.dumps({"metric": "config2_seed_study", **r}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -785,6 +800,9 @@ def main():
                     help="precision studies of configs 2 and 3 instead of the MLUPS line")
     ap.add_argument("--validate-steps2", type=int, default=160000)
     ap.add_argument("--validate-steps3", type=int, default=20000)
+    ap.add_argument("--config2-seeds", action="store_true",
+                    help="configuration 2 in FP32 and FP64 over --seeds noise seeds")
+    ap.add_argument("--seeds", type=int, default=3)
     ap.add_argument("--config3-rate", action="store_true",
                     help="step rate of the 64-cylinder 16384x4096 lattice per storage")
     ap.add_argument("--learned-ncu-case", action="store_true",
@@ -807,6 +825,8 @@ def main():
         run_plate(a)
     elif a.config3_ncu_case:
         run_config3_ncu_case(a)
+    elif a.config2_seeds:
+        run_config2_seeds(a)
     elif a.plate_ncu_case:
         run_plate_ncu_case(a)
     elif a.adjoint_ncu_case:

@@ -11,7 +11,10 @@ object.  nvcc cross-compiles, so this runs without a GPU.
 
 Then the C++ host layer (host/: the reference's Mesh / Lattice classes and
 its main.cpp driver over the C ABI) is compiled with the host compiler into
-./ippi_main, linked against ./libippi_lbm.so.
+./ippi_main, linked against ./libippi_lbm.so, and the libtorch extension
+(torch_ext/ippi_autograd.cpp: torch::autograd::Function wrappers of the
+adjoint over the C ABI) into ./torch_ext/_build/ippi_autograd.so with
+torch.utils.cpp_extension, in-tree.
 """
 from __future__ import annotations
 
@@ -82,6 +85,7 @@ def build(force: bool = False, jobs: int | None = None) -> str:
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
     build_host(force)
+    build_torch_ext(force)
     return LIB
 
 
@@ -104,6 +108,28 @@ def build_host(force: bool = False) -> str:
     if r.returncode != 0:
         raise RuntimeError(f"host build failed:\n{r.stderr}")
     return MAIN
+
+
+TORCH_EXT = os.path.join(HERE, "torch_ext")
+TORCH_EXT_SO = os.path.join(TORCH_EXT, "_build", "ippi_autograd.so")
+
+
+def build_torch_ext(force: bool = False) -> str:
+    """torch_ext/_build/ippi_autograd.so: the libtorch extension (C++, no
+    device code of its own) linked against libippi_lbm.so."""
+    src = os.path.join(TORCH_EXT, "ippi_autograd.cpp")
+    deps = [src, LIB, os.path.join(REPO, "include", "ippi_lbm.h")]
+    if not force and os.path.exists(TORCH_EXT_SO) and os.path.getmtime(TORCH_EXT_SO) >= max(map(os.path.getmtime, deps)):
+        return TORCH_EXT_SO
+    from torch.utils import cpp_extension
+
+    bdir = os.path.dirname(TORCH_EXT_SO)
+    os.makedirs(bdir, exist_ok=True)
+    cpp_extension.load(name="ippi_autograd", sources=[src], build_directory=bdir, with_cuda=False,
+                       extra_cflags=["-O2"], extra_include_paths=[os.path.join(REPO, "include")],
+                       extra_ldflags=[f"-L{HERE}", "-lippi_lbm", f"-Wl,-rpath,{HERE}"], verbose=False)
+    os.utime(TORCH_EXT_SO, None)
+    return TORCH_EXT_SO
 
 
 if __name__ == "__main__":

@@ -602,60 +602,29 @@ __global__ void adj_ib_back3_kernel(const AdjArgs A, IbArgs I)
 }
 
 // ---- transposed streaming and boundaries -----------------------------------
-__device__ __forceinline__ void scatter_pull(const AdjArgs& A, int x, int y, const double* lam)
+// The pull maps (destination, direction) one to one onto (source, direction)
+// except at the lattice's edges, whose maps are folded into the destination
+// adjoint first (adj_edges_kernel, one thread per row):
+//   outlet  x = nx-1 pulls nothing: its f~ is the NEE of node nx-2 (f~ =
+//           feq(rho0, u_b) + f~_b - feq(rho_b, u_b)), so its adjoint is
+//           transposed onto node nx-2's and then cleared;
+//   inlet   x = 0: the regularised Zou-He map of the pulled populations is
+//           linear; its transposed Jacobian (one dual evaluation) replaces
+//           the node's adjoint;
+// and walls, where a pull from beyond y bounces back (the source is the node
+// itself, opposite direction).  adj_gather_kernel then writes every entry of
+// lam_in from exactly one term: no atomics, the same bits on every run.
+__global__ void __launch_bounds__(kT) adj_edges_kernel(const AdjArgs A)
 {
     const StepArgs& a = A.s;
     const long long nn = (long long)a.nx * a.ny;
+    const int y = blockIdx.x * kT + threadIdx.x;
+    if (y >= a.ny) return;
+    {
+        const long long node = (long long)y * a.nx + (a.nx - 1), b = node - 1;
+        double lam[9];
 #pragma unroll
-    for (int k = 0; k < 9; k++) {
-        if (lam[k] == 0.0) continue;
-        const int sx = x - EX(k), sy = y - EY(k);
-        if (sy < 0 || sy >= a.ny)
-            atomicAdd(A.lam_in + OPP(k) * nn + (long long)y * a.nx + x, lam[k]);
-        else if (sx >= 0)
-            atomicAdd(A.lam_in + k * nn + (long long)sy * a.nx + sx, lam[k]);
-    }
-}
-
-// transposed ch_fluid at (x, y): Zou-He (x = 0), then the pull
-__device__ __forceinline__ void fluid_back(const AdjArgs& A, int x, int y, double* lam)
-{
-    const StepArgs& a = A.s;
-    if (x == 0) {
-        // the regularised Zou-He inlet is linear in the pulled populations:
-        // its Jacobian from one dual evaluation, transposed onto lam
-        using D9 = Dual<9>;
-        D9 g[9];
-#pragma unroll
-        for (int k = 0; k < 9; k++) g[k] = D9::seed(0.0, k);
-        zh_inlet<D9>(g, D9(inlet_profile<double>(y, a.ny, a.u_in)), D9(0.0));
-        double lp[9];
-#pragma unroll
-        for (int j = 0; j < 9; j++) {
-            double v = 0.0;
-#pragma unroll
-            for (int k = 0; k < 9; k++) v += lam[k] * g[k].d[j];
-            lp[j] = v;
-        }
-#pragma unroll
-        for (int k = 0; k < 9; k++) lam[k] = lp[k];
-    }
-    scatter_pull(A, x, y, lam);
-}
-
-__global__ void __launch_bounds__(kT) adj_stream_kernel(const AdjArgs A)
-{
-    const StepArgs& a = A.s;
-    const long long nn = (long long)a.nx * a.ny;
-    const long long node = blockIdx.x * (long long)kT + threadIdx.x;
-    if (node >= nn) return;
-    const int x = (int)(node % a.nx), y = (int)(node / a.nx);
-    double lam[9];
-#pragma unroll
-    for (int k = 0; k < 9; k++) lam[k] = A.lam_ft[k * nn + node];
-    if (x == a.nx - 1) {
-        // NEE outlet: f~ = feq(rho0, ub) + fb - feq(rho_b, ub), fb = f~(nx-2, y)
-        const long long b = node - 1;
+        for (int k = 0; k < 9; k++) lam[k] = A.lam_ft[k * nn + node];
         const double rb = A.m[b], ux = A.m[nn + b], uy = A.m[2 * nn + b];
         const double r0 = a.rho0;
         double gr = 0.0, gx = 0.0, gy = 0.0;
@@ -669,12 +638,51 @@ __global__ void __launch_bounds__(kT) adj_stream_kernel(const AdjArgs A)
             gx += lam[k] * (r0 - rb) * w * (3.0 * EX(k) + 9.0 * eu * EX(k) - 3.0 * ux);
             gy += lam[k] * (r0 - rb) * w * (3.0 * EY(k) + 9.0 * eu * EY(k) - 3.0 * uy);
         }
-        double lb[9];
 #pragma unroll
-        for (int k = 0; k < 9; k++) lb[k] = lam[k] + gr + (gx * (EX(k) - ux) + gy * (EY(k) - uy)) / rb;
-        fluid_back(A, a.nx - 2, y, lb);
-    } else {
-        fluid_back(A, x, y, lam);
+        for (int k = 0; k < 9; k++) {
+            A.lam_ft[k * nn + b] += lam[k] + gr + (gx * (EX(k) - ux) + gy * (EY(k) - uy)) / rb;
+            A.lam_ft[k * nn + node] = 0.0;
+        }
+    }
+    {
+        const long long node = (long long)y * a.nx;
+        using D9 = Dual<9>;
+        D9 g[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) g[k] = D9::seed(0.0, k);
+        zh_inlet<D9>(g, D9(inlet_profile<double>(y, a.ny, a.u_in)), D9(0.0));
+        double lam[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) lam[k] = A.lam_ft[k * nn + node];
+#pragma unroll
+        for (int j = 0; j < 9; j++) {
+            double v = 0.0;
+#pragma unroll
+            for (int k = 0; k < 9; k++) v += lam[k] * g[k].d[j];
+            A.lam_ft[j * nn + node] = v;
+        }
+    }
+}
+
+// lam_in(x, y, j): the adjoint of the destination that pulled f_in_j(x, y) --
+// (x + e_j) when that is inside the lattice in y (nothing beyond x), else the
+// node itself in direction opp(j) (bounce-back)
+__global__ void __launch_bounds__(kT) adj_gather_kernel(const AdjArgs A)
+{
+    const StepArgs& a = A.s;
+    const long long nn = (long long)a.nx * a.ny;
+    const long long node = blockIdx.x * (long long)kT + threadIdx.x;
+    if (node >= nn) return;
+    const int x = (int)(node % a.nx), y = (int)(node / a.nx);
+#pragma unroll
+    for (int j = 0; j < 9; j++) {
+        const int dy = y + EY(j), dx = x + EX(j);
+        double v;
+        if (dy < 0 || dy >= a.ny)
+            v = A.lam_ft[OPP(j) * nn + node];
+        else
+            v = (dx >= 0 && dx < a.nx) ? A.lam_ft[j * nn + (long long)dy * a.nx + dx] : 0.0;
+        A.lam_in[j * nn + node] = v;
     }
 }
 
@@ -772,7 +780,8 @@ cudaError_t adj_ib_back(const AdjArgs& A, cudaStream_t st)
 cudaError_t adj_stream(const AdjArgs& A, cudaStream_t st)
 {
     const long long nn = (long long)A.s.nx * A.s.ny;
-    adj_stream_kernel<<<blocks(nn, kT), kT, 0, st>>>(A);
+    adj_edges_kernel<<<blocks(A.s.ny, kT), kT, 0, st>>>(A);
+    adj_gather_kernel<<<blocks(nn, kT), kT, 0, st>>>(A);
     return cudaGetLastError();
 }
 

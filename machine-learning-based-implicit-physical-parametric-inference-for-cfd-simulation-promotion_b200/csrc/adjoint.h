@@ -13,7 +13,8 @@
 //   adj_ib_back    transposed spreading and interpolation: lam of the marker
 //                  forces (plus the loss on the body forces) back to lam_f~
 //   adj_stream     lam_in = (d f~ / d f_in)^T lam_f~: transposed pull,
-//                  bounce-back, Zou-He inlet and NEE outlet
+//                  bounce-back, Zou-He inlet and NEE outlet, as a gather
+//                  (every lam_in entry written once; no atomics)
 #pragma once
 
 #include "lbm_kernels.cuh"
@@ -27,7 +28,7 @@ struct AdjArgs {
     double* m;           // [3][nn] rho, ux, uy of f~
     const double* lam_out;  // [9][nn] dL / d f_out
     double* lam_ft;      // [9][nn] dL / d f~
-    double* lam_in;      // [9][nn] dL / d f_in (accumulated by adj_stream)
+    double* lam_in;      // [9][nn] dL / d f_in (written by adj_stream)
     double* grad_tau;    // [nn] accumulated (tau field), or null
     double* xs;          // [nn][6] standardised features of learned nodes (else 0)
     double* up;          // [nn] dL / d softplus * out_scale of learned nodes (else 0)

@@ -2050,8 +2050,7 @@ int ippi_adjoint_backward(ippi_lbm* h, const double* dl_dforce, const double* dl
             if (e == cudaSuccess && dldm && s == nsteps - 1) e = adj_inject_moments(A, h->st);
             if (e == cudaSuccess && gmlp) e = mlp_grad_upstream_f64(A.xs, A.up, (int)nn, h->mlp_dev, part, gmlp, h->st);
             if (e == cudaSuccess && h->ib_active) e = adj_ib_back(A, h->st);
-            if (e == cudaSuccess) e = cudaMemsetAsync(lb, 0, 9 * nn * sizeof(double), h->st);
-            if (e == cudaSuccess) e = adj_stream(A, h->st);
+            if (e == cudaSuccess) e = adj_stream(A, h->st);  // writes every entry of lb
             if (e != cudaSuccess) rc = fail(h, IPPI_ERR_CUDA, "adjoint step %d: %s", s, cudaGetErrorString(e));
             std::swap(la, lb);
         }

@@ -12,13 +12,46 @@ forces is [nsteps][nbody][2] (body force of every step), macros [3][ny][nx]
 (rho, ux, uy of the last step's post-stream state).  `reset(lattice)` puts
 the lattice in the rollout's initial state before every forward pass (the
 gradient treats that state as fixed).
+
+The same Functions written in C++ against libtorch (torch_ext/ippi_autograd.cpp,
+torch::autograd::Function) are loaded by native():
+
+    ext = native()
+    roll = ext.tau_field_rollout(lattice.handle.value, nsteps, t0, ckpt_every, base_tau)
+    forces, macros = roll(tau)          # differentiable in tau
+    roll = ext.network_rollout(lattice.handle.value, nx, ny, nsteps, t0, ckpt_every, base_w, stats)
+    forces, macros = roll(w)            # differentiable in w
+
+where the starting state is the lattice's state when the rollout is made and
+base_tau / base_w the parameters in force then.
 """
 from __future__ import annotations
+
+import importlib.util
+import os
 
 import numpy as np
 import torch
 
 from . import _lib as L
+
+NATIVE_SO = os.path.join(L.PKG_DIR, "torch_ext", "_build", "ippi_autograd.so")
+_native = None
+
+
+def native():
+    """The libtorch extension (built in-tree by build.py); raises ImportError
+    when it has not been built."""
+    global _native
+    if _native is None:
+        if not os.path.exists(NATIVE_SO):
+            raise ImportError(f"{NATIVE_SO} is missing; run build.py")
+        L.lib()  # the C-ABI library the extension links against
+        spec = importlib.util.spec_from_file_location("ippi_autograd", NATIVE_SO)
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        _native = mod
+    return _native
 
 
 class Rollout:

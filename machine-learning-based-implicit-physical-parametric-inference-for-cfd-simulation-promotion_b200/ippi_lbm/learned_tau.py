@@ -217,14 +217,17 @@ def predict(net, x_raw, device=0, bf16=True):
 # ---------------------------------------------------------------------------
 # runs
 # ---------------------------------------------------------------------------
-def run_cylinder(sc, steps, avg_from, net=None, snapshot=None, device=0, chunk=2000):
+def run_cylinder(sc, steps, avg_from, net=None, snapshot=None, device=0, chunk=2000, means=False):
     """Run a cylinder scene (scenes.cylinder_channel dict) for `steps` steps;
     returns mean Cd / Cl over steps >= avg_from, the Strouhal number of Cl in
-    that window, the device wall time of the stepping, and the snapshots
-    taken by snapshot = (factor, first_step, stride, count)."""
+    that window, the device wall time of the stepping, the snapshots taken by
+    snapshot = (factor, first_step, stride, count), and with `means` the
+    time-averaged velocity [2][ny][nx] over the same window."""
     from .lattice import Lattice
 
     params = dict(sc["params"])
+    if means:
+        params["avg_start"] = avg_from
     if net is not None:
         params["les_model"] = L.LES_LEARNED
     lat = Lattice(sc["nx"], sc["ny"], device=device, **params)
@@ -252,13 +255,14 @@ def run_cylinder(sc, steps, avg_from, net=None, snapshot=None, device=0, chunk=2
         if end in marks:
             snaps.append(lat.filter_snapshot(snapshot[0]))
         t = end + 1
+    mean_u = np.stack([lat.download(L.FIELD_AVG_U), lat.download(L.FIELD_AVG_V)]) if means else None
     lat.close()
     q = 0.5 * sc["u_ref"] ** 2 * sc["d"]
     cd, cl = forces[:, 0] / q, forces[:, 1] / q
     win = slice(avg_from - 1, steps)
     return dict(cd=float(cd[win].mean()), cl=float(cl[win].mean()),
                 st=strouhal(cl[win], sc["d"], sc["u_ref"]), wall_s=wall,
-                cd_series=cd, cl_series=cl, snapshots=snaps)
+                cd_series=cd, cl_series=cl, snapshots=snaps, mean_u=mean_u)
 
 
 def strouhal(cl, d, u, pad=16):
@@ -281,34 +285,60 @@ def strouhal(cl, d, u, pad=16):
 # ---------------------------------------------------------------------------
 # the learned-tau experiment: fine plain run -> data -> training -> coarse runs
 # ---------------------------------------------------------------------------
-def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=160000,
-               avg_steps=64000, n_snap=200, max_samples=2_000_000, epochs=30, seed=0, device=0,
-               finetune_iters=0, finetune_lr=2e-3, calibrate=True, log=None):
-    """Fine lattice (plain Smagorinsky MRT, FP32) -> `n_snap` filtered
-    snapshots over its averaging window -> training -> the coarse lattice
-    (nx/factor x ny/factor, same Re and Mach) with plain Smagorinsky and with
-    the learned tau.  calibrate: the network's output scale is then fitted
-    to the fine run's drag (calibrate_scale) on the coarse scene started
-    from another noise seed (seed + 1) than the evaluation run; finetune_iters
-    adjoint iterations (train_through_solver) may follow.  Mean Cd / Cl and
-    St over the same physical window, and the device wall time of each
-    run."""
+def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=320000,
+               avg_steps=256000, n_snap=200, max_samples=2_000_000, epochs=30, seed=0, fine_seeds=(0, 1),
+               eval_seeds=(0, 1, 2), field_iters=120, field_lr=1e-3, wake_fit=True, wake_grid=(0.25, 1, 4, 16, 64),
+               wake_iters=4, ladder=(48, 64, 96), finetune_iters=0, finetune_lr=2e-3, calibrate_drag=False,
+               device=0, log=None):
+    """The learned-tau experiment.
+
+    1. Fine lattice (nx x ny, cylinder D = d, plain Smagorinsky MRT, FP32),
+       one run per seed of `fine_seeds`: their mean drag over the last
+       `avg_steps` steps is the reference, their spread the noise floor of
+       that window.  The first run also gives `n_snap` filtered snapshots
+       (factor x factor boxes) and its time-averaged velocity.
+    2. A priori: the network fitted to the eddy viscosity that carries the
+       filtered stress (samples_from_snapshot, train).
+    3. Through the solver on the filtered field: train_on_field_pairs on
+       consecutive snapshots (the drag is never a target).
+    4. Optionally the output scale fitted to the fine run's time-averaged
+       near-wake velocity (fit_scale_to_wake, on another noise seed), a
+       quantity other than the judged drag.
+    5. Each network and plain Smagorinsky on the coarse lattice (nx/factor x
+       ny/factor, same Re and Mach) over the same physical window, for every
+       seed of `eval_seeds`: mean drag, its spread, St, device wall time.
+    6. Plain Smagorinsky on a ladder of resolutions (cylinder diameters in
+       `ladder`, same physical window): drag error against wall time, so the
+       time plain Smagorinsky needs for a learned run's drag error can be read
+       off (time_at_error).
+    calibrate_drag / finetune_iters keep the earlier routes (output scale, or
+    adjoint fine-tuning, fitted to the fine drag itself) for comparison; they
+    fit the judged quantity and are off by default."""
     from . import scenes
 
-    say = log or (lambda s: None)
+    say = log or (lambda s_: None)
     cx, cy = nx / 4, ny / 2
-    fine = scenes.cylinder_channel(nx, ny, d, cx, cy, u, re, seed=seed)
     first = fine_steps - avg_steps + 1
     stride = max(avg_steps // n_snap, 1)
-    say(f"fine {nx}x{ny}: {fine_steps} steps, snapshots every {stride} from {first}")
-    rf = run_cylinder(fine, fine_steps, first, snapshot=(factor, first + stride - 1, stride, n_snap),
-                      device=device)
-    say(f"fine: Cd {rf['cd']:.5f} St {rf['st']:.4f} wall {rf['wall_s']:.2f} s")
+    fines = []
+    for k, fs in enumerate(fine_seeds):
+        fine = scenes.cylinder_channel(nx, ny, d, cx, cy, u, re, seed=fs)
+        snap = (factor, first + stride - 1, stride, n_snap) if k == 0 else None
+        r = run_cylinder(fine, fine_steps, first, snapshot=snap, device=device, means=(k == 0))
+        fines.append(r)
+        say(f"fine {nx}x{ny} seed {fs}: Cd {r['cd']:.5f} St {r['st']:.4f} wall {r['wall_s']:.2f} s")
+    rf = fines[0]
+    cd_ref = float(np.mean([r["cd"] for r in fines]))
+    fine_spread = float(np.std([r["cd"] for r in fines], ddof=1) / cd_ref) if len(fines) > 1 else None
     mx, my, dc = nx // factor, ny // factor, d / factor
-    coarse = scenes.cylinder_channel(mx, my, dc, cx / factor, cy / factor, u, re, seed=seed)
-    tau0c = coarse["params"]["tau0"]
-    mask = cylinder_mask(mx, my, cx / factor, cy / factor, dc)
-    xs, ys = zip(*(samples_from_snapshot(s, tau0c, mask) for s in rf["snapshots"]))
+    ccx, ccy = cx / factor, cy / factor
+
+    def coarse(sd):
+        return scenes.cylinder_channel(mx, my, dc, ccx, ccy, u, re, seed=sd)
+
+    tau0c = coarse(seed)["params"]["tau0"]
+    mask = cylinder_mask(mx, my, ccx, ccy, dc)
+    xs, ys = zip(*(samples_from_snapshot(s_, tau0c, mask) for s_ in rf["snapshots"]))
     x, y = np.concatenate(xs), np.concatenate(ys)
     rng = np.random.default_rng(seed)
     if x.shape[0] > max_samples:
@@ -317,53 +347,84 @@ def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=
     t0 = time.perf_counter()
     net, hist = train(x, y, epochs=epochs, seed=seed, device=device, log=log)
     train_s = time.perf_counter() - t0
-    say(f"trained on {x.shape[0]} samples in {train_s:.1f} s, loss {hist[0]:.4g} -> {hist[-1]:.4g}")
+    say(f"a priori: {x.shape[0]} samples in {train_s:.1f} s, loss {hist[0]:.4g} -> {hist[-1]:.4g}")
     csteps, cfirst = fine_steps // factor, (fine_steps - avg_steps) // factor + 1
-    rp = run_cylinder(coarse, csteps, cfirst, device=device)
-    rl = run_cylinder(coarse, csteps, cfirst, net=net, device=device)
-    say(f"coarse plain: Cd {rp['cd']:.5f}; learned (a priori): Cd {rl['cd']:.5f}")
-    a_priori, cal = rl, None
-    if calibrate:
+
+    def evaluate(n, name):
+        runs = [run_cylinder(coarse(sd), csteps, cfirst, net=n, device=device) for sd in eval_seeds]
+        cds = [r["cd"] for r in runs]
+        out = dict(cd=float(np.mean(cds)), cd_per_seed=cds,
+                   cd_spread=float(np.std(cds, ddof=1) / np.mean(cds)) if len(cds) > 1 else None,
+                   st=runs[0]["st"], wall_s=float(np.mean([r["wall_s"] for r in runs])))
+        out["cd_rel_err"] = abs(out["cd"] - cd_ref) / abs(cd_ref)
+        say(f"coarse {name}: Cd {out['cd']:.5f} (error {100 * out['cd_rel_err']:.1f} %) St {out['st']:.4f}")
+        return out
+
+    res = dict(fine=dict(nx=nx, ny=ny, steps=fine_steps, avg_steps=avg_steps, cd=cd_ref,
+                         cd_per_seed=[r["cd"] for r in fines], cd_seed_spread=fine_spread, st=rf["st"],
+                         wall_s=rf["wall_s"]),
+               coarse=dict(nx=mx, ny=my, steps=csteps, seeds=list(eval_seeds)),
+               training=dict(samples=int(x.shape[0]), epochs=epochs, loss_first=hist[0], loss_last=hist[-1],
+                             seconds=train_s))
+    res["plain"] = evaluate(None, "plain Smagorinsky")
+    res["a_priori"] = evaluate(net, "learned, a priori")
+    nets = {"a_priori": net}
+    if field_iters:
+        horizon = max(stride // factor, 1)
+        pairs = list(zip(rf["snapshots"][:-1], rf["snapshots"][1:]))
         t1 = time.perf_counter()
-        other = scenes.cylinder_channel(mx, my, dc, cx / factor, cy / factor, u, re, seed=seed + 1)
-        net_c, cal_hist = calibrate_scale(net, other, rf["cd"], csteps, cfirst, device=device, log=log)
-        cal_s = time.perf_counter() - t1
-        cal = dict(scale=net_c.out_scale / net.out_scale, runs=len(cal_hist), seconds=cal_s,
-                   history=[dict(scale=a, cd=b) for a, b in cal_hist])
-        net = net_c
-        rl = run_cylinder(coarse, csteps, cfirst, net=net, device=device)
-        say(f"coarse learned, output scale x{cal['scale']:.4g}: Cd {rl['cd']:.5f}")
-    tuned = None
+        net_f, fh = train_on_field_pairs(net, coarse(seed), pairs, horizon, iters=field_iters, lr=field_lr,
+                                         device=device, log=log, seed=seed)
+        res["field_training"] = dict(iters=field_iters, horizon=horizon, pairs=len(pairs), lr=field_lr,
+                                     seconds=time.perf_counter() - t1, loss_first=fh[0]["loss"],
+                                     loss_last=float(np.mean([h["loss"] for h in fh[-10:]])))
+        res["through_solver_field"] = evaluate(net_f, "learned, trained through the solver on the field")
+        nets["through_solver_field"] = net_f
+    if wake_fit:
+        ref_u = box_filter(rf["mean_u"], factor)
+        t1 = time.perf_counter()
+        net_w, wh = fit_scale_to_wake(net, coarse(seed + 100), ref_u, csteps, cfirst, grid=wake_grid,
+                                      iters=wake_iters, device=device, log=log)
+        res["wake_fit"] = dict(scale=net_w.out_scale / net.out_scale, runs=len(wh),
+                               seconds=time.perf_counter() - t1,
+                               history=[dict(scale=a_, wake_l2=b_, cd=c_) for a_, b_, c_ in wh])
+        res["a_priori_wake_scale"] = evaluate(net_w, "learned, scale fitted to the wake velocity")
+        nets["a_priori_wake_scale"] = net_w
+    if calibrate_drag:
+        net_c, ch = calibrate_scale(net, coarse(seed + 1), cd_ref, csteps, cfirst, device=device, log=log)
+        res["drag_fitted_scale"] = evaluate(net_c, "learned, scale fitted to the fine drag")
+        res["drag_fitted_scale"]["scale"] = net_c.out_scale / net.out_scale
     if finetune_iters:
-        t1 = time.perf_counter()
-        net_ft, ft_hist = train_through_solver(net, coarse, rf["cd"], iters=finetune_iters,
-                                               spinup=cfirst - 1, lr=finetune_lr, device=device, log=log)
-        ft_s = time.perf_counter() - t1
-        rt = run_cylinder(coarse, csteps, cfirst, net=net_ft, device=device)
-        say(f"coarse learned + through-solver training: Cd {rt['cd']:.5f}")
-        tuned = dict(cd=rt["cd"], st=rt["st"], wall_s=rt["wall_s"],
-                     cd_rel_err=abs(rt["cd"] - rf["cd"]) / abs(rf["cd"]), iters=finetune_iters,
-                     train_seconds=ft_s, history=ft_hist)
-        net = net_ft
-
-    def err(r):
-        return abs(r["cd"] - rf["cd"]) / abs(rf["cd"])
-
-    return dict(
-        fine=dict(nx=nx, ny=ny, steps=fine_steps, cd=rf["cd"], cl=rf["cl"], st=rf["st"],
-                  wall_s=rf["wall_s"]),
-        coarse_plain=dict(nx=mx, ny=my, steps=csteps, cd=rp["cd"], st=rp["st"], wall_s=rp["wall_s"],
-                          cd_rel_err=err(rp)),
-        coarse_learned=dict(nx=mx, ny=my, steps=csteps, cd=rl["cd"], st=rl["st"], wall_s=rl["wall_s"],
-                            cd_rel_err=err(rl)),
-        coarse_learned_a_priori=dict(cd=a_priori["cd"], st=a_priori["st"], wall_s=a_priori["wall_s"],
-                                     cd_rel_err=err(a_priori)),
-        calibration=cal,
-        training=dict(samples=int(x.shape[0]), epochs=epochs, loss_first=hist[0], loss_last=hist[-1],
-                      seconds=train_s),
-        coarse_learned_through_solver=tuned,
-        speedup_vs_fine=rf["wall_s"] / rl["wall_s"],
-        net=net)
+        net_t, th = train_through_solver(nets.get("a_priori_wake_scale", net), coarse(seed), cd_ref,
+                                         iters=finetune_iters, spinup=cfirst - 1, lr=finetune_lr, device=device,
+                                         log=log)
+        res["drag_finetuned"] = evaluate(net_t, "learned, adjoint fine-tuning on the fine drag")
+        res["drag_finetuned"]["iters"] = finetune_iters
+    # plain Smagorinsky on a ladder of resolutions over the same physical window
+    points = [(0.0, rf["wall_s"]), (res["plain"]["cd_rel_err"], res["plain"]["wall_s"])]
+    res["ladder"] = []
+    for dl in ladder:
+        f_ = d / dl
+        lx, ly = int(round(nx / f_)), int(round(ny / f_))
+        lsteps, lfirst = int(round(fine_steps / f_)), int(round((fine_steps - avg_steps) / f_)) + 1
+        r = run_cylinder(scenes.cylinder_channel(lx, ly, dl, cx / f_, cy / f_, u, re, seed=seed), lsteps, lfirst,
+                         device=device)
+        e = abs(r["cd"] - cd_ref) / abs(cd_ref)
+        res["ladder"].append(dict(d=dl, nx=lx, ny=ly, steps=lsteps, cd=r["cd"], cd_rel_err=e, wall_s=r["wall_s"]))
+        points.append((e, r["wall_s"]))
+        say(f"plain D = {dl} ({lx}x{ly}): Cd {r['cd']:.5f} (error {100 * e:.1f} %), {r['wall_s']:.2f} s")
+    res["time_to_solution"] = {}
+    for name in ("a_priori", "through_solver_field", "a_priori_wake_scale"):
+        if name not in res:
+            continue
+        v = res[name]
+        t_plain = time_at_error(points, v["cd_rel_err"])
+        res["time_to_solution"][name] = dict(
+            cd_rel_err=v["cd_rel_err"], plain_wall_at_equal_error=t_plain, learned_wall=v["wall_s"],
+            ratio=None if t_plain is None else t_plain / v["wall_s"])
+    res["speedup_vs_fine"] = rf["wall_s"] / res["plain"]["wall_s"]
+    res["nets"] = nets
+    return res
 
 
 # ---------------------------------------------------------------------------
@@ -502,3 +563,156 @@ def train_through_solver(net, sc, cd_ref, iters=8, nsteps=4000, ckpt=64, spinup=
     lat.close()
     out = TauNet(wd.cpu().numpy(), net.mean, net.std, net.lo, net.hi, net.out_scale)
     return out, hist
+
+
+# ---------------------------------------------------------------------------
+# training through the solver on the filtered fine field (solver in the loop)
+# ---------------------------------------------------------------------------
+def box_filter(field, factor):
+    """Mean over factor x factor blocks of [..., ny][nx] arrays."""
+    a = np.asarray(field, dtype=np.float64)
+    ny, nx = a.shape[-2] // factor, a.shape[-1] // factor
+    a = a[..., :ny * factor, :nx * factor]
+    return a.reshape(*a.shape[:-2], ny, factor, nx, factor).mean(axis=(-3, -1))
+
+
+def train_on_field_pairs(net, sc, pairs, horizon, iters=120, lr=1e-3, ckpt=32, device=0, log=None,
+                         seed=0):
+    """Fine-tune the network through the coarse solver on short rollouts (the
+    "solver in the loop" of learned-correction training): each iteration
+    starts the coarse lattice `sc` at the equilibrium of one filtered fine
+    snapshot's moments, runs `horizon` coarse steps with the learned tau, and
+    takes the loss
+        sum_mask |u(horizon) - u_target|^2 / sum_mask |u_target|^2
+    against the filtered fine snapshot `horizon` coarse steps later (mask:
+    cylinder_mask, away from the edges and the IB band).  The gradient with
+    respect to the FP32 weights is the library's adjoint (checkpoints every
+    `ckpt` steps), the update the library's Adam kernel.  The drag is never a
+    target.  Before training the network's input range is widened to the
+    features of the rollouts' states, so that the nodes the loss sees are
+    not outside it (Smagorinsky fallback, no gradient).  pairs: list of
+    (snapshot, snapshot `horizon` coarse steps later), each [6][ny][nx] as
+    Lattice.filter_snapshot returns.  Returns (net, per-iteration history)."""
+    import torch
+
+    from .lattice import Lattice
+
+    nx, ny = sc["nx"], sc["ny"]
+    params = dict(sc["params"], les_model=L.LES_LEARNED)
+    mask = cylinder_mask(nx, ny, sc["markers"][:, 0].mean(), sc["markers"][:, 1].mean(), sc["d"])
+    lat = Lattice(nx, ny, device=device, **params)
+    lat.set_markers(sc["markers"], ds=sc["ds"])
+    # the features the rollouts visit (a few steps in, from three snapshots)
+    lo, hi = net.lo.copy(), net.hi.copy()
+    for s0, _ in pairs[:: max(len(pairs) // 3, 1)][:3]:
+        lat.init_macros(s0[0], s0[1], s0[2])
+        lat.load_tau_mlp_f32(net.w.astype(np.float32), net.stats())
+        lat.step(horizon // 2, 1)
+        x = state_features(lat, params["tau0"])
+        lo, hi = np.minimum(lo, x.min(0)), np.maximum(hi, x.max(0))
+    span = hi - lo
+    net = TauNet(net.w, net.mean, net.std, (lo - 0.1 * span).astype(np.float32),
+                 (hi + 0.1 * span).astype(np.float32), net.out_scale)
+    stats = net.stats()
+    dev = torch.device("cuda", device)
+    wd = torch.from_numpy(net.w.astype(np.float32)).to(dev)
+    md, vd, gd = torch.zeros_like(wd), torch.zeros_like(wd), torch.zeros_like(wd)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    lib = L.lib()
+    rng = np.random.default_rng(seed + 7)
+    order = rng.permutation(len(pairs))
+    hist = []
+    m = mask.astype(np.float64)
+    for it in range(iters):
+        s0, s1 = pairs[order[it % len(pairs)]]
+        t0 = time.perf_counter()
+        lat.init_macros(s0[0], s0[1], s0[2])
+        lat.load_tau_mlp_f32(wd.cpu().numpy(), stats)
+        lat.adjoint_forward(horizon, 1, ckpt)
+        ux, uy = lat.download(L.FIELD_UX), lat.download(L.FIELD_UY)
+        den = float(np.sum(m * (s1[1] ** 2 + s1[2] ** 2)))
+        ex, ey = ux - s1[1], uy - s1[2]
+        loss = float(np.sum(m * (ex * ex + ey * ey))) / den
+        dm = np.stack([np.zeros_like(ux), 2.0 * m * ex / den, 2.0 * m * ey / den])
+        g = lat.adjoint_backward(dl_dmacro=dm, mlp=True)["mlp"]
+        gd.copy_(torch.from_numpy(g.astype(np.float32)))
+        L.check(lib.ippi_mlp_adam(wd.data_ptr(), gd.data_ptr(), md.data_ptr(), vd.data_ptr(), it + 1, lr,
+                                  0.9, 0.999, 1e-8, stream))
+        torch.cuda.synchronize(dev)
+        hist.append(dict(loss=loss, seconds=time.perf_counter() - t0))
+        if log and (it % 10 == 0 or it == iters - 1):
+            log(f"field training {it}: loss {loss:.5g} ({hist[-1]['seconds']:.2f} s)")
+    lat.close()
+    return TauNet(wd.cpu().numpy(), net.mean, net.std, net.lo, net.hi, net.out_scale), hist
+
+
+# ---------------------------------------------------------------------------
+# an output scale fitted to the wake's mean velocity (not to the drag)
+# ---------------------------------------------------------------------------
+def wake_mask(nx, ny, cx, cy, d):
+    """Cells of the near wake: x from the cylinder's rear + 1 to 6 D behind
+    its centre, |y - cy| < 1.5 D."""
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    return (xx + 0.5 > cx + 0.5 * d + 1) & (xx + 0.5 < cx + 6 * d) & (np.abs(yy + 0.5 - cy) < 1.5 * d)
+
+
+def fit_scale_to_wake(net, sc, mean_u_ref, steps, avg_from, grid=(0.25, 1, 4, 16, 64), iters=4, device=0,
+                      log=None):
+    """Fit the network's output scale so that the coarse lattice's
+    time-averaged velocity in the near wake (wake_mask) comes closest, in L2,
+    to mean_u_ref [2][ny][nx] (the fine run's time average, box-filtered to
+    the coarse grid).  Forward runs of `sc`: the scales of `grid`, then a
+    golden-section search of log(scale) between the best grid point's
+    neighbours.  Returns (net with the best scale, [(scale, wake L2, Cd)]).
+    The drag of each run is recorded, not used."""
+    cx, cy = sc["markers"][:, 0].mean(), sc["markers"][:, 1].mean()
+    m = wake_mask(sc["nx"], sc["ny"], cx, cy, sc["d"])
+    ref = np.asarray(mean_u_ref)[:, m]
+    hist = []
+
+    def err(x):
+        n = TauNet(net.w, net.mean, net.std, net.lo, net.hi, net.out_scale * math.exp(x))
+        r = run_cylinder(sc, steps, avg_from, net=n, device=device, means=True)
+        e = float(np.sqrt(np.sum((r["mean_u"][:, m] - ref) ** 2) / np.sum(ref ** 2)))
+        hist.append((math.exp(x), e, r["cd"]))
+        if log:
+            log(f"wake fit: scale {math.exp(x):.4g} -> wake L2 {e:.4g} (Cd {r['cd']:.4f})")
+        return e
+
+    xs = [math.log(g) for g in grid]
+    es = [err(x) for x in xs]
+    k = int(np.argmin(es))
+    a, b = xs[max(k - 1, 0)], xs[min(k + 1, len(xs) - 1)]
+    r = (math.sqrt(5.0) - 1.0) / 2.0
+    c, d = b - r * (b - a), a + r * (b - a)
+    ec, ed = err(c), err(d)
+    for _ in range(max(iters - 2, 0)):
+        if ec < ed:
+            b, d, ed = d, c, ec
+            c = b - r * (b - a)
+            ec = err(c)
+        else:
+            a, c, ec = c, d, ed
+            d = a + r * (b - a)
+            ed = err(d)
+    best = min(hist, key=lambda h: h[1])
+    return TauNet(net.w, net.mean, net.std, net.lo, net.hi, net.out_scale * best[0]), hist
+
+
+# ---------------------------------------------------------------------------
+# time to solution at equal drag error
+# ---------------------------------------------------------------------------
+def time_at_error(points, err):
+    """Wall time plain Smagorinsky needs for a drag error `err`, from
+    (error, wall seconds) points of a resolution ladder (the fine reference
+    itself as error 0): log(time) interpolated linearly in the error between
+    the two ladder points that bracket it.  None when `err` is larger than
+    every ladder point's error (the coarsest plain run is already as good)."""
+    pts = sorted(points, key=lambda p: p[0])
+    if err >= pts[-1][0]:
+        return None
+    for (e0, t0), (e1, t1) in zip(pts, pts[1:]):
+        if e0 <= err <= e1:
+            w = 0.0 if e1 == e0 else (err - e0) / (e1 - e0)
+            return math.exp((1 - w) * math.log(t0) + w * math.log(t1))
+    return pts[0][1]

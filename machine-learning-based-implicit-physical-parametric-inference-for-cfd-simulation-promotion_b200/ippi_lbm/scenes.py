@@ -61,10 +61,11 @@ def config1():
                             les=False)
 
 
-def config2(collision=L.MRT, storage=L.F32):
-    """4096x1024, D = 128 at (1024, 512), Re 3900, u_max 0.04, Smagorinsky Cs 0.1."""
+def config2(collision=L.MRT, storage=L.F32, seed=0):
+    """4096x1024, D = 128 at (1024, 512), Re 3900, u_max 0.04, Smagorinsky Cs 0.1
+    (initial noise from `seed`)."""
     return cylinder_channel(4096, 1024, 128, 1024, 512, 0.04, 3900, collision=collision,
-                            storage=storage, cs=0.1)
+                            storage=storage, cs=0.1, seed=seed)
 
 
 def drag_lift(force_xy, d, u_ref, rho0=1.0):

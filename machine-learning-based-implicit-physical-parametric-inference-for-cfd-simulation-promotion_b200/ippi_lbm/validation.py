@@ -72,6 +72,43 @@ def config2_precision(steps=160000, avg=64000, collisions=(L.MRT, L.RR), log=Non
     return out
 
 
+def config2_seeds(seeds=(0, 1, 2), steps=480000, avg=400000, collision=L.MRT, log=None):
+    """Configuration 2 (4096 x 1024, D = 128, Re 3900, MRT + Smagorinsky) in
+    FP32 and FP64 from several seeds of the +-1e-4 initial noise: per seed and
+    precision the mean Cd, mean Cl, Cl rms and St over the last `avg` steps.
+    The wake is chaotic, so the FP32-FP64 difference of one seed is set
+    against the spread between seeds of the same precision."""
+    per = {"f32": [], "f64": []}
+    for seed in seeds:
+        for st, name in ((L.F64, "f64"), (L.F32, "f32")):
+            sc = scenes.config2(collision=collision, storage=st, seed=seed)
+            r = _run(sc["nx"], sc["ny"], sc["params"], sc["init"], sc["markers"], sc["ds"], None, steps,
+                     steps - avg + 1)
+            q = 0.5 * sc["u_ref"] ** 2 * sc["d"]
+            f = r["forces"][steps - avg:, 0] / q
+            rec = dict(seed=int(seed), cd=float(f[:, 0].mean()), cl=float(f[:, 1].mean()),
+                       cl_rms=float(f[:, 1].std()), st=strouhal(f[:, 1], sc["d"], sc["u_ref"]),
+                       wall_s=r["wall_s"])
+            per[name].append(rec)
+            if log:
+                log(f"config2 seed {seed} {name}: Cd {rec['cd']:.5f} Cl {rec['cl']:+.4f} St {rec['st']:.4f} "
+                    f"({r['wall_s']:.1f} s)")
+
+    def spread(v):
+        v = np.asarray(v, dtype=np.float64)
+        return dict(mean=float(v.mean()), std=float(v.std(ddof=1)) if len(v) > 1 else 0.0,
+                    min=float(v.min()), max=float(v.max()))
+
+    out = dict(steps=steps, avg=avg, seeds=[int(s) for s in seeds], runs=per)
+    for name in ("f32", "f64"):
+        out[name] = {k: spread([r[k] for r in per[name]]) for k in ("cd", "cl", "cl_rms", "st")}
+    gaps = [abs(a["cd"] - b["cd"]) / b["cd"] for a, b in zip(per["f32"], per["f64"])]
+    out["cd_f32_vs_f64_same_seed"] = dict(per_seed=gaps, mean=float(np.mean(gaps)))
+    out["cd_seed_spread_f64"] = out["f64"]["cd"]["std"] / out["f64"]["cd"]["mean"]
+    out["cd_mean_f32_vs_f64"] = abs(out["f32"]["cd"]["mean"] - out["f64"]["cd"]["mean"]) / out["f64"]["cd"]["mean"]
+    return out
+
+
 def seeded_cylinders(nx, ny, d, n, gap, seed=0, margin=None):
     """n non-overlapping cylinder centres (centre distance >= d + gap), at
     least `margin` from the lattice edges (default 2 d) and from the inlet

@@ -116,6 +116,32 @@ def test_network_weight_gradient_matches_finite_differences():
         assert abs(fd - want) <= 2e-5 * max(abs(fd), 1e-12), (fd, want)
 
 
+def test_backward_sweep_is_bit_reproducible():
+    """The transposed streaming is a gather (each dL/df_in entry written once,
+    no atomics) and every other reduction has a fixed order: two backward
+    sweeps of the same rollout give the same bits, for the tau field and the
+    network weights, on a channel whose outlet and inlet columns carry
+    adjoint."""
+    nx, ny, nsteps = 64, 32, 25
+    sc, p, rng = setup(nx, ny, ip.MRT, ip.LES_LEARNED, seed=4)
+    w = (tm.xavier_init(7) + rng.normal(0, 0.1, tm.NPARAM)).astype(np.float32)
+    stats = np.concatenate([[1.0, 0.03, 0, 0, 0, 5e-3], [2e-3, 0.02, 0.5, 0.5, 0.5, 5e-3],
+                            [0.9, 0.0, -1, -1, -1, 0.0], [1.1, 0.2, 1, 1, 1, 0.2],
+                            [0.02]]).astype(np.float32)
+    a, b = loss_weights(rng, nsteps, nx, ny)
+    runs = [run_gpu(sc, p, nsteps, a, b, w=w, stats=stats, grads=dict(mlp=True, f0=True))[1] for _ in range(2)]
+    assert np.abs(runs[0]["mlp"]).max() > 0
+    for k in ("mlp", "f0"):
+        assert np.array_equal(runs[0][k], runs[1][k]), k
+    # the edge columns carry adjoint (the inlet's and outlet's transposes ran)
+    f0 = runs[0]["f0"].reshape(9, ny, nx)
+    assert np.abs(f0[:, :, 0]).max() > 0 and np.abs(f0[:, :, nx - 2]).max() > 0
+    sc, p, rng = setup(nx, ny, ip.RR, ip.LES_FIELD, seed=5)
+    tau = 0.56 + smooth_field(rng, ny, nx, 0.01)
+    runs = [run_gpu(sc, p, nsteps, a, b, tau=tau, grads=dict(tau=True))[1]["tau"] for _ in range(2)]
+    assert np.abs(runs[0]).max() > 0 and np.array_equal(runs[0], runs[1])
+
+
 def test_gradient_matches_fp64_oracle_on_128x64_200_steps():
     """The adjoint's directional derivatives against central differences of
     the FP64 CPU oracle (an independent forward implementation)."""
