@@ -217,17 +217,20 @@ def test_pipeline_small_end_to_end():
 def test_experiment_driver_small():
     """The learned-tau experiment driver end to end on a small channel (the
     code path behind the bench's learned mode): fine run, filtered snapshots,
-    training, the coarse plain and learned runs and one through-solver
-    iteration, with every reported figure finite."""
+    a-priori training, training through the solver on the filtered field,
+    the wake-velocity scale fit, the coarse runs and the plain resolution
+    ladder, with every reported figure finite."""
     r = lt.experiment(nx=512, ny=128, d=32, u=0.05, re=300.0, fine_steps=2000, avg_steps=800,
-                      n_snap=10, epochs=3, finetune_iters=1)
-    for k in ("fine", "coarse_plain", "coarse_learned"):
+                      n_snap=10, epochs=3, fine_seeds=(0, 1), eval_seeds=(0, 1), field_iters=2,
+                      wake_grid=(1, 4), wake_iters=2, ladder=(16,))
+    for k in ("plain", "a_priori", "through_solver_field", "a_priori_wake_scale"):
         assert np.isfinite(r[k]["cd"]) and r[k]["cd"] > 0, k
-        assert r[k]["wall_s"] > 0, k
-    assert r["coarse_plain"]["nx"] == 128 and r["coarse_learned"]["steps"] == 500
-    assert r["speedup_vs_fine"] > 0
-    ts = r["coarse_learned_through_solver"]
-    assert ts["iters"] == 1 and len(ts["history"]) == 1 and np.isfinite(ts["cd"])
+        assert r[k]["wall_s"] > 0 and len(r[k]["cd_per_seed"]) == 2, k
+    assert np.isfinite(r["fine"]["cd"]) and r["fine"]["cd_seed_spread"] is not None
+    assert r["coarse"]["nx"] == 128 and r["coarse"]["steps"] == 500
+    assert r["field_training"]["iters"] == 2 and r["field_training"]["horizon"] == 20
+    assert r["wake_fit"]["runs"] == 4 and r["ladder"][0]["nx"] == 256
+    assert set(r["time_to_solution"]) == {"a_priori", "through_solver_field", "a_priori_wake_scale"}
     assert r["training"]["samples"] > 0
 
 
