@@ -429,8 +429,8 @@ def run_learned_ncu_case(a):
     """The command profiled by ncu for the learned-tau step: the coarse
     1024 x 256 channel of the learned comparison (MRT, FP32, learned tau with
     a seeded Xavier network whose range covers every node), --steps steps
-    after 200 warm-up steps, timed on the host around the synchronising
-    ippi_step call."""
+    after 200 warm-up steps, device-timed (ippi_step_timed); with
+    --tensor-cores the network's hidden layer runs on the tensor cores."""
     import numpy as np
     import torch
 
@@ -446,14 +446,16 @@ def run_learned_ncu_case(a):
                             [-1e6] * 6, [1e6] * 6, [1e-3]]).astype(np.float32)
     bits, _ = lt.bf16_bits(lt.xavier(0))
     lat.load_tau_mlp(bits, stats)
+    if a.tensor_cores:
+        lat.set_learned_tensor_cores(True)
     lat.step(200, 1)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    lat.step(a.steps, 201)  # returns after the handle's stream has drained
-    us = (time.perf_counter() - t0) * 1e6 / a.steps
+    ms = lat.step_timed(a.steps, 201)
+    us = ms * 1e3 / a.steps
     d = lat.diagnostics()
     lat.close()
     print(json.dumps({"learned_ncu_case": "channel_cylinder_1024x256_mrt_learned_tau", "steps": a.steps,
+                      "hidden_layer": "bf16 tensor cores (mma.sync)" if a.tensor_cores else "fp32 fma",
                       "us_per_step": round(us, 2), "fallback_nodes": d["fallback_nodes"]}))
 
 
@@ -809,6 +811,8 @@ def main():
                     help="step rate of the 64-cylinder 16384x4096 lattice per storage")
     ap.add_argument("--learned-ncu-case", action="store_true",
                     help="learned-tau steps of the coarse channel for an ncu capture")
+    ap.add_argument("--tensor-cores", action="store_true",
+                    help="with --learned-ncu-case: the hidden layer on the tensor cores")
     ap.add_argument("--adjoint-ncu-case", action="store_true",
                     help="short adjoint rollout and backward sweep for an ncu capture")
     ap.add_argument("--ncu-case", action="store_true",

@@ -239,6 +239,15 @@ int ippi_profile_steps(ippi_lbm* h, int nsteps, int t0, double* ms_bulk,
 int ippi_load_tau_mlp(ippi_lbm* h, const uint16_t* w_bf16, size_t n, const float* stats,
                       size_t nstats);
 
+/* No counterpart in the reference: the learned tau's 32 x 32 hidden layer on
+ * the tensor cores (on != 0) or on FP32 FMA (0, the default) in the step's
+ * bulk row segments.  On the tensor cores each warp multiplies its 32 nodes'
+ * layer-1 activations, rounded to BF16, by the BF16 weights with FP32
+ * accumulation (mma.sync m16n8k16); the IB-forced nodes, downloads and the
+ * adjoint keep the FMA network, and the adjoint refuses to run while this is
+ * on.  IPPI_LES_LEARNED with FP32 / FP16 / BF16 storage only. */
+int ippi_set_learned_tensor_cores(ippi_lbm* h, int on);
+
 /* No counterpart in the reference: the relaxation time of every node for
  * IPPI_LES_FIELD, tau[ny][nx] (host, each > 0.5) -- the parameter field of
  * the adjoint's tau gradient. */

@@ -105,6 +105,9 @@ struct ippi_lbm {
     long long hist_written = 0;
     // learned tau: parameters (FP32 values of the BF16 weights) + statistics
     float* mlp_dev = nullptr;
+    std::vector<float> mlp_host;   // the loaded parameters + statistics (FP32 values)
+    bool mlp_tc = false;           // hidden layer on the tensor cores (ippi_set_learned_tensor_cores)
+    MlpFrag* mlp_frag = nullptr;   // lane fragments of W2, b2, w3 for warp_mlp_tc
     unsigned long long mlp_version = 0;  // unique per network load (g_mlp_serial)
     double* tau_field = nullptr;  // IPPI_LES_FIELD: [ny][nx]
     unsigned long long* ib_bar = nullptr;  // arrival counter of the one-launch step's IB blocks
@@ -226,6 +229,49 @@ cudaError_t dalloc(P** p, size_t bytes)
 void dfree(void* p)
 {
     if (p) cudaFree(p);
+}
+
+// FP32 value -> BF16 bits, round to nearest even (finite values)
+uint16_t bf16_bits(float v)
+{
+    uint32_t u;
+    std::memcpy(&u, &v, 4);
+    return (uint16_t)((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
+}
+
+// The lane fragments of warp_mlp_tc from a parameter block (lbm_common.cuh
+// layout): for lane (g = lane / 4, t = lane % 4), k step kt and output tile
+// nt, the B registers of mma.m16n8k16 hold W2[n][k], W2[n][k + 1] and
+// W2[n][k + 8], W2[n][k + 9] as BF16 pairs (n = 8 nt + g, k = 16 kt + 2 t,
+// the smaller k in the low half); then b2 and w3 at columns c, c + 1
+// (c = 8 nt + 2 t), the accumulator columns the lane holds.
+MlpFrag mlp_fragments(const float* w)
+{
+    MlpFrag fr;
+    for (int lane = 0; lane < 32; lane++) {
+        const int g = lane >> 2, t = lane & 3;
+        uint32_t words[16];
+        for (int kt = 0; kt < 2; kt++)
+            for (int nt = 0; nt < 4; nt++) {
+                const int n = 8 * nt + g, k = 16 * kt + 2 * t;
+                const float* row = w + kMlpW2 + n * kMlpHid;
+                words[(kt * 4 + nt) * 2] = bf16_bits(row[k]) | ((uint32_t)bf16_bits(row[k + 1]) << 16);
+                words[(kt * 4 + nt) * 2 + 1] = bf16_bits(row[k + 8]) | ((uint32_t)bf16_bits(row[k + 9]) << 16);
+            }
+        for (int q = 0; q < 4; q++)
+            fr.e[q][lane] = make_uint4(words[4 * q], words[4 * q + 1], words[4 * q + 2], words[4 * q + 3]);
+        auto bits = [](float v) {
+            uint32_t u;
+            std::memcpy(&u, &v, 4);
+            return u;
+        };
+        for (int nt = 0; nt < 4; nt++) {
+            const int c = 8 * nt + 2 * t;
+            fr.e[4 + nt][lane] = make_uint4(bits(w[kMlpB2 + c]), bits(w[kMlpB2 + c + 1]), bits(w[kMlpW3 + c]),
+                                            bits(w[kMlpW3 + c + 1]));
+        }
+    }
+    return fr;
 }
 
 // grid of the grid-stride conversion kernels: 256-thread blocks, at most
@@ -765,6 +811,7 @@ LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int pa
     a.ny = h->p.ny;
     a.les = h->p.les_model;
     a.mlp = h->mlp_dev;
+    a.mlp_frag = h->mlp_tc ? h->mlp_frag : nullptr;
     a.tau_field = h->tau_field;
     a.mac = h->mac;
     a.wall_dist = h->wall_dist;
@@ -1144,6 +1191,7 @@ int ippi_destroy(ippi_lbm* h)
     adjoint_free(h);
     for (int b = 0; b < 2; b++) dfree(h->f[b]);
     dfree(h->mlp_dev);
+    dfree(h->mlp_frag);
     dfree(h->tau_field);
     dfree(h->mac);
     dfree(h->wall_dist);
@@ -1798,6 +1846,34 @@ int ippi_last_error(ippi_lbm* h, char* buf, size_t n)
 
 }  // extern "C"
 
+namespace {
+// the tensor-core fragments of the loaded network, on the device
+int upload_mlp_frag(ippi_lbm* h)
+{
+    if (h->mlp_host.size() < (size_t)kMlpParams) return IPPI_OK;
+    const MlpFrag fr = mlp_fragments(h->mlp_host.data());
+    if (!h->mlp_frag) CK(h, dalloc(&h->mlp_frag, sizeof(MlpFrag)));
+    CK(h, cudaMemcpy(h->mlp_frag, &fr, sizeof(MlpFrag), cudaMemcpyHostToDevice));
+    return IPPI_OK;
+}
+}  // namespace
+
+int ippi_set_learned_tensor_cores(ippi_lbm* h, int on)
+{
+    if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
+    if (on && h->p.les_model != IPPI_LES_LEARNED)
+        return fail(h, IPPI_ERR_STATE, "tensor cores for the learned tau need les_model IPPI_LES_LEARNED");
+    if (on && h->p.storage == IPPI_F64)
+        return fail(h, IPPI_ERR_ARG, "the tensor-core network is for FP32 arithmetic (not FP64 storage)");
+    CK(h, cudaSetDevice(h->p.device));
+    CK(h, cudaStreamSynchronize(h->st));
+    h->mlp_tc = on != 0;
+    if (h->mlp_tc)
+        if (int rc = upload_mlp_frag(h)) return rc;
+    drop_graphs(h);
+    return IPPI_OK;
+}
+
 int ippi_load_tau_mlp(ippi_lbm* h, const uint16_t* w_bf16, size_t n, const float* stats, size_t nstats)
 {
     if (!h) return fail(nullptr, IPPI_ERR_ARG, "null handle");
@@ -1822,6 +1898,9 @@ int ippi_load_tau_mlp(ippi_lbm* h, const uint16_t* w_bf16, size_t n, const float
     h->mlp_version = ++g_mlp_serial;
     h->mlp_hash = ckp_hash(reinterpret_cast<const unsigned char*>(blob.data()), blob.size() * sizeof(float),
                            0x6d6c70ull);
+    h->mlp_host = blob;
+    if (h->mlp_tc)
+        if (int rc = upload_mlp_frag(h)) return rc;
     // step graphs captured before the first load hold a null network pointer
     drop_graphs(h);
     h->dl_valid = false;
@@ -1880,6 +1959,9 @@ int ippi_load_tau_mlp_f32(ippi_lbm* h, const float* w, size_t n, const float* st
     for (size_t i = 0; i < n; i++)
         if (!std::isfinite(w[i])) return fail(h, IPPI_ERR_ARG, "tau network weight %zu is not finite", i);
     CK(h, cudaMemcpy(h->mlp_dev, w, n * sizeof(float), cudaMemcpyHostToDevice));
+    std::copy(w, w + n, h->mlp_host.begin());
+    if (h->mlp_tc)
+        if (int rc2 = upload_mlp_frag(h)) return rc2;
     h->mlp_version = ++g_mlp_serial;
     h->mlp_hash = ckp_hash(reinterpret_cast<const unsigned char*>(stats), nstats * sizeof(float),
                            ckp_hash(reinterpret_cast<const unsigned char*>(w), n * sizeof(float), 0x6d6c7033ull));
@@ -1894,6 +1976,8 @@ int ippi_adjoint_forward(ippi_lbm* h, int nsteps, int t0, int ckpt_every)
     if (!h->solid.empty()) return fail(h, IPPI_ERR_STATE, "the adjoint does not take solid nodes");
     if (h->p.les_model >= IPPI_LES_WALE)
         return fail(h, IPPI_ERR_STATE, "the adjoint takes the relaxation-time models 0-3");
+    if (h->mlp_tc)
+        return fail(h, IPPI_ERR_STATE, "the adjoint linearises the FMA network: switch the tensor cores off");
     if (h->ib_active && h->p.mdf_iters != 1)
         return fail(h, IPPI_ERR_STATE, "the adjoint supports one direct-forcing pass (mdf_iters = 1)");
     if (h->ib_active && (long long)nsteps > h->hist_cap)

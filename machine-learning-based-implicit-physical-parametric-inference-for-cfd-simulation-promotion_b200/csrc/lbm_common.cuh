@@ -450,6 +450,121 @@ __device__ __forceinline__ C mlp_forward(const C* x)
     return softplus(z);
 }
 
+// ---------------------------------------------------------------------------
+// the same network with its 32 x 32 hidden layer on the tensor cores, for the
+// 32 nodes of a warp at once (an opt-in per handle): every lane evaluates
+// layer 1 for its own node (FMA, constant-memory weights) and writes the 32
+// activations, rounded to BF16, as the A operand's row; the warp multiplies
+// the 32 x 32 activation tile by W2^T with mma.sync m16n8k16 (BF16 inputs,
+// FP32 accumulation: 2 node tiles x 4 output tiles x 2 k steps = 16 MMAs);
+// each lane applies tanh and the output weights to the accumulator elements
+// it holds, and the per-node sums meet in the node's lane through shuffles.
+// The B operand (W2 as BF16 pairs in this lane's fragment order) and the
+// lane's share of b2 / w3 come from a 4 KB table built on the host
+// (MlpFrag).  All 32 lanes must call it together; the tile rows are 16-byte
+// aligned (kTcRow words of 4 bytes).
+// ---------------------------------------------------------------------------
+constexpr int kTcRow = 20;  // 32-bit words per node row of the activation tile (16 + 4: no bank conflicts)
+
+// The fragment table: kFragQ x 32 16-byte entries, entry [q][lane] (q-major,
+// so each of a warp's eight loads is one coalesced 512-byte request):
+//   q 0-3  W2 B fragments of the lane, words [k step][output tile][2] as BF16 pairs
+//   q 4-7  per output tile q - 4: b2[c], b2[c + 1], w3[c], w3[c + 1] (FP32 bits),
+//          c = 8 (q - 4) + 2 (lane & 3)
+constexpr int kFragQ = 8;
+struct MlpFrag {
+    uint4 e[kFragQ][32];
+};
+
+__device__ __forceinline__ void mma_bf16_16816(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                               uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// z (before softplus) of this lane's node; x: standardised inputs; sh: the
+// warp's 32 x kTcRow-word tile in shared memory
+__device__ __forceinline__ float warp_mlp_tc(const float* x, uint32_t* sh, const MlpFrag* __restrict__ frag)
+{
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    // this lane's fragments first: their loads run under layer 1
+    uint4 fq[kFragQ];
+#pragma unroll
+    for (int q = 0; q < kFragQ; q++) fq[q] = __ldg(&frag->e[q][lane]);
+    uint32_t* row = sh + lane * kTcRow;
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        uint32_t wd[4];
+#pragma unroll
+        for (int ww = 0; ww < 4; ww++) {
+            float h[2];
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const int j = 2 * (4 * v + ww) + q;
+                float s = c_mlp[kMlpB1 + j];
+#pragma unroll
+                for (int i = 0; i < kMlpIn; i++) s += c_mlp[kMlpW1 + j * kMlpIn + i] * x[i];
+                h[q] = mlp_tanh(s);
+            }
+            const __nv_bfloat162 pr = __floats2bfloat162_rn(h[0], h[1]);  // low half: the even column
+            wd[ww] = *reinterpret_cast<const uint32_t*>(&pr);
+        }
+        // 16-byte stores: at a 20-word row stride the 8 lanes of each phase hit distinct banks
+        *reinterpret_cast<uint4*>(row + 4 * v) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+    }
+    const uint32_t b[16] = {fq[0].x, fq[0].y, fq[0].z, fq[0].w, fq[1].x, fq[1].y, fq[1].z, fq[1].w,
+                            fq[2].x, fq[2].y, fq[2].z, fq[2].w, fq[3].x, fq[3].y, fq[3].z, fq[3].w};
+    float4 bw[4];
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++)
+        bw[nt] = make_float4(__uint_as_float(fq[4 + nt].x), __uint_as_float(fq[4 + nt].y),
+                             __uint_as_float(fq[4 + nt].z), __uint_as_float(fq[4 + nt].w));
+    __syncwarp();
+    float acc[2][4][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+            acc[mt][nt][0] = acc[mt][nt][2] = bw[nt].x;
+            acc[mt][nt][1] = acc[mt][nt][3] = bw[nt].y;
+        }
+#pragma unroll
+    for (int kt = 0; kt < 2; kt++)
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++) {
+            const uint32_t* r0 = sh + (mt * 16 + g) * kTcRow + kt * 8 + t;
+            const uint32_t* r1 = r0 + 8 * kTcRow;
+            const uint32_t a0 = r0[0], a1 = r1[0], a2 = r0[4], a3 = r1[4];
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++)
+                mma_bf16_16816(acc[mt][nt], a0, a1, a2, a3, b[(kt * 4 + nt) * 2], b[(kt * 4 + nt) * 2 + 1]);
+        }
+    // rows of this lane's accumulators: g, g + 8 (tile 0), 16 + g, 24 + g (tile 1)
+    float p[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+            p[2 * mt] += bw[nt].z * mlp_tanh(acc[mt][nt][0]) + bw[nt].w * mlp_tanh(acc[mt][nt][1]);
+            p[2 * mt + 1] += bw[nt].z * mlp_tanh(acc[mt][nt][2]) + bw[nt].w * mlp_tanh(acc[mt][nt][3]);
+        }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        p[q] += __shfl_xor_sync(0xffffffffu, p[q], 1);
+        p[q] += __shfl_xor_sync(0xffffffffu, p[q], 2);
+    }
+    // node `lane` = 8 q + g' sits in row q of the lanes of group g'
+    const int src = 4 * (lane & 7), q = lane >> 3;
+    const float v0 = __shfl_sync(0xffffffffu, p[0], src), v1 = __shfl_sync(0xffffffffu, p[1], src);
+    const float v2 = __shfl_sync(0xffffffffu, p[2], src), v3 = __shfl_sync(0xffffffffu, p[3], src);
+    const float z = q == 0 ? v0 : q == 1 ? v1 : q == 2 ? v2 : v3;
+    return z + c_mlp[kMlpB3];
+}
+
 // relaxation time from the network (constant memory), Smagorinsky where a
 // feature leaves the training range
 template <typename C>

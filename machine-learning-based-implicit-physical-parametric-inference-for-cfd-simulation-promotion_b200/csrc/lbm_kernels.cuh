@@ -61,6 +61,8 @@ struct StepArgs {
     const float* mlp;     // learned tau: parameters + feature statistics in device memory (the
                           // adjoint reads them here; the LRN step kernels read the copy in
                           // constant memory, c_mlp)
+    const MlpFrag* mlp_frag; // learned tau on the tensor cores (bulk row segments): per-lane W2
+                          // fragments, b2 and w3; null = the FMA network
     const double* tau_field; // les == 3: relaxation time per node [ny][nx]
     void* mac;            // les 4, 5: [2][ny][nx] compute type, ux and uy of this step's
                           // post-stream (and IB-corrected) state, for the velocity gradient
@@ -617,12 +619,101 @@ __device__ __forceinline__ void bulk_tile(const StepArgs& a, int bx, int by, int
     if (bad) flag_error(a.ctr, __ldcg(&a.ctr->t[a.par]));
 }
 
+// The learned-tau row segment with the network's hidden layer on the tensor
+// cores (warp_mlp_tc): the same pull, moments, collision and stores as
+// bulk_tile, but every lane of a warp reaches the network together -- lanes
+// beyond the lattice or on deferred / solid nodes run it on dummy features
+// and store nothing.
+template <int S, int CO, int SC, int AV>
+__device__ __forceinline__ void bulk_tile_tc(const StepArgs& a, int bx, int by, int tx)
+{
+    using C = typename Store<S>::C;
+    using T = typename Store<S>::T;
+    static_assert(S != ST_F64, "the tensor-core network is for FP32 arithmetic");
+    __shared__ __align__(16) uint32_t h1s[kBlockX / 32][32 * kTcRow];
+    const int x = bx * kBlockX + tx, y = by;
+    const int nx = a.nx, ny = a.ny;
+    const int pitch = (int)a.pitch, plane = (int)a.plane;
+    bool active = x < nx;
+    const int node = y * nx + x;
+    uint8_t nf = 0;
+    const int rbit = y >> a.row_shift;
+    if (active && ((a.rowmask[rbit >> 5] >> (rbit & 31)) & 1u) && a.tile[by * a.tiles_x + bx]) nf = a.nflag[node];
+    if (nf & (NF_DEFER | NF_SOLID)) active = false;
+    const C rbs = rbase<S>(a);
+    C f[9], rho = C(1), ux = C(0), uy = C(0);
+#pragma unroll
+    for (int k = 0; k < 9; k++) f[k] = C(0);
+    const int cell = y * pitch + x;
+    if (active) {
+        if (nf & NF_SBND) {
+            solid_pull<S>(a, x, y, f);
+            macros<C>(f, rbs, rho, ux, uy);
+        } else if (x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
+            const T* p = reinterpret_cast<const T*>(a.f_in) + cell;
+#pragma unroll
+            for (int k = 0; k < 9; k++) f[k] = Store<S>::ld(__ldg(p + (k * plane - EY(k) * pitch - EX(k))));
+            macros<C>(f, rbs, rho, ux, uy);
+        } else if (SC == SC_REF) {
+            ref_state<S>(a, x, y, f, rho, ux, uy);
+        } else {
+            ch_state<S>(a, x, y, f, rho, ux, uy);
+        }
+    }
+    const C tau0 = prm<C>(a.tau0, a.f_tau0), cs = prm<C>(a.cs, a.f_cs);
+    C pxx, pxy, pyy;
+    pi_neq<C>(f, rho, ux, uy, rbs, pxx, pxy, pyy);
+    // features, range and standardisation as learned_tau
+    constexpr int st = kMlpParams;
+    C xs[kMlpIn];
+    mlp_features<C>(pxx, pxy, pyy, rho, ux, uy, tau0, xs);
+    bool in = active;
+#pragma unroll
+    for (int i = 0; i < kMlpIn; i++) {
+        in = in && xs[i] >= C(c_mlp[st + 2 * kMlpIn + i]) && xs[i] <= C(c_mlp[st + 3 * kMlpIn + i]);
+        xs[i] = active ? (xs[i] - C(c_mlp[st + i])) / C(c_mlp[st + kMlpIn + i]) : C(0);
+    }
+    __syncwarp();
+    const float z = warp_mlp_tc(xs, h1s[tx >> 5], a.mlp_frag);
+    if (!active) return;
+    const bool bad = !(rho <= C(10) && rho >= C(0));
+    const C tau = in ? tau0 + C(c_mlp[st + 4 * kMlpIn]) * softplus(z) : les_tau<C>(pxx, pxy, pyy, rho, tau0, cs);
+    if (AV) {
+        const int t = __ldcg(&a.ctr->t[a.par]);
+        C* av = reinterpret_cast<C*>(a.avg);
+        const int pl = nx * ny;
+        const C n0 = C(t - a.avg_start), n1 = C(t - a.avg_start + 1);
+        av[node] = (av[node] * n0 + ux) / n1;
+        av[pl + node] = (av[pl + node] * n0 + uy) / n1;
+        av[2 * pl + node] = (av[2 * pl + node] * n0 + rho) / n1;
+    }
+    collide_node<C, CO>(f, rho, ux, uy, rbs, tau);
+    T* q = reinterpret_cast<T*>(a.f_out) + cell;
+#pragma unroll
+    for (int k = 0; k < 9; k++) q[k * plane] = Store<S>::st(f[k]);
+    if (bad) flag_error(a.ctr, __ldcg(&a.ctr->t[a.par]));
+}
+
+// a learned-tau row segment: the tensor-core network when the handle holds
+// one (a warp-uniform kernel parameter), else bulk_tile's FMA network
+template <int S, int CO, int SC, bool LRN, int XT, int AV>
+__device__ __forceinline__ void bulk_tile_any(const StepArgs& a, int bx, int by, int tx)
+{
+    if constexpr (LRN && S != ST_F64 && XT == 0) {
+        if (a.mlp_frag) {
+            bulk_tile_tc<S, CO, SC, AV>(a, bx, by, tx);
+            return;
+        }
+    }
+    bulk_tile<S, CO, SC, LRN, XT, AV>(a, bx, by, tx);
+}
+
 // a normal step without immersed boundary work in the same launch: one
 // block per row segment; block (0, 0) advances the step counter
 template <int S, int CO, int SC, bool LRN, int XT = 0, int AV = 0>
 __global__ void __launch_bounds__(kBlockX, (step_min_blocks<S, LRN>())) step_fast(const StepArgs ap)
 {
-    bulk_tile<S, CO, SC, LRN, XT, AV>(ap, blockIdx.x, blockIdx.y, threadIdx.x);
+    bulk_tile_any<S, CO, SC, LRN, XT, AV>(ap, blockIdx.x, blockIdx.y, threadIdx.x);
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
         ap.ctr->t[ap.par ^ 1] = __ldcg(&ap.ctr->t[ap.par]) + 1;
 }
@@ -1250,7 +1341,7 @@ __global__ void __launch_bounds__(kBlockX, (step_min_blocks<S, LRN>())) step_ib_
     }
     const int tile = blockIdx.x - nib;
     const int by = tile / ia.s.tiles_x, bx = tile - by * ia.s.tiles_x;
-    bulk_tile<S, CO, SC, LRN, XT, AV>(ia.s, bx, by, threadIdx.x);
+    bulk_tile_any<S, CO, SC, LRN, XT, AV>(ia.s, bx, by, threadIdx.x);
 }
 
 // the post-stream velocity of node (x, y) into StepArgs::mac (closures 4,

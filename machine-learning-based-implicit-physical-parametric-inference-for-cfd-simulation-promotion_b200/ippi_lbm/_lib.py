@@ -24,7 +24,7 @@ DELTA_BILINEAR, DELTA_PESKIN4 = 0, 1
  FIELD_FLAGS, FIELD_NNFLAG) = range(10)
 
 EXPORTS = ("ippi_abi_version", "ippi_params_default", "ippi_create", "ippi_destroy",
-           "ippi_init_macros", "ippi_init_macros_f32", "ippi_download_f32", "ippi_set_les_cs", "ippi_set_markers", "ippi_load_band_net", "ippi_step", "ippi_step_timed",
+           "ippi_init_macros", "ippi_init_macros_f32", "ippi_download_f32", "ippi_set_les_cs", "ippi_set_learned_tensor_cores", "ippi_set_markers", "ippi_load_band_net", "ippi_step", "ippi_step_timed",
            "ippi_download", "ippi_forces", "ippi_force_history", "ippi_get_stream",
            "ippi_profile_steps", "ippi_last_error", "ippi_mass_noalloc", "ippi_load_tau_mlp",
            "ippi_filter_snapshot", "ippi_mlp_param_count", "ippi_mlp_scratch_floats", "ippi_mlp_grad",
@@ -78,6 +78,7 @@ def lib() -> C.CDLL:
         L.ippi_init_macros_f32.argtypes = [C.c_void_p, _fp, _fp, _fp]
         L.ippi_download_f32.argtypes = [C.c_void_p, C.c_int, _fp, C.c_size_t]
         L.ippi_set_les_cs.argtypes = [C.c_void_p, C.c_double]
+        L.ippi_set_learned_tensor_cores.argtypes = [C.c_void_p, C.c_int]
         L.ippi_set_markers.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.POINTER(C.c_int), _dp]
         L.ippi_load_band_net.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.c_size_t]
         L.ippi_step.argtypes = [C.c_void_p, C.c_int, C.c_int]

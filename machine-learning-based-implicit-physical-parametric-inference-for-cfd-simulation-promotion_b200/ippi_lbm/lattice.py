@@ -113,6 +113,11 @@ class Lattice:
     def step(self, n=1, t0=1):
         L.check(L.lib().ippi_step(self._h, n, t0), self._h)
 
+    def set_learned_tensor_cores(self, on=True):
+        """The learned tau's hidden layer on the tensor cores (BF16 mma.sync,
+        FP32 accumulation) or on FP32 FMA (ippi_set_learned_tensor_cores)."""
+        L.check(L.lib().ippi_set_learned_tensor_cores(self._h, int(bool(on))), self._h)
+
     def set_les_cs(self, cs):
         """Smagorinsky constant of the following steps (ippi_set_les_cs)."""
         L.check(L.lib().ippi_set_les_cs(self._h, float(cs)), self._h)

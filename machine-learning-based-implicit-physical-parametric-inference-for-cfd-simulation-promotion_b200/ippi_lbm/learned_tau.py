@@ -217,12 +217,15 @@ def predict(net, x_raw, device=0, bf16=True):
 # ---------------------------------------------------------------------------
 # runs
 # ---------------------------------------------------------------------------
-def run_cylinder(sc, steps, avg_from, net=None, snapshot=None, device=0, chunk=2000, means=False):
+def run_cylinder(sc, steps, avg_from, net=None, snapshot=None, device=0, chunk=2000, means=False,
+                 tensor_cores=True):
     """Run a cylinder scene (scenes.cylinder_channel dict) for `steps` steps;
     returns mean Cd / Cl over steps >= avg_from, the Strouhal number of Cl in
     that window, the device wall time of the stepping, the snapshots taken by
     snapshot = (factor, first_step, stride, count), and with `means` the
-    time-averaged velocity [2][ny][nx] over the same window."""
+    time-averaged velocity [2][ny][nx] over the same window.  A learned run
+    evaluates the network's hidden layer on the tensor cores unless
+    tensor_cores is false (FP32-arithmetic storage; it is faster than FMA)."""
     from .lattice import Lattice
 
     params = dict(sc["params"])
@@ -235,6 +238,8 @@ def run_cylinder(sc, steps, avg_from, net=None, snapshot=None, device=0, chunk=2
     lat.set_markers(sc["markers"], ds=sc["ds"])
     if net is not None:
         lat.load_tau_mlp(*net.export())
+        if tensor_cores and params["storage"] != L.F64:
+            lat.set_learned_tensor_cores(True)
     forces = np.zeros((steps, 2))
     snaps = []
     marks = []

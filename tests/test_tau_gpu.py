@@ -288,3 +288,53 @@ def test_networks_of_several_handles_take_turns_in_constant_memory():
     assert not errs
     for s in (1, 2):
         assert np.array_equal(b[s].download(ip.FIELD_F), solo[s][0])
+
+
+def _tc_pair(storage=ip.F32):
+    """Two learned lattices from the same seeded network (range covering every
+    node): the hidden layer on FMA and on the tensor cores."""
+    out = []
+    for tc in (False, True):
+        g = _learned_lattice(2, storage)
+        if tc:
+            g.set_learned_tensor_cores(True)
+        out.append(g)
+    return out
+
+
+def test_tensor_core_network_matches_the_fma_network():
+    """The learned tau's 32 x 32 hidden layer on the tensor cores (BF16
+    activations and weights, FP32 accumulation, mma.sync m16n8k16 over the
+    32 nodes of a warp) against the FMA network: after 1 step the
+    populations agree to 1e-6 of max |f|, after 40 steps to 1e-4; the body
+    forces to 1e-3.  The network has not gone missing: switching it off
+    again gives the FMA lattice's bits."""
+    a, b = _tc_pair()
+    for n, t0, tol in ((1, 1, 1e-6), (39, 2, 1e-4)):
+        a.step(n, t0)
+        b.step(n, t0)
+        fa, fb = a.download(ip.FIELD_F), b.download(ip.FIELD_F)
+        assert np.abs(fa - fb).max() <= tol * np.abs(fa).max(), (n, np.abs(fa - fb).max())
+    assert np.abs(fa - fb).max() > 0  # BF16 activations do change the result
+    np.testing.assert_allclose(b.forces(), a.forces(), rtol=1e-3, atol=1e-6)
+    c, d = _learned_lattice(3), _learned_lattice(3)
+    d.set_learned_tensor_cores(True)
+    d.set_learned_tensor_cores(False)
+    c.step(10, 1)
+    d.step(10, 1)
+    assert np.array_equal(c.download(ip.FIELD_F), d.download(ip.FIELD_F))
+
+
+def test_tensor_core_network_is_refused_where_it_does_not_apply():
+    g = _learned_lattice(1, ip.F64)
+    with pytest.raises(ip.IppiError, match="FP32 arithmetic"):
+        g.set_learned_tensor_cores(True)
+    plain = ip.Lattice(64, 32, collision=ip.MRT, bc_set=ip.BC_CHANNEL, u_in=0.05, tau0=0.56,
+                       storage=ip.F32)
+    with pytest.raises(ip.IppiError, match="IPPI_LES_LEARNED"):
+        plain.set_learned_tensor_cores(True)
+    h = _learned_lattice(1)
+    h.set_learned_tensor_cores(True)
+    h.step(2, 1)
+    with pytest.raises(ip.IppiError, match="tensor cores off"):
+        h.adjoint_forward(4, 3, 2)
