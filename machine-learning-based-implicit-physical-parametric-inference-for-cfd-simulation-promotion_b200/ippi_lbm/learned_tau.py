@@ -306,9 +306,10 @@ def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=
        filtered stress (samples_from_snapshot, train).
     3. Through the solver on the filtered field: train_on_field_pairs on
        consecutive snapshots (the drag is never a target).
-    4. Optionally the output scale fitted to the fine run's time-averaged
-       near-wake velocity (fit_scale_to_wake, on another noise seed), a
-       quantity other than the judged drag.
+    4. Optionally the output scale fitted to the fine run's mean
+       recirculation length behind the cylinder (fit_scale_to_wake, on
+       another noise seed), a quantity of the mean wake other than the
+       judged drag.
     5. Each network and plain Smagorinsky on the coarse lattice (nx/factor x
        ny/factor, same Re and Mach) over the same physical window, for every
        seed of `eval_seeds`: mean drag, its spread, St, device wall time.
@@ -387,13 +388,17 @@ def experiment(nx=4096, ny=1024, d=128, u=0.04, re=3900.0, factor=4, fine_steps=
         nets["through_solver_field"] = net_f
     if wake_fit:
         ref_u = box_filter(rf["mean_u"], factor)
+        lr_ref = recirculation_length(rf["mean_u"], cx, cy, d)
+        res["fine"]["recirculation_length"] = lr_ref
         t1 = time.perf_counter()
         net_w, wh = fit_scale_to_wake(net, coarse(seed + 100), ref_u, csteps, cfirst, grid=wake_grid,
-                                      iters=wake_iters, device=device, log=log)
-        res["wake_fit"] = dict(scale=net_w.out_scale / net.out_scale, runs=len(wh),
+                                      iters=wake_iters, device=device, log=log, lr_ref=lr_ref)
+        res["wake_fit"] = dict(quantity="mean recirculation length", fine_recirculation_length=lr_ref,
+                               scale=net_w.out_scale / net.out_scale, runs=len(wh),
                                seconds=time.perf_counter() - t1,
-                               history=[dict(scale=a_, wake_l2=b_, cd=c_) for a_, b_, c_ in wh])
-        res["a_priori_wake_scale"] = evaluate(net_w, "learned, scale fitted to the wake velocity")
+                               history=[dict(scale=a_, objective=b_, cd=c_, recirculation_length=d_, wake_l2=e_)
+                                        for a_, b_, c_, d_, e_ in wh])
+        res["a_priori_wake_scale"] = evaluate(net_w, "learned, scale fitted to the recirculation length")
         nets["a_priori_wake_scale"] = net_w
     if calibrate_drag:
         net_c, ch = calibrate_scale(net, coarse(seed + 1), cd_ref, csteps, cfirst, device=device, log=log)
@@ -654,6 +659,28 @@ def train_on_field_pairs(net, sc, pairs, horizon, iters=120, lr=1e-3, ckpt=32, d
 # ---------------------------------------------------------------------------
 # an output scale fitted to the wake's mean velocity (not to the drag)
 # ---------------------------------------------------------------------------
+def recirculation_length(mean_u, cx, cy, d):
+    """Length of the mean recirculation bubble behind a cylinder, in
+    diameters: the first zero crossing (negative to positive, linearly
+    interpolated) of the time-averaged streamwise velocity on the centre
+    line (the mean of the two rows around cy) behind the cylinder's rear,
+    measured from the rear; 0 without a reversed-flow region."""
+    u = np.asarray(mean_u)[0]
+    ny, nx = u.shape
+    r0 = int(math.floor(cy - 0.5))
+    line = 0.5 * (u[r0] + u[min(r0 + 1, ny - 1)])
+    rear = cx + 0.5 * d
+    xs = np.arange(nx) + 0.5  # cell centres
+    k0 = int(np.searchsorted(xs, rear))
+    seen_neg = False
+    for k in range(k0, nx - 1):
+        if line[k] < 0:
+            seen_neg = True
+        if seen_neg and line[k] < 0 <= line[k + 1]:
+            x0 = xs[k] - line[k] * (xs[k + 1] - xs[k]) / (line[k + 1] - line[k])
+            return float((x0 - rear) / d)
+    return 0.0
+
 def wake_mask(nx, ny, cx, cy, d):
     """Cells of the near wake: x from the cylinder's rear + 1 to 6 D behind
     its centre, |y - cy| < 1.5 D."""
@@ -662,14 +689,17 @@ def wake_mask(nx, ny, cx, cy, d):
 
 
 def fit_scale_to_wake(net, sc, mean_u_ref, steps, avg_from, grid=(0.25, 1, 4, 16, 64), iters=4, device=0,
-                      log=None):
-    """Fit the network's output scale so that the coarse lattice's
-    time-averaged velocity in the near wake (wake_mask) comes closest, in L2,
-    to mean_u_ref [2][ny][nx] (the fine run's time average, box-filtered to
-    the coarse grid).  Forward runs of `sc`: the scales of `grid`, then a
-    golden-section search of log(scale) between the best grid point's
-    neighbours.  Returns (net with the best scale, [(scale, wake L2, Cd)]).
-    The drag of each run is recorded, not used."""
+                      log=None, lr_ref=None):
+    """Fit the network's output scale to the fine run's mean wake, by forward
+    runs of `sc`.  With lr_ref (the fine run's recirculation length in
+    diameters) the objective is |L_r(scale) - lr_ref| (recirculation_length
+    of the coarse time-averaged velocity); otherwise the L2 distance, over the
+    near wake (wake_mask), of the coarse time-averaged velocity from
+    mean_u_ref [2][ny][nx] (the fine run's, box-filtered to the coarse grid).
+    The scales of `grid`, then a golden-section search of log(scale) between
+    the best grid point's neighbours.  Returns (net with the best scale,
+    [(scale, objective, Cd, L_r, wake L2)]).  The drag of each run is
+    recorded, not used."""
     cx, cy = sc["markers"][:, 0].mean(), sc["markers"][:, 1].mean()
     m = wake_mask(sc["nx"], sc["ny"], cx, cy, sc["d"])
     ref = np.asarray(mean_u_ref)[:, m]
@@ -678,10 +708,12 @@ def fit_scale_to_wake(net, sc, mean_u_ref, steps, avg_from, grid=(0.25, 1, 4, 16
     def err(x):
         n = TauNet(net.w, net.mean, net.std, net.lo, net.hi, net.out_scale * math.exp(x))
         r = run_cylinder(sc, steps, avg_from, net=n, device=device, means=True)
-        e = float(np.sqrt(np.sum((r["mean_u"][:, m] - ref) ** 2) / np.sum(ref ** 2)))
-        hist.append((math.exp(x), e, r["cd"]))
+        l2 = float(np.sqrt(np.sum((r["mean_u"][:, m] - ref) ** 2) / np.sum(ref ** 2)))
+        lr = recirculation_length(r["mean_u"], cx, cy, sc["d"])
+        e = abs(lr - lr_ref) if lr_ref is not None else l2
+        hist.append((math.exp(x), e, r["cd"], lr, l2))
         if log:
-            log(f"wake fit: scale {math.exp(x):.4g} -> wake L2 {e:.4g} (Cd {r['cd']:.4f})")
+            log(f"wake fit: scale {math.exp(x):.4g} -> L_r {lr:.3f} D, wake L2 {l2:.4g} (Cd {r['cd']:.4f})")
         return e
 
     xs = [math.log(g) for g in grid]
