@@ -574,27 +574,38 @@ __device__ __forceinline__ void bulk_tile(const StepArgs& a, int bx, int by, int
     const int x = bx * kBlockX + tx, y = by;
     const int nx = a.nx, ny = a.ny;
     const int pitch = (int)a.pitch, plane = (int)a.plane;
-    if (x >= nx) return;
     const int node = y * nx + x;
-    uint8_t nf = 0;
     const int rbit = y >> a.row_shift;
-    if (((a.rowmask[rbit >> 5] >> (rbit & 31)) & 1u) && a.tile[by * a.tiles_x + bx]) nf = a.nflag[node];
-    if (nf & (NF_DEFER | NF_SOLID)) return;
+    const bool row_flagged = (a.rowmask[rbit >> 5] >> (rbit & 31)) & 1u;
+    // the whole segment interior, in a row without flagged tiles (decided
+    // once per block): no per-node bound, flag or boundary-kind test
+    const bool interior_seg = !row_flagged && bx >= 1 && (bx + 1) * kBlockX <= nx - 1 && y >= 1 && y <= ny - 2;
     const C rbs = rbase<S>(a);
     C f[9], rho, ux, uy;
     const int cell = y * pitch + x;
-    if (nf & NF_SBND) {
-        solid_pull<S>(a, x, y, f);
-        macros<C>(f, rbs, rho, ux, uy);
-    } else if (x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
+    if (interior_seg) {
         const T* p = reinterpret_cast<const T*>(a.f_in) + cell;
 #pragma unroll
         for (int k = 0; k < 9; k++) f[k] = Store<S>::ld(__ldg(p + (k * plane - EY(k) * pitch - EX(k))));
         macros<C>(f, rbs, rho, ux, uy);
-    } else if (SC == SC_REF) {
-        ref_state<S>(a, x, y, f, rho, ux, uy);
     } else {
-        ch_state<S>(a, x, y, f, rho, ux, uy);
+        if (x >= nx) return;
+        uint8_t nf = 0;
+        if (row_flagged && a.tile[by * a.tiles_x + bx]) nf = a.nflag[node];
+        if (nf & (NF_DEFER | NF_SOLID)) return;
+        if (nf & NF_SBND) {
+            solid_pull<S>(a, x, y, f);
+            macros<C>(f, rbs, rho, ux, uy);
+        } else if (x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) {
+            const T* p = reinterpret_cast<const T*>(a.f_in) + cell;
+#pragma unroll
+            for (int k = 0; k < 9; k++) f[k] = Store<S>::ld(__ldg(p + (k * plane - EY(k) * pitch - EX(k))));
+            macros<C>(f, rbs, rho, ux, uy);
+        } else if (SC == SC_REF) {
+            ref_state<S>(a, x, y, f, rho, ux, uy);
+        } else {
+            ch_state<S>(a, x, y, f, rho, ux, uy);
+        }
     }
     // Mesh::ErrorCatch (mesh.cpp:2103): rho outside [0, 10]; NaN too
     const bool bad = !(rho <= C(10) && rho >= C(0));
