@@ -42,10 +42,10 @@ sys.path.insert(0, PKG)
 NX, NY = 4096, 1024
 BYTES_PER_NODE = 72  # FP32: 9 loads + 9 stores
 # DRAM bytes (read + write) of one step launch on this workload, from the
-# ncu capture summarised under profiles/ (dram__bytes_read.sum 151.99 MB +
-# dram__bytes_write.sum 104.70 MB; part of the writes is still in L2 when the
+# ncu capture summarised under profiles/ (dram__bytes_read.sum 151.98 MB +
+# dram__bytes_write.sum 103.09 MB; part of the writes is still in L2 when the
 # kernel ends)
-NCU_TRAFFIC_BYTES = 256.69e6
+NCU_TRAFFIC_BYTES = 255.07e6
 METRIC = "MLUPS"
 WORKLOAD = "channel_cylinder_4096x1024_mrt_smagorinsky_ib_fp32"
 
