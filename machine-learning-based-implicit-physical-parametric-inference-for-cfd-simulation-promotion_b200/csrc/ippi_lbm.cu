@@ -863,13 +863,13 @@ LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int pa
         B.work_type = h->band_type_d;
         for (int t = 0; t < 8; t++) {
             if (!h->nets[t].loaded) continue;
-            const int nin = h->nets[t].nin;
             float* base = h->net_dev[t];
-            B.net[t].w1t = base;
-            B.net[t].b1 = base + nin * kHidden;
-            B.net[t].wht = B.net[t].b1 + kHidden;
-            B.net[t].bh = B.net[t].wht + 6 * kHidden * kHidden;
+            B.net[t].w1f = base;
+            B.net[t].b1 = base + kBandW1Frag;
+            B.net[t].whf = B.net[t].b1 + kHidden;
+            B.net[t].bh = B.net[t].whf + 6 * kBandLayerFrag;
             B.net[t].wo = B.net[t].bh + 6 * kHidden;
+            B.net[t].nin = h->nets[t].nin;
             B.net[t].bo = h->nets[t].w.back();
         }
         B.s = a;
@@ -1368,21 +1368,37 @@ int ippi_load_band_net(ippi_lbm* h, int type, const float* w, size_t n)
     net.loaded = true;
     net.nin = nin;
     net.w.assign(w, w + n);
-    // device layout: w1t[nin][128], b1, wht[6][128][128], bh[6][128], wo[128]
-    std::vector<float> d((size_t)nin * kHidden + kHidden + 6 * kHidden * kHidden + 6 * kHidden + kHidden);
+    // device layout (band_kernel's tensor-core fragment order):
+    //   w1f[8 warps][2 k steps][2 output tiles][32 lanes][2]   layer 1, K padded to 16
+    //   b1[128]
+    //   whf[6][8][16 k steps][2][32][2]                         layers 2..7, 64 KB each
+    //   bh[6][128], wo[128]
+    // Lane (g, t) = (lane / 4, lane % 4) of warp w holds, for k step ks and
+    // tile nt, the mma.m16n8k8 B registers W[n][k], W[n][k + 4] with
+    // n = 16 w + 8 nt + g and k = 8 ks + t (W = torch's weight[out][in]).
     const float* p = w;
-    size_t o = 0;
-    for (int i = 0; i < nin; i++)
-        for (int j = 0; j < kHidden; j++) d[o++] = p[j * nin + i];
+    std::vector<float> d((size_t)kBandW1Frag + kHidden + 6 * kBandLayerFrag + 6 * kHidden + kHidden, 0.f);
+    auto frag = [](float* out, const float* W, int nin_, int ksteps) {
+        for (int wp = 0; wp < 8; wp++)
+            for (int ks = 0; ks < ksteps; ks++)
+                for (int nt = 0; nt < 2; nt++)
+                    for (int lane = 0; lane < 32; lane++) {
+                        const int g = lane >> 2, t = lane & 3, n = 16 * wp + 8 * nt + g, k = 8 * ks + t;
+                        float* e = out + ((((size_t)wp * ksteps + ks) * 2 + nt) * 32 + lane) * 2;
+                        e[0] = k < nin_ ? W[(size_t)n * nin_ + k] : 0.f;
+                        e[1] = k + 4 < nin_ ? W[(size_t)n * nin_ + k + 4] : 0.f;
+                    }
+    };
+    frag(d.data(), p, nin, kBandIn / 8);
     p += kHidden * nin;
+    size_t o = kBandW1Frag;
     for (int j = 0; j < kHidden; j++) d[o++] = p[j];
     p += kHidden;
     const float* hp = p;
-    size_t ob = o + 6 * kHidden * kHidden;
+    size_t ob = o + 6 * (size_t)kBandLayerFrag;
     for (int l = 0; l < 6; l++) {
         const float* W = hp + (size_t)l * (kHidden * kHidden + kHidden);
-        for (int i = 0; i < kHidden; i++)
-            for (int j = 0; j < kHidden; j++) d[o++] = W[j * kHidden + i];
+        frag(d.data() + o + (size_t)l * kBandLayerFrag, W, kHidden, kHidden / 8);
         for (int j = 0; j < kHidden; j++) d[ob++] = W[kHidden * kHidden + j];
     }
     o = ob;

@@ -765,32 +765,37 @@ __global__ void __launch_bounds__(256, (step_min_blocks<S, false>())) prep_kerne
 // boundary nets (Mesh::NNmodel_Type00..07, mesh.cpp:2767-3259)
 //
 // One block evaluates one net (Linear(nin,128)+ReLU, 6 x (Linear(128,128)+
-// ReLU), Linear(128,1)) on up to kBandNodes band nodes in FP32, as libtorch
-// does on the CPU.  Each hidden layer's 128 x 128 weight matrix (64 KB) is
-// brought into shared memory once per block by a TMA bulk copy
-// (cp.async.bulk, completion on an mbarrier), two layer buffers deep, so the
-// next layer's weights arrive while this layer computes.  Thread (warp w,
-// lane l) holds a 5-node x 4-output register tile: nodes 5w..5w+4, outputs
-// 4l..4l+3; per 4 inputs it reads 5 broadcast float4 activations and 4 float4
-// weight rows from shared memory for 80 FMAs.  kBandNodes = 40 puts the
-// 5,796 band nodes of the 2401 x 501 plate in 146 blocks, one wave.
+// ReLU), Linear(128,1)) on up to kBandNodes band nodes.  The seven linear
+// layers run on the tensor cores with FP32 accuracy: every operand x is
+// split into two TF32 parts x = hi + lo, and each mma.m16n8k8 product is
+// taken as lo.hi + hi.lo + hi.hi (the lo.lo term is below FP32 rounding), in
+// FP32 accumulators -- as close to libtorch's FP32 CPU forward as an FP32
+// FMA chain with another summation order.  The output layer is an FP32 dot
+// product.  Warp w owns output columns 16 w .. 16 w + 15 of all 48 rows
+// (3 x 2 tiles of 16 x 8).  Each hidden layer's weights (64 KB, stored on
+// the device in the warps' B-fragment order, so every fragment load is one
+// conflict-free 256-byte row) come into shared memory by one TMA bulk copy
+// (cp.async.bulk, completion on an mbarrier), two layer buffers deep.  The
+// activations sit in shared memory already split (hi and lo planes).
+// kBandNodes = 48 puts the 5,796 band nodes of the 2401 x 501 plate in 122
+// blocks, one wave.
 // ---------------------------------------------------------------------------
-constexpr int kBandWarpNodes = 5;                          // nodes per warp
 constexpr int kBandWarps = 8;
-constexpr int kBandNodes = kBandWarpNodes * kBandWarps;    // band nodes per block
+constexpr int kBandNodes = 48;                     // band nodes per block: three 16-row tiles
 constexpr int kBandThreads = 32 * kBandWarps;
 constexpr int kHidden = 128;
-constexpr int kBandIn = 16;                                // input width, zero-padded
-constexpr int kBandAct = kHidden + 4;                      // floats per activation row
-// dynamic shared memory of band_kernel: two hidden-layer weight buffers,
-// activations, the first layer's weights, outputs, two mbarriers
-constexpr int kBandSmemW = 2 * kHidden * kHidden;
+constexpr int kBandIn = 16;                        // layer-1 inputs, zero-padded
+constexpr int kBandAct = kHidden + 4;              // words per activation row
+constexpr int kBandLayerFrag = kHidden * kHidden;  // floats of one hidden layer in fragment order
+constexpr int kBandW1Frag = kBandWarps * (kBandIn / 8) * 2 * 32 * 2;  // layer 1 in fragment order
+// dynamic shared memory of band_kernel: two hidden-layer weight buffers, the
+// activations (hi and lo planes), outputs, two mbarriers
+constexpr int kBandSmemW = 2 * kBandLayerFrag;
 constexpr int kBandSmemAct = kBandNodes * kBandAct;
-constexpr int kBandSmemW1 = kBandIn * kHidden;
 constexpr size_t kBandSmemBytes =
-    (size_t)(kBandSmemW + kBandSmemAct + kBandSmemW1 + kBandNodes) * sizeof(float) + 2 * sizeof(uint64_t);
+    (size_t)(kBandSmemW + 2 * kBandSmemAct + kBandNodes) * sizeof(float) + 2 * sizeof(uint64_t);
 static_assert(kBandSmemBytes <= 227 * 1024, "band_kernel shared memory");
-static_assert(((kBandSmemW + kBandSmemAct + kBandSmemW1 + kBandNodes) * 4) % 8 == 0, "mbarrier alignment");
+static_assert(((kBandSmemW + 2 * kBandSmemAct + kBandNodes) * 4) % 8 == 0, "mbarrier alignment");
 
 struct BandNode {
     int x, y, slot, nin;   // nin = 15 or 9
@@ -798,13 +803,14 @@ struct BandNode {
     int nb_stale;          // bit q: neighbour q reads the previous step's moments
 };
 
-struct BandNet {            // weights transposed to [in][out]
-    const float* w1t;       // [nin][128]
+struct BandNet {            // fragment-ordered weights (ippi_load_band_net)
+    const float* w1f;       // layer 1 [8][2][2][32][2]
     const float* b1;        // [128]
-    const float* wht;       // [6][128][128], each layer 16-byte aligned and contiguous
+    const float* whf;       // [6][8][16][2][32][2], each layer 64 KB, 16-byte aligned
     const float* bh;        // [6][128]
     const float* wo;        // [128]
     float bo;
+    int nin;
 };
 
 struct BandArgs {
@@ -824,7 +830,7 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p)
 // the TMA engine; the mbarrier completes when all bytes have landed
 __device__ __forceinline__ void band_weights_async(float* dst, const float* src, uint64_t* bar)
 {
-    constexpr uint32_t bytes = kHidden * kHidden * sizeof(float);
+    constexpr uint32_t bytes = kBandLayerFrag * sizeof(float);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
@@ -852,43 +858,115 @@ __device__ __forceinline__ bool band_wait(uint64_t* bar, uint32_t parity)
     return false;
 }
 
-// acc[j][i] += sum over k < K of act[node 5w+j][k] * wt[k][4l+i]
-template <int K>
-__device__ __forceinline__ void band_layer(const float* __restrict__ act, const float* __restrict__ wt,
-                                           int warp, int lane, float (&acc)[kBandWarpNodes][4])
+// x = hi + lo with hi, lo TF32 (round to nearest, ties away from zero)
+__device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo)
 {
-    const float* arow = act + warp * kBandWarpNodes * kBandAct;
-    // fully unrolled: one block per SM leaves the whole register file to its
-    // 256 threads, so the shared-memory loads can run well ahead of the FMAs
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(x - __uint_as_float(hi)));
+}
+
+__device__ __forceinline__ void mma_tf32_1688(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                              uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// acc[mt][nt] += act[rows of tile mt][K] x W^T[K][columns of tile nt] in
+// 3 x TF32; wf: this layer's fragments (shared or global memory).  The
+// tensor cores' own FP32 accumulation does not round to nearest, so the
+// large hi.hi products of each k step are summed from zero and added to acc
+// by an ordinary (round-to-nearest) FP32 add; the small lo.hi + hi.lo terms,
+// 2^-11 of the result, accumulate in the tensor cores in `small`.
+template <int KSTEPS>
+__device__ __forceinline__ void band_mma_layer(const uint32_t* __restrict__ ah, const uint32_t* __restrict__ al,
+                                               const float2* __restrict__ wf, int warp, int lane,
+                                               float (&acc)[3][2][4])
+{
+    const int g = lane >> 2, t = lane & 3;
+    float small[3][2][4];
 #pragma unroll
-    for (int k = 0; k < K; k += 4) {
-        float4 x[kBandWarpNodes];
+    for (int mt = 0; mt < 3; mt++)
 #pragma unroll
-        for (int j = 0; j < kBandWarpNodes; j++) x[j] = *reinterpret_cast<const float4*>(arow + j * kBandAct + k);
+        for (int nt = 0; nt < 2; nt++)
 #pragma unroll
-        for (int kk = 0; kk < 4; kk++) {
-            const float4 w = *reinterpret_cast<const float4*>(wt + (k + kk) * kHidden + 4 * lane);
+            for (int i = 0; i < 4; i++) small[mt][nt][i] = 0.f;
+#pragma unroll 4
+    for (int ks = 0; ks < KSTEPS; ks++) {
+        uint32_t bh[2][2], bl[2][2];
 #pragma unroll
-            for (int j = 0; j < kBandWarpNodes; j++) {
-                const float xv = kk == 0 ? x[j].x : kk == 1 ? x[j].y : kk == 2 ? x[j].z : x[j].w;
-                acc[j][0] = fmaf(xv, w.x, acc[j][0]);
-                acc[j][1] = fmaf(xv, w.y, acc[j][1]);
-                acc[j][2] = fmaf(xv, w.z, acc[j][2]);
-                acc[j][3] = fmaf(xv, w.w, acc[j][3]);
+        for (int nt = 0; nt < 2; nt++) {
+            const float2 w = wf[((warp * KSTEPS + ks) * 2 + nt) * 32 + lane];
+            tf32_split(w.x, bh[nt][0], bl[nt][0]);
+            tf32_split(w.y, bh[nt][1], bl[nt][1]);
+        }
+        const int k0 = ks * 8 + t;
+#pragma unroll
+        for (int mt = 0; mt < 3; mt++) {
+            const int r0 = (mt * 16 + g) * kBandAct + k0, r1 = r0 + 8 * kBandAct;
+            const uint32_t h0 = ah[r0], h1 = ah[r1], h2 = ah[r0 + 4], h3 = ah[r1 + 4];
+            const uint32_t l0 = al[r0], l1 = al[r1], l2 = al[r0 + 4], l3 = al[r1 + 4];
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++) {
+                float big[4] = {0.f, 0.f, 0.f, 0.f};
+                mma_tf32_1688(big, h0, h1, h2, h3, bh[nt][0], bh[nt][1]);
+                mma_tf32_1688(small[mt][nt], l0, l1, l2, l3, bh[nt][0], bh[nt][1]);
+                mma_tf32_1688(small[mt][nt], h0, h1, h2, h3, bl[nt][0], bl[nt][1]);
+#pragma unroll
+                for (int i = 0; i < 4; i++) acc[mt][nt][i] += big[i];
             }
+        }
+    }
+#pragma unroll
+    for (int mt = 0; mt < 3; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+            for (int i = 0; i < 4; i++) acc[mt][nt][i] += small[mt][nt][i];
+}
+
+// accumulators <- the layer's bias
+__device__ __forceinline__ void band_bias(const float* __restrict__ bias, int warp, int lane, float (&acc)[3][2][4])
+{
+#pragma unroll
+    for (int nt = 0; nt < 2; nt++) {
+        const int c = warp * 16 + nt * 8 + 2 * (lane & 3);
+        const float b0 = bias[c], b1 = bias[c + 1];
+#pragma unroll
+        for (int mt = 0; mt < 3; mt++) {
+            acc[mt][nt][0] = acc[mt][nt][2] = b0;
+            acc[mt][nt][1] = acc[mt][nt][3] = b1;
         }
     }
 }
 
-// ReLU of the register tile into the activation rows (after every thread has
-// finished reading them)
-__device__ __forceinline__ void band_store(float* act, int warp, int lane, const float (&acc)[kBandWarpNodes][4])
+// ReLU of the accumulators into the activation rows (after every thread has
+// finished reading them): split into hi / lo, or (last) FP32 values in ah
+__device__ __forceinline__ void band_store(uint32_t* ah, uint32_t* al, int warp, int lane,
+                                           const float (&acc)[3][2][4], bool last)
 {
+    const int g = lane >> 2, t = lane & 3;
 #pragma unroll
-    for (int j = 0; j < kBandWarpNodes; j++)
-        *reinterpret_cast<float4*>(act + (warp * kBandWarpNodes + j) * kBandAct + 4 * lane) =
-            make_float4(fmaxf(acc[j][0], 0.f), fmaxf(acc[j][1], 0.f), fmaxf(acc[j][2], 0.f),
-                        fmaxf(acc[j][3], 0.f));
+    for (int mt = 0; mt < 3; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+            for (int half = 0; half < 2; half++) {
+                const int idx = (mt * 16 + g + 8 * half) * kBandAct + warp * 16 + nt * 8 + 2 * t;
+                const float v0 = fmaxf(acc[mt][nt][2 * half], 0.f), v1 = fmaxf(acc[mt][nt][2 * half + 1], 0.f);
+                if (last) {
+                    *reinterpret_cast<uint2*>(ah + idx) = make_uint2(__float_as_uint(v0), __float_as_uint(v1));
+                } else {
+                    uint32_t h0, l0, h1, l1;
+                    tf32_split(v0, h0, l0);
+                    tf32_split(v1, h1, l1);
+                    *reinterpret_cast<uint2*>(ah + idx) = make_uint2(h0, h1);
+                    *reinterpret_cast<uint2*>(al + idx) = make_uint2(l0, l1);
+                }
+            }
 }
 
 template <int S, int CO>
@@ -897,11 +975,11 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_kernel(const BandArgs ba
     using C = typename Store<S>::C;
     const StepArgs& a = ba.s;
     extern __shared__ __align__(128) float band_smem[];
-    float* wbuf = band_smem;                  // [2][128][128]
-    float* act = wbuf + kBandSmemW;           // [kBandNodes][kBandAct]
-    float* w1 = act + kBandSmemAct;           // [16][128]
-    float* outv = w1 + kBandSmemW1;           // [kBandNodes]
-    uint64_t* bar = reinterpret_cast<uint64_t*>(outv + kBandNodes);  // [2]
+    float* wbuf = band_smem;                                        // [2][kBandLayerFrag]
+    uint32_t* ah = reinterpret_cast<uint32_t*>(wbuf + kBandSmemW);  // [kBandNodes][kBandAct] TF32 hi
+    uint32_t* al = ah + kBandSmemAct;                               // [kBandNodes][kBandAct] TF32 lo
+    float* outv = reinterpret_cast<float*>(al + kBandSmemAct);      // [kBandNodes]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(outv + kBandNodes); // [2]
     const int2 w = ba.work[blockIdx.x];
     const BandNet& net = ba.net[ba.work_type[blockIdx.x]];
     const C* sm_cur = reinterpret_cast<const C*>(a.side_m) + (long long)a.par * a.nslots * 3;
@@ -916,12 +994,9 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_kernel(const BandArgs ba
     }
     __syncthreads();
     if (tid == 0) {
-        band_weights_async(wbuf, net.wht, &bar[0]);
-        band_weights_async(wbuf + kHidden * kHidden, net.wht + kHidden * kHidden, &bar[1]);
+        band_weights_async(wbuf, net.whf, &bar[0]);
+        band_weights_async(wbuf + kBandLayerFrag, net.whf + kBandLayerFrag, &bar[1]);
     }
-    // first layer's weights, zero rows beyond nin
-    for (int i = tid; i < kBandIn * kHidden; i += kBandThreads)
-        w1[i] = i / kHidden < nin ? net.w1t[i] : 0.f;
     // inputs: (u_x, u_y, rho) of each neighbour cast to float (mesh.cpp:2805-2808)
     for (int i = tid; i < kBandNodes * kBandIn; i += kBandThreads) {
         const int n = i / kBandIn, q = i % kBandIn;
@@ -933,34 +1008,29 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_kernel(const BandArgs ba
             const C* mm = m + (long long)bn.nb_slot[nb] * 3;
             v = float(comp == 0 ? mm[1] : (comp == 1 ? mm[2] : mm[0]));
         }
-        act[n * kBandAct + q] = v;
+        tf32_split(v, ah[n * kBandAct + q], al[n * kBandAct + q]);
     }
     __syncthreads();
 
-    float acc[kBandWarpNodes][4];
-    // layer 1: Linear(nin, 128) + ReLU
-#pragma unroll
-    for (int j = 0; j < kBandWarpNodes; j++)
-#pragma unroll
-        for (int i = 0; i < 4; i++) acc[j][i] = net.b1[4 * lane + i];
-    band_layer<kBandIn>(act, w1, warp, lane, acc);
+    float acc[3][2][4];
+    // layer 1: Linear(nin, 128) + ReLU; its fragments (zero beyond nin) from global memory
+    band_bias(net.b1, warp, lane, acc);
+    band_mma_layer<kBandIn / 8>(ah, al, reinterpret_cast<const float2*>(net.w1f), warp, lane, acc);
     __syncthreads();
-    band_store(act, warp, lane, acc);
+    band_store(ah, al, warp, lane, acc, false);
     __syncthreads();
     // hidden layers 2..7: Linear(128, 128) + ReLU, weights from shared memory
     bool ok = true;
     for (int l = 0; l < 6; l++) {
         const int b = l & 1;
-#pragma unroll
-        for (int j = 0; j < kBandWarpNodes; j++)
-#pragma unroll
-            for (int i = 0; i < 4; i++) acc[j][i] = net.bh[l * kHidden + 4 * lane + i];
+        band_bias(net.bh + l * kHidden, warp, lane, acc);
         ok = band_wait(&bar[b], (l >> 1) & 1) && ok;
-        band_layer<kHidden>(act, wbuf + b * kHidden * kHidden, warp, lane, acc);
+        band_mma_layer<kHidden / 8>(ah, al, reinterpret_cast<const float2*>(wbuf + b * kBandLayerFrag), warp, lane,
+                                    acc);
         __syncthreads();  // this layer's weights and inputs are read
         if (tid == 0 && l + 2 < 6)
-            band_weights_async(wbuf + b * kHidden * kHidden, net.wht + (size_t)(l + 2) * kHidden * kHidden, &bar[b]);
-        band_store(act, warp, lane, acc);
+            band_weights_async(wbuf + b * kBandLayerFrag, net.whf + (size_t)(l + 2) * kBandLayerFrag, &bar[b]);
+        band_store(ah, al, warp, lane, acc, l == 5);
         __syncthreads();
     }
     if (!ok) {
@@ -970,15 +1040,17 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_kernel(const BandArgs ba
         band_wait(&bar[0], 0);
         band_wait(&bar[1], 0);
     }
-    // output layer: Linear(128, 1)
+    // output layer: Linear(128, 1) in FP32 on the last hidden layer's values
+    const float4 wo = *reinterpret_cast<const float4*>(net.wo + 4 * lane);
+    const float* hl = reinterpret_cast<const float*>(ah);
 #pragma unroll
-    for (int j = 0; j < kBandWarpNodes; j++) {
-        const int n = warp * kBandWarpNodes + j;
-        const float4 x = *reinterpret_cast<const float4*>(act + n * kBandAct + 4 * lane);
-        float v = x.x * net.wo[4 * lane];
-        v = fmaf(x.y, net.wo[4 * lane + 1], v);
-        v = fmaf(x.z, net.wo[4 * lane + 2], v);
-        v = fmaf(x.w, net.wo[4 * lane + 3], v);
+    for (int j = 0; j < kBandNodes / kBandWarps; j++) {
+        const int n = warp * (kBandNodes / kBandWarps) + j;
+        const float4 x = *reinterpret_cast<const float4*>(hl + n * kBandAct + 4 * lane);
+        float v = x.x * wo.x;
+        v = fmaf(x.y, wo.y, v);
+        v = fmaf(x.z, wo.z, v);
+        v = fmaf(x.w, wo.w, v);
 #pragma unroll
         for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
         if (lane == 0) outv[n] = v + net.bo;
