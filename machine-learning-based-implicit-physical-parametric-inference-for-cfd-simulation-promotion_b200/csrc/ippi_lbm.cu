@@ -863,12 +863,9 @@ LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int pa
         B.work_type = h->band_type_d;
         for (int t = 0; t < 8; t++) {
             if (!h->nets[t].loaded) continue;
-            float* base = h->net_dev[t];
-            B.net[t].w1f = base;
-            B.net[t].b1 = base + kBandW1Frag;
-            B.net[t].whf = B.net[t].b1 + kHidden;
-            B.net[t].bh = B.net[t].whf + 6 * kBandLayerFrag;
-            B.net[t].wo = B.net[t].bh + 6 * kHidden;
+            char* base = reinterpret_cast<char*>(h->net_dev[t]);
+            B.net[t].w16 = reinterpret_cast<const uint16_t*>(base);
+            B.net[t].w32 = reinterpret_cast<const float*>(base + (size_t)kBandHalves * 2);
             B.net[t].nin = h->nets[t].nin;
             B.net[t].bo = h->nets[t].w.back();
         }
@@ -1368,47 +1365,46 @@ int ippi_load_band_net(ippi_lbm* h, int type, const float* w, size_t n)
     net.loaded = true;
     net.nin = nin;
     net.w.assign(w, w + n);
-    // device layout (band_kernel's tensor-core fragment order):
-    //   w1f[8 warps][2 k steps][2 output tiles][32 lanes][2]   layer 1, K padded to 16
-    //   b1[128]
-    //   whf[6][8][16 k steps][2][32][2]                         layers 2..7, 64 KB each
-    //   bh[6][128], wo[128]
-    // Lane (g, t) = (lane / 4, lane % 4) of warp w holds, for k step ks and
-    // tile nt, the mma.m16n8k8 B registers W[n][k], W[n][k + 4] with
-    // n = 16 w + 8 nt + g and k = 8 ks + t (W = torch's weight[out][in]).
-    const float* p = w;
-    std::vector<float> d((size_t)kBandW1Frag + kHidden + 6 * kBandLayerFrag + 6 * kHidden + kHidden, 0.f);
-    auto frag = [](float* out, const float* W, int nin_, int ksteps) {
-        for (int wp = 0; wp < 8; wp++)
-            for (int ks = 0; ks < ksteps; ks++)
-                for (int nt = 0; nt < 2; nt++)
-                    for (int lane = 0; lane < 32; lane++) {
-                        const int g = lane >> 2, t = lane & 3, n = 16 * wp + 8 * nt + g, k = 8 * ks + t;
-                        float* e = out + ((((size_t)wp * ksteps + ks) * 2 + nt) * 32 + lane) * 2;
-                        e[0] = k < nin_ ? W[(size_t)n * nin_ + k] : 0.f;
-                        e[1] = k + 4 < nin_ ? W[(size_t)n * nin_ + k + 4] : 0.f;
-                    }
+    // device layout (band_kernel's tensor-core operands): every weight
+    // matrix as two FP16 planes hi = fp16(W), lo = fp16((W - hi) 2^11)
+    // (round to nearest even), each in the instruction's K-major no-swizzle
+    // A layout (band_w_index):
+    //   layer 1 hi, lo [128 x 16, inputs beyond nin zero];
+    //   layers 2..7 hi, lo [128 x 128] each;
+    // then FP32 b1[128], bh[6][128], wo[128]
+    auto planes = [](uint16_t* hi, uint16_t* lo, const float* W, int nin_, int kpad) {
+        for (int m = 0; m < kHidden; m++)
+            for (int k = 0; k < kpad; k++) {
+                const float x = k < nin_ ? W[(size_t)m * nin_ + k] : 0.f;
+                const __half xh = __float2half_rn(x);
+                const __half xl = __float2half_rn((x - __half2float(xh)) * kBandLoScale);
+                std::memcpy(&hi[band_w_index(m, k)], &xh, 2);
+                std::memcpy(&lo[band_w_index(m, k)], &xl, 2);
+            }
     };
-    frag(d.data(), p, nin, kBandIn / 8);
+    const float* p = w;
+    std::vector<uint16_t> d16((size_t)kBandHalves, 0);
+    std::vector<float> d32((size_t)kBandF32, 0.f);
+    planes(d16.data(), d16.data() + kBandL1Plane, p, nin, kBandIn);
     p += kHidden * nin;
-    size_t o = kBandW1Frag;
-    for (int j = 0; j < kHidden; j++) d[o++] = p[j];
+    for (int j = 0; j < kHidden; j++) d32[kBandF32B1 + j] = p[j];
     p += kHidden;
-    const float* hp = p;
-    size_t ob = o + 6 * (size_t)kBandLayerFrag;
     for (int l = 0; l < 6; l++) {
-        const float* W = hp + (size_t)l * (kHidden * kHidden + kHidden);
-        frag(d.data() + o + (size_t)l * kBandLayerFrag, W, kHidden, kHidden / 8);
-        for (int j = 0; j < kHidden; j++) d[ob++] = W[kHidden * kHidden + j];
+        const float* W = p + (size_t)l * (kHidden * kHidden + kHidden);
+        uint16_t* hi = d16.data() + kBandOffHid + (size_t)l * 2 * kBandLayerPlane;
+        planes(hi, hi + kBandLayerPlane, W, kHidden, kHidden);
+        for (int j = 0; j < kHidden; j++) d32[kBandF32Bh + l * kHidden + j] = W[kHidden * kHidden + j];
     }
-    o = ob;
-    p = hp + 6 * (size_t)(kHidden * kHidden + kHidden);
-    for (int j = 0; j < kHidden; j++) d[o++] = p[j];
+    p += 6 * (size_t)(kHidden * kHidden + kHidden);
+    for (int j = 0; j < kHidden; j++) d32[kBandF32Wo + j] = p[j];
+    std::vector<char> d(d16.size() * 2 + d32.size() * 4);
+    std::memcpy(d.data(), d16.data(), d16.size() * 2);
+    std::memcpy(d.data() + d16.size() * 2, d32.data(), d32.size() * 4);
     CK(h, cudaStreamSynchronize(h->st));
     dfree(h->net_dev[type]);
     h->net_dev[type] = nullptr;
-    CK(h, dalloc(&h->net_dev[type], d.size() * sizeof(float)));
-    CK(h, cudaMemcpy(h->net_dev[type], d.data(), d.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(h, dalloc(&h->net_dev[type], d.size()));
+    CK(h, cudaMemcpy(h->net_dev[type], d.data(), d.size(), cudaMemcpyHostToDevice));
     return rebuild(h);
 }
 

@@ -765,37 +765,78 @@ __global__ void __launch_bounds__(256, (step_min_blocks<S, false>())) prep_kerne
 // boundary nets (Mesh::NNmodel_Type00..07, mesh.cpp:2767-3259)
 //
 // One block evaluates one net (Linear(nin,128)+ReLU, 6 x (Linear(128,128)+
-// ReLU), Linear(128,1)) on up to kBandNodes band nodes.  The seven linear
-// layers run on the tensor cores with FP32 accuracy: every operand x is
-// split into two TF32 parts x = hi + lo, and each mma.m16n8k8 product is
-// taken as lo.hi + hi.lo + hi.hi (the lo.lo term is below FP32 rounding), in
-// FP32 accumulators -- as close to libtorch's FP32 CPU forward as an FP32
-// FMA chain with another summation order.  The output layer is an FP32 dot
-// product.  Warp w owns output columns 16 w .. 16 w + 15 of all 48 rows
-// (3 x 2 tiles of 16 x 8).  Each hidden layer's weights (64 KB, stored on
-// the device in the warps' B-fragment order, so every fragment load is one
-// conflict-free 256-byte row) come into shared memory by one TMA bulk copy
-// (cp.async.bulk, completion on an mbarrier), two layer buffers deep.  The
-// activations sit in shared memory already split (hi and lo planes).
-// kBandNodes = 48 puts the 5,796 band nodes of the 2401 x 501 plate in 122
-// blocks, one wave.
+// ReLU), Linear(128,1)) on up to kBandNodes band nodes, each linear layer as
+// tensor-core products D[128 outputs][48 nodes] = W x act^T by tcgen05.mma
+// (kind::f16: FP16 operands, FP32 accumulators in tensor memory; M = 128,
+// N = 48, K = 16 per instruction).  FP32 accuracy from two FP16 parts: every
+// operand is x = hi + lo 2^-11 with hi = fp16(x) and lo = fp16((x - hi) 2^11)
+// (round to nearest; the scaled remainder stays clear of FP16's subnormals),
+// and a product is hi.hi + (hi.lo + lo.hi) 2^-11 (lo.lo is below FP32
+// rounding): 22 significant bits per operand, as many as two TF32 parts, in
+// half the instructions and bytes.  The weights come split from the host;
+// the activations are split when they are written.  The tensor cores' FP32
+// accumulation is not IEEE round-to-nearest, so the large hi.hi terms go to
+// two accumulators of 64 inputs each, which the epilogue adds with ordinary
+// FP32 adds; the scaled small terms share a third.  The output layer is an
+// FP32 dot product.
+//
+// Shared memory: two layer buffers of hi and lo weight planes (32 KB each,
+// the canonical K-major no-swizzle layout of the instruction's A operand,
+// prepared on the host; layer l + 2 is copied in by TMA bulk copies as soon
+// as layer l's products are done), the activation planes (B operand, hi and
+// lo), the output layer's partial sums and the mbarriers.  One thread issues
+// the products; sixteen warps run the epilogue (warp w reads accumulator
+// lanes 32 (w % 4) .. and nodes 12 (w / 4) ..).  Every wait is bounded.
 // ---------------------------------------------------------------------------
-constexpr int kBandWarps = 8;
-constexpr int kBandNodes = 48;                     // band nodes per block: three 16-row tiles
+constexpr int kBandWarps = 16;
+constexpr int kBandNodes = 48;                     // N of each product: band nodes per block
 constexpr int kBandThreads = 32 * kBandWarps;
-constexpr int kHidden = 128;
+constexpr int kHidden = 128;                       // M of each product: one layer's outputs
 constexpr int kBandIn = 16;                        // layer-1 inputs, zero-padded
-constexpr int kBandAct = kHidden + 4;              // words per activation row
-constexpr int kBandLayerFrag = kHidden * kHidden;  // floats of one hidden layer in fragment order
-constexpr int kBandW1Frag = kBandWarps * (kBandIn / 8) * 2 * 32 * 2;  // layer 1 in fragment order
-// dynamic shared memory of band_kernel: two hidden-layer weight buffers, the
-// activations (hi and lo planes), outputs, two mbarriers
-constexpr int kBandSmemW = 2 * kBandLayerFrag;
-constexpr int kBandSmemAct = kBandNodes * kBandAct;
-constexpr size_t kBandSmemBytes =
-    (size_t)(kBandSmemW + 2 * kBandSmemAct + kBandNodes) * sizeof(float) + 2 * sizeof(uint64_t);
+constexpr float kBandLoScale = 2048.f;             // 2^11: the lo parts' scale
+// per-net device layout: FP16 planes (layer 1 hi, lo [128 x 16]; layers 2..7
+// hi, lo [128 x 128]), then FP32 b1[128], bh[6][128], wo[128]
+constexpr int kBandL1Plane = kHidden * kBandIn;    // halves
+constexpr int kBandLayerPlane = kHidden * kHidden; // halves
+constexpr int kBandOffHid = 2 * kBandL1Plane;
+constexpr int kBandHalves = kBandOffHid + 12 * kBandLayerPlane;
+constexpr int kBandF32B1 = 0, kBandF32Bh = kHidden, kBandF32Wo = 7 * kHidden, kBandF32 = 8 * kHidden;
+static_assert(kBandHalves % 8 == 0, "16-byte aligned FP32 part");
+// A operand (weights), K-major no swizzle: 8-row x 16-byte core matrices,
+// rows (outputs) 16 B apart, row groups of 8 128 B apart, k groups of 8
+// (16 B) 2 KB apart
+constexpr uint32_t kBandWSbo = 128, kBandWLbo = (kHidden / 8) * 128;
+__host__ __device__ constexpr int band_w_index(int m, int k)  // half index in a weight plane
+{
+    return (k >> 3) * (int)(kBandWLbo / 2) + (m >> 3) * 64 + (m & 7) * 8 + (k & 7);
+}
+// B operand (activations), the same form with N = 48 nodes; the k-group
+// stride is padded by 16 B so that a warp's 32 features land in 16 banks
+constexpr uint32_t kBandASbo = 128, kBandALbo = (kBandNodes / 8) * 128 + 16;
+constexpr int kBandActPlane = (kHidden / 8) * kBandALbo;
+__device__ __forceinline__ uint32_t band_a_offset(int n, int k)  // byte offset in an activation plane
+{
+    return (uint32_t)(k >> 3) * kBandALbo + (uint32_t)(n >> 3) * 128 + (uint32_t)(n & 7) * 16 + (uint32_t)(k & 7) * 2;
+}
+// shared memory (bytes): weight buffer b at b * kBandSmWBuf, hi plane then lo
+constexpr int kBandSmWPlane = kBandLayerPlane * 2;
+constexpr int kBandSmWBuf = 2 * kBandSmWPlane;
+constexpr int kBandSmAH = 2 * kBandSmWBuf;
+constexpr int kBandSmAL = kBandSmAH + kBandActPlane;
+constexpr int kBandSmRed = kBandSmAL + kBandActPlane;        // [4][kBandNodes] output partial sums
+constexpr int kBandSmOut = kBandSmRed + 4 * kBandNodes * 4;  // [kBandNodes] net outputs
+constexpr int kBandSmBar = kBandSmOut + kBandNodes * 4;      // 3 mbarriers, tensor-memory address
+constexpr size_t kBandSmemBytes = (size_t)kBandSmBar + 3 * 8 + 8;
+static_assert(kBandActPlane % 16 == 0 && kBandSmBar % 8 == 0, "band_kernel shared-memory layout");
 static_assert(kBandSmemBytes <= 227 * 1024, "band_kernel shared memory");
-static_assert(((kBandSmemW + 2 * kBandSmemAct + kBandNodes) * 4) % 8 == 0, "mbarrier alignment");
+static_assert(kBandSmemBytes > 114 * 1024, "one band block per SM");
+// tensor memory: big accumulators at columns 0 and 64, the small one at 128
+constexpr uint32_t kBandTmemCols = 256;
+constexpr uint32_t kBandAccSmall = 128;
+// instruction descriptor (kind::f16): D F32 (bit 4), A and B F16 (0 at bits
+// 7, 10), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+constexpr uint32_t kBandIdesc = (1u << 4) | ((uint32_t)(kBandNodes >> 3) << 17) | ((uint32_t)(kHidden >> 4) << 24);
+static_assert(kBandNodes % 16 == 0 && kBandNodes <= 64, "tcgen05 N, accumulators 64 columns apart");
 
 struct BandNode {
     int x, y, slot, nin;   // nin = 15 or 9
@@ -803,12 +844,9 @@ struct BandNode {
     int nb_stale;          // bit q: neighbour q reads the previous step's moments
 };
 
-struct BandNet {            // fragment-ordered weights (ippi_load_band_net)
-    const float* w1f;       // layer 1 [8][2][2][32][2]
-    const float* b1;        // [128]
-    const float* whf;       // [6][8][16][2][32][2], each layer 64 KB, 16-byte aligned
-    const float* bh;        // [6][128]
-    const float* wo;        // [128]
+struct BandNet {
+    const uint16_t* w16;    // kBandHalves FP16 plane values, 16-byte aligned
+    const float* w32;       // kBandF32 biases and output weights
     float bo;
     int nin;
 };
@@ -826,17 +864,24 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p)
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// one layer's weights (64 KB, this GPU's global memory) into shared memory by
-// the TMA engine; the mbarrier completes when all bytes have landed
-__device__ __forceinline__ void band_weights_async(float* dst, const float* src, uint64_t* bar)
+// `bytes` (a multiple of 16) from this GPU's global memory into shared memory
+// by the TMA engine; completes `bytes` of the mbarrier's expected transfer
+__device__ __forceinline__ void band_copy(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
-    constexpr uint32_t bytes = kBandLayerFrag * sizeof(float);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
+}
+
+// one layer's two weight planes (hi at the buffer, lo one plane after it);
+// the mbarrier's phase completes when both have landed
+__device__ __forceinline__ void band_planes_async(uint32_t buf, const uint16_t* hi, uint32_t plane_bytes,
+                                                  uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(2 * plane_bytes)
+                 : "memory");
+    band_copy(buf, hi, plane_bytes, bar);
+    band_copy(buf + kBandSmWPlane, reinterpret_cast<const char*>(hi) + plane_bytes, plane_bytes, bar);
 }
 
 // wait for phase `parity` of an mbarrier, at most 2^22 polls (each poll may
@@ -858,115 +903,66 @@ __device__ __forceinline__ bool band_wait(uint64_t* bar, uint32_t parity)
     return false;
 }
 
-// x = hi + lo with hi, lo TF32 (round to nearest, ties away from zero)
-__device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo)
+// x = hi + lo 2^-11, hi and lo FP16 (round to nearest even)
+__device__ __forceinline__ void f16_split(float x, __half& hi, __half& lo)
 {
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(x - __uint_as_float(hi)));
+    hi = __float2half_rn(x);
+    lo = __float2half_rn((x - __half2float(hi)) * kBandLoScale);
 }
 
-__device__ __forceinline__ void mma_tf32_1688(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
-                                              uint32_t b0, uint32_t b1)
+// shared-memory matrix descriptor: K-major, no swizzle, start / leading
+// (k-group) / stride (8-row group) byte offsets in 16-byte units, version 1
+__device__ __forceinline__ uint64_t band_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// D (tensor memory) = A x B^T (+ D when acc), issued by one thread
+__device__ __forceinline__ void band_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc)
 {
     asm volatile(
-        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d), "l"(a), "l"(b), "r"(kBandIdesc), "r"(acc)
+        : "memory");
 }
 
-// acc[mt][nt] += act[rows of tile mt][K] x W^T[K][columns of tile nt] in
-// 3 x TF32; wf: this layer's fragments (shared or global memory).  The
-// tensor cores' own FP32 accumulation does not round to nearest, so the
-// large hi.hi products of each k step are summed from zero and added to acc
-// by an ordinary (round-to-nearest) FP32 add; the small lo.hi + hi.lo terms,
-// 2^-11 of the result, accumulate in the tensor cores in `small`.
-template <int KSTEPS>
-__device__ __forceinline__ void band_mma_layer(const uint32_t* __restrict__ ah, const uint32_t* __restrict__ al,
-                                               const float2* __restrict__ wf, int warp, int lane,
-                                               float (&acc)[3][2][4])
+// the mbarrier's arrival once every product this thread issued is done
+__device__ __forceinline__ void band_commit(uint64_t* bar)
 {
-    const int g = lane >> 2, t = lane & 3;
-    float small[3][2][4];
-#pragma unroll
-    for (int mt = 0; mt < 3; mt++)
-#pragma unroll
-        for (int nt = 0; nt < 2; nt++)
-#pragma unroll
-            for (int i = 0; i < 4; i++) small[mt][nt][i] = 0.f;
-#pragma unroll 4
-    for (int ks = 0; ks < KSTEPS; ks++) {
-        uint32_t bh[2][2], bl[2][2];
-#pragma unroll
-        for (int nt = 0; nt < 2; nt++) {
-            const float2 w = wf[((warp * KSTEPS + ks) * 2 + nt) * 32 + lane];
-            tf32_split(w.x, bh[nt][0], bl[nt][0]);
-            tf32_split(w.y, bh[nt][1], bl[nt][1]);
-        }
-        const int k0 = ks * 8 + t;
-#pragma unroll
-        for (int mt = 0; mt < 3; mt++) {
-            const int r0 = (mt * 16 + g) * kBandAct + k0, r1 = r0 + 8 * kBandAct;
-            const uint32_t h0 = ah[r0], h1 = ah[r1], h2 = ah[r0 + 4], h3 = ah[r1 + 4];
-            const uint32_t l0 = al[r0], l1 = al[r1], l2 = al[r0 + 4], l3 = al[r1 + 4];
-#pragma unroll
-            for (int nt = 0; nt < 2; nt++) {
-                float big[4] = {0.f, 0.f, 0.f, 0.f};
-                mma_tf32_1688(big, h0, h1, h2, h3, bh[nt][0], bh[nt][1]);
-                mma_tf32_1688(small[mt][nt], l0, l1, l2, l3, bh[nt][0], bh[nt][1]);
-                mma_tf32_1688(small[mt][nt], h0, h1, h2, h3, bl[nt][0], bl[nt][1]);
-#pragma unroll
-                for (int i = 0; i < 4; i++) acc[mt][nt][i] += big[i];
-            }
-        }
-    }
-#pragma unroll
-    for (int mt = 0; mt < 3; mt++)
-#pragma unroll
-        for (int nt = 0; nt < 2; nt++)
-#pragma unroll
-            for (int i = 0; i < 4; i++) acc[mt][nt][i] += small[mt][nt][i];
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
 }
 
-// accumulators <- the layer's bias
-__device__ __forceinline__ void band_bias(const float* __restrict__ bias, int warp, int lane, float (&acc)[3][2][4])
+__device__ __forceinline__ void tmem_ld4(uint32_t addr, uint32_t (&r)[4])
 {
-#pragma unroll
-    for (int nt = 0; nt < 2; nt++) {
-        const int c = warp * 16 + nt * 8 + 2 * (lane & 3);
-        const float b0 = bias[c], b1 = bias[c + 1];
-#pragma unroll
-        for (int mt = 0; mt < 3; mt++) {
-            acc[mt][nt][0] = acc[mt][nt][2] = b0;
-            acc[mt][nt][1] = acc[mt][nt][3] = b1;
-        }
-    }
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr));
 }
 
-// ReLU of the accumulators into the activation rows (after every thread has
-// finished reading them): split into hi / lo, or (last) FP32 values in ah
-__device__ __forceinline__ void band_store(uint32_t* ah, uint32_t* al, int warp, int lane,
-                                           const float (&acc)[3][2][4], bool last)
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// one layer's products from weight buffer `wb` (K = 16 ksteps): big
+// accumulator c <- hi.hi of inputs 64 c .. 64 c + 63; the small one <- hi.lo
+// + lo.hi (scaled by 2^11); the mbarrier arrives when all are done
+__device__ __forceinline__ void band_layer_mma(uint32_t tmem, uint32_t wb, uint32_t ah, uint32_t al, int ksteps,
+                                               uint64_t* bar)
 {
-    const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int mt = 0; mt < 3; mt++)
-#pragma unroll
-        for (int nt = 0; nt < 2; nt++)
-#pragma unroll
-            for (int half = 0; half < 2; half++) {
-                const int idx = (mt * 16 + g + 8 * half) * kBandAct + warp * 16 + nt * 8 + 2 * t;
-                const float v0 = fmaxf(acc[mt][nt][2 * half], 0.f), v1 = fmaxf(acc[mt][nt][2 * half + 1], 0.f);
-                if (last) {
-                    *reinterpret_cast<uint2*>(ah + idx) = make_uint2(__float_as_uint(v0), __float_as_uint(v1));
-                } else {
-                    uint32_t h0, l0, h1, l1;
-                    tf32_split(v0, h0, l0);
-                    tf32_split(v1, h1, l1);
-                    *reinterpret_cast<uint2*>(ah + idx) = make_uint2(h0, h1);
-                    *reinterpret_cast<uint2*>(al + idx) = make_uint2(l0, l1);
-                }
-            }
+    const uint32_t wl = wb + kBandSmWPlane;
+    for (int ks = 0; ks < ksteps; ks++)
+        band_mma(tmem + 64u * (uint32_t)(ks >> 2), band_desc(wb + ks * 2 * kBandWLbo, kBandWLbo, kBandWSbo),
+                 band_desc(ah + ks * 2 * kBandALbo, kBandALbo, kBandASbo), (ks & 3) != 0);
+    for (int ks = 0; ks < ksteps; ks++)
+        band_mma(tmem + kBandAccSmall, band_desc(wb + ks * 2 * kBandWLbo, kBandWLbo, kBandWSbo),
+                 band_desc(al + ks * 2 * kBandALbo, kBandALbo, kBandASbo), ks != 0);
+    for (int ks = 0; ks < ksteps; ks++)
+        band_mma(tmem + kBandAccSmall, band_desc(wl + ks * 2 * kBandWLbo, kBandWLbo, kBandWSbo),
+                 band_desc(ah + ks * 2 * kBandALbo, kBandALbo, kBandASbo), 1u);
+    band_commit(bar);
 }
 
 template <int S, int CO>
@@ -974,30 +970,40 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_kernel(const BandArgs ba
 {
     using C = typename Store<S>::C;
     const StepArgs& a = ba.s;
-    extern __shared__ __align__(128) float band_smem[];
-    float* wbuf = band_smem;                                        // [2][kBandLayerFrag]
-    uint32_t* ah = reinterpret_cast<uint32_t*>(wbuf + kBandSmemW);  // [kBandNodes][kBandAct] TF32 hi
-    uint32_t* al = ah + kBandSmemAct;                               // [kBandNodes][kBandAct] TF32 lo
-    float* outv = reinterpret_cast<float*>(al + kBandSmemAct);      // [kBandNodes]
-    uint64_t* bar = reinterpret_cast<uint64_t*>(outv + kBandNodes); // [2]
+    extern __shared__ __align__(1024) unsigned char band_smem[];
+    const uint32_t sb = smem_u32(band_smem);
+    float* red = reinterpret_cast<float*>(band_smem + kBandSmRed);
+    float* outv = reinterpret_cast<float*>(band_smem + kBandSmOut);
+    // bar[0] / bar[1]: weight buffer 0 / 1 landed; bar[2]: a layer's products done
+    uint64_t* bar = reinterpret_cast<uint64_t*>(band_smem + kBandSmBar);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 3);
     const int2 w = ba.work[blockIdx.x];
     const BandNet& net = ba.net[ba.work_type[blockIdx.x]];
+    const uint16_t* __restrict__ w16 = net.w16;
+    const float* __restrict__ w32 = net.w32;
     const C* sm_cur = reinterpret_cast<const C*>(a.side_m) + (long long)a.par * a.nslots * 3;
     const C* sm_old = reinterpret_cast<const C*>(a.side_m) + (long long)(a.par ^ 1) * a.nslots * 3;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nin = ba.nodes[w.x].nin;
 
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[0])) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[1])) : "memory");
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[i])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        // layer 1 into buffer 0, layer 2 into buffer 1
+        band_planes_async(sb, w16, kBandL1Plane * 2, &bar[0]);
+        band_planes_async(sb + kBandSmWBuf, w16 + kBandOffHid, kBandLayerPlane * 2, &bar[1]);
     }
-    __syncthreads();
-    if (tid == 0) {
-        band_weights_async(wbuf, net.whf, &bar[0]);
-        band_weights_async(wbuf + kBandLayerFrag, net.whf + kBandLayerFrag, &bar[1]);
+    __syncwarp();
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(kBandTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     // inputs: (u_x, u_y, rho) of each neighbour cast to float (mesh.cpp:2805-2808)
+#pragma unroll
     for (int i = tid; i < kBandNodes * kBandIn; i += kBandThreads) {
         const int n = i / kBandIn, q = i % kBandIn;
         float v = 0.f;
@@ -1008,54 +1014,111 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_kernel(const BandArgs ba
             const C* mm = m + (long long)bn.nb_slot[nb] * 3;
             v = float(comp == 0 ? mm[1] : (comp == 1 ? mm[2] : mm[0]));
         }
-        tf32_split(v, ah[n * kBandAct + q], al[n * kBandAct + q]);
+        __half hi, lo;
+        f16_split(v, hi, lo);
+        *reinterpret_cast<__half*>(band_smem + kBandSmAH + band_a_offset(n, q)) = hi;
+        *reinterpret_cast<__half*>(band_smem + kBandSmAL + band_a_offset(n, q)) = lo;
     }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
     __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
 
-    float acc[3][2][4];
-    // layer 1: Linear(nin, 128) + ReLU; its fragments (zero beyond nin) from global memory
-    band_bias(net.b1, warp, lane, acc);
-    band_mma_layer<kBandIn / 8>(ah, al, reinterpret_cast<const float2*>(net.w1f), warp, lane, acc);
-    __syncthreads();
-    band_store(ah, al, warp, lane, acc, false);
-    __syncthreads();
-    // hidden layers 2..7: Linear(128, 128) + ReLU, weights from shared memory
     bool ok = true;
-    for (int l = 0; l < 6; l++) {
+    const int qd = warp & 3, k = 32 * qd + lane;  // this thread's output feature in the epilogue
+    const int nb = 12 * (warp >> 2);              // and its first node
+    const uint32_t trow = tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)nb;
+    const float wo = __ldg(w32 + kBandF32Wo + k);
+    float bias = __ldg(w32 + kBandF32B1 + k);
+#pragma unroll 1
+    for (int l = 0; l < 7; l++) {
         const int b = l & 1;
-        band_bias(net.bh + l * kHidden, warp, lane, acc);
-        ok = band_wait(&bar[b], (l >> 1) & 1) && ok;
-        band_mma_layer<kHidden / 8>(ah, al, reinterpret_cast<const float2*>(wbuf + b * kBandLayerFrag), warp, lane,
-                                    acc);
-        __syncthreads();  // this layer's weights and inputs are read
-        if (tid == 0 && l + 2 < 6)
-            band_weights_async(wbuf + b * kBandLayerFrag, net.whf + (size_t)(l + 2) * kBandLayerFrag, &bar[b]);
-        band_store(ah, al, warp, lane, acc, l == 5);
+        // the next layer's bias, a layer ahead of its use
+        const float bias_next = l < 6 ? __ldg(w32 + kBandF32Bh + l * kHidden + k) : 0.f;
+        if (tid == 0) {
+            ok = band_wait(&bar[b], (l >> 1) & 1) && ok;
+            tc_fence_after();
+            band_layer_mma(tmem, sb + b * kBandSmWBuf, sb + kBandSmAH, sb + kBandSmAL,
+                           l == 0 ? kBandIn / 16 : kHidden / 16, &bar[2]);
+            if (l + 2 < 7) {
+                // layer l + 2 into this buffer once the products here are done
+                ok = band_wait(&bar[2], l & 1) && ok;
+                band_planes_async(sb + b * kBandSmWBuf, w16 + kBandOffHid + (size_t)(l + 1) * 2 * kBandLayerPlane,
+                                  kBandLayerPlane * 2, &bar[b]);
+            }
+        }
+        __syncwarp();
+        ok = band_wait(&bar[2], l & 1) && ok;
+        __syncwarp();  // the tensor-memory loads below are warp-collective
+        tc_fence_after();
+        // epilogue: bias + the three accumulators, ReLU; split into the next
+        // layer's activation planes, or (last layer) the output layer's
+        // partial sums over this warp's 32 features
+        uint32_t r[3][3][4];
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) tmem_ld4(trow + 64u * (uint32_t)c + 4u * (uint32_t)p, r[p][c]);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        float v[16];
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                float x = bias + __uint_as_float(r[p][0][j]);
+                if (l > 0) x += __uint_as_float(r[p][1][j]);
+                v[4 * p + j] = fmaxf(fmaf(__uint_as_float(r[p][2][j]), 1.f / kBandLoScale, x), 0.f);
+            }
+        if (l < 6) {
+#pragma unroll
+            for (int j = 0; j < 12; j++) {
+                __half hi, lo;
+                f16_split(v[j], hi, lo);
+                *reinterpret_cast<__half*>(band_smem + kBandSmAH + band_a_offset(nb + j, k)) = hi;
+                *reinterpret_cast<__half*>(band_smem + kBandSmAL + band_a_offset(nb + j, k)) = lo;
+            }
+        } else {
+            // output layer: the warp's 32 features of v * wo summed per node
+            // by a reduce-scatter (lane L ends with node L % 16)
+#pragma unroll
+            for (int j = 0; j < 16; j++) v[j] = j < 12 ? v[j] * wo : 0.f;
+#pragma unroll
+            for (int o = 8; o >= 1; o >>= 1) {
+                const bool up = lane & o;
+#pragma unroll
+                for (int i = 0; i < o; i++) {
+                    const float send = up ? v[i] : v[i + o];
+                    const float keep = up ? v[i + o] : v[i];
+                    v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+                }
+            }
+            v[0] += __shfl_xor_sync(0xffffffffu, v[0], 16);
+            if (lane < 12) red[qd * kBandNodes + nb + lane] = v[0];
+        }
+        bias = bias_next;
+        tc_fence_before();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
     }
-    if (!ok) {
-        // a weight copy did not land in time: report it, and give the copies
-        // still in flight one more bounded wait before the block exits
-        if (tid == 0) atomicExch(&a.ctr->err, 3);
-        band_wait(&bar[0], 0);
+    if (tid < kBandNodes)
+        outv[tid] = ((red[tid] + red[kBandNodes + tid]) + (red[2 * kBandNodes + tid] + red[3 * kBandNodes + tid])) +
+                    net.bo;
+    if (!ok && tid == 0) {
+        // a wait ran out: report it, and give what may still be in flight one
+        // more bounded wait before the tensor memory is freed
+        atomicExch(&a.ctr->err, 3);
+        band_wait(&bar[2], 0);
+        band_wait(&bar[0], 1);
         band_wait(&bar[1], 0);
     }
-    // output layer: Linear(128, 1) in FP32 on the last hidden layer's values
-    const float4 wo = *reinterpret_cast<const float4*>(net.wo + 4 * lane);
-    const float* hl = reinterpret_cast<const float*>(ah);
-#pragma unroll
-    for (int j = 0; j < kBandNodes / kBandWarps; j++) {
-        const int n = warp * (kBandNodes / kBandWarps) + j;
-        const float4 x = *reinterpret_cast<const float4*>(hl + n * kBandAct + 4 * lane);
-        float v = x.x * wo.x;
-        v = fmaf(x.y, wo.y, v);
-        v = fmaf(x.z, wo.z, v);
-        v = fmaf(x.w, wo.w, v);
-#pragma unroll
-        for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if (lane == 0) outv[n] = v + net.bo;
-    }
     __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kBandTmemCols)
+                     : "memory");
+    }
+
 
     // tau (net output if >= 0.501, else Smagorinsky; mesh.cpp:2821-2827,
     // 392-396) and the collision of the band node
