@@ -93,6 +93,7 @@ struct ippi_lbm {
     BandNode* band_nodes_d = nullptr;
     int2* band_work_d = nullptr;
     int* band_type_d = nullptr;
+    int* band_in_d = nullptr;  // [blocks][kBandNodes][5] net input slots
     int band_blocks = 0;
     // immersed boundary
     int nmark = 0, nbody = 0, nforced = 0, hist_cap = 0;
@@ -632,6 +633,8 @@ int rebuild(ippi_lbm* h)
     dfree(h->band_nodes_d);
     dfree(h->band_work_d);
     dfree(h->band_type_d);
+    dfree(h->band_in_d);
+    h->band_in_d = nullptr;
     h->band_nodes_d = nullptr;
     h->band_work_d = nullptr;
     h->band_type_d = nullptr;
@@ -640,6 +643,7 @@ int rebuild(ippi_lbm* h)
         std::vector<BandNode> nodes;
         std::vector<int2> work;
         std::vector<int> wtype;
+        std::vector<int> in_slot;  // per block, node and neighbour: 2 slot + stale, or -1
         for (int t = 0; t < 8; t++) {
             int first = (int)nodes.size();
             for (auto& kv : band) {
@@ -660,12 +664,21 @@ int rebuild(ippi_lbm* h)
             for (int s0 = first; s0 < (int)nodes.size(); s0 += kBandNodes) {
                 work.push_back(make_int2(s0, std::min(kBandNodes, (int)nodes.size() - s0)));
                 wtype.push_back(t);
+                for (int n = 0; n < kBandNodes; n++)
+                    for (int q = 0; q < 5; q++) {
+                        int code = -1;
+                        if (s0 + n < (int)nodes.size() && 3 * q < nodes[s0 + n].nin)
+                            code = 2 * nodes[s0 + n].nb_slot[q] + ((nodes[s0 + n].nb_stale >> q) & 1);
+                        in_slot.push_back(code);
+                    }
             }
         }
         h->band_nodes = nodes;
         CK(h, dalloc(&h->band_nodes_d, nodes.size() * sizeof(BandNode)));
         CK(h, dalloc(&h->band_work_d, work.size() * sizeof(int2)));
         CK(h, dalloc(&h->band_type_d, wtype.size() * sizeof(int)));
+        CK(h, dalloc(&h->band_in_d, in_slot.size() * sizeof(int)));
+        CK(h, cudaMemcpy(h->band_in_d, in_slot.data(), in_slot.size() * sizeof(int), cudaMemcpyHostToDevice));
         CK(h, cudaMemcpy(h->band_nodes_d, nodes.data(), nodes.size() * sizeof(BandNode), cudaMemcpyHostToDevice));
         CK(h, cudaMemcpy(h->band_work_d, work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice));
         CK(h, cudaMemcpy(h->band_type_d, wtype.data(), wtype.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -861,6 +874,7 @@ LaunchSet make_launch(ippi_lbm* h, int mode, const void* fin, void* fout, int pa
         B.nodes = h->band_nodes_d;
         B.work = h->band_work_d;
         B.work_type = h->band_type_d;
+        B.in_slot = h->band_in_d;
         for (int t = 0; t < 8; t++) {
             if (!h->nets[t].loaded) continue;
             char* base = reinterpret_cast<char*>(h->net_dev[t]);
@@ -1213,6 +1227,7 @@ int ippi_destroy(ippi_lbm* h)
     dfree(h->band_nodes_d);
     dfree(h->band_work_d);
     dfree(h->band_type_d);
+    dfree(h->band_in_d);
     for (auto& b : h->ib_bufs) dfree(b.p);
     if (h->fork) cudaEventDestroy(h->fork);
     if (h->join) cudaEventDestroy(h->join);

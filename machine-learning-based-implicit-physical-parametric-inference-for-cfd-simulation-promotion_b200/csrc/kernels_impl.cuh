@@ -80,6 +80,54 @@ static void launch_merged(const LaunchSet& L)
     }
 }
 
+// the boundary nets' kernel (dynamic shared memory: two weight buffers and
+// the activations, allowed once per device by band_setup); `pdl`: launched as
+// the programmatic dependent of the kernel before it on the stream
+template <int S, int CO>
+static void launch_band(const LaunchSet& L, cudaStream_t st, bool pdl)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(L.band_blocks);
+    cfg.blockDim = dim3(kBandThreads);
+    cfg.dynamicSmemBytes = kBandSmemBytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = L.side_prio;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 2 : 1;
+    cudaLaunchKernelEx(&cfg, band_kernel<S, CO>, L.band_args);
+}
+
+// A normal step with boundary nets (no markers), in one stream: prep_kernel,
+// then band_kernel as its programmatic dependent, then the bulk kernel as
+// band_kernel's.  Each primary lets its dependent launch from its first
+// instruction, so the band blocks are resident (waiting for prep's moments)
+// before the bulk row segments take the rest of the GPU, and the nets run
+// beside the bulk step instead of after it.  The bulk grid's last block waits
+// for band_kernel's completion, so the step ends after all three.
+template <int S, int CO, int SC>
+static void launch_band_step(const LaunchSet& L)
+{
+    launch_prio(prep_kernel<S, SC>, (L.nprep + 255) / 256, 256, L.stream, L.side_prio, L.step, L.prep, L.nprep);
+    launch_band<S, CO>(L, L.stream, true);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = L.grid;
+    cfg.blockDim = dim3(kBlockX);
+    cfg.stream = L.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (L.avg_on)
+        cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, false, 0, 1>, L.step);
+    else
+        cudaLaunchKernelEx(&cfg, step_fast<S, CO, SC, false, 0, 0>, L.step);
+}
+
 template <int S, int CO, int SC, bool LRN, int XT = 0>
 static cudaError_t launch_tpl(const LaunchSet& L)
 {
@@ -135,6 +183,10 @@ static cudaError_t launch_tpl(const LaunchSet& L)
         launch_merged<S, CO, SC, LRN, 0>(L);
         return cudaGetLastError();
     }
+    if (!LRN && !XT && L.step.mode == MODE_STEP && L.band && L.nprep > 0 && !L.ib && !L.events) {
+        launch_band_step<S, CO, SC>(L);
+        return cudaGetLastError();
+    }
     const bool side = L.nprep > 0 || L.band || L.ib;
     if (side) {
         cudaEventRecord(L.fork, L.stream);
@@ -143,21 +195,7 @@ static cudaError_t launch_tpl(const LaunchSet& L)
         if (L.nprep > 0)
             launch_prio(prep_kernel<S, SC>, (L.nprep + 255) / 256, 256, L.side, L.side_prio, L.step,
                         L.prep, L.nprep);
-        if (L.band) {
-            // dynamic shared memory (two hidden-layer weight buffers and the
-            // activations), allowed once per device by band_setup
-            cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3(L.band_blocks);
-            cfg.blockDim = dim3(kBandThreads);
-            cfg.dynamicSmemBytes = kBandSmemBytes;
-            cfg.stream = L.side;
-            cudaLaunchAttribute attr[1];
-            attr[0].id = cudaLaunchAttributePriority;
-            attr[0].val.priority = L.side_prio;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            cudaLaunchKernelEx(&cfg, band_kernel<S, CO>, L.band_args);
-        }
+        if (L.band) launch_band<S, CO>(L, L.side, false);
         if (L.ib) launch_ib<S, SC, CO, LRN>(L, L.side);
         if (L.events) cudaEventRecord(L.events[3], L.side);
         cudaEventRecord(L.join, L.side);

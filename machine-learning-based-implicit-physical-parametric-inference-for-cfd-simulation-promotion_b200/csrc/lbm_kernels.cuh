@@ -724,6 +724,13 @@ __device__ __forceinline__ void bulk_tile_any(const StepArgs& a, int bx, int by,
 template <int S, int CO, int SC, bool LRN, int XT = 0, int AV = 0>
 __global__ void __launch_bounds__(kBlockX, (step_min_blocks<S, LRN>())) step_fast(const StepArgs ap)
 {
+    // When launched as a programmatic dependent (the boundary-net step), the
+    // grid's last block waits for its primary to complete, so the grid cannot
+    // complete before it; it is scheduled last and waits on a grid that was
+    // resident before any bulk block started, so there is no circular wait.
+    // Without a primary the wait returns at once.
+    if (blockIdx.x == gridDim.x - 1 && blockIdx.y == gridDim.y - 1 && threadIdx.x == 0)
+        asm volatile("griddepcontrol.wait;" ::: "memory");
     bulk_tile_any<S, CO, SC, LRN, XT, AV>(ap, blockIdx.x, blockIdx.y, threadIdx.x);
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
         ap.ctr->t[ap.par ^ 1] = __ldcg(&ap.ctr->t[ap.par]) + 1;
@@ -743,6 +750,9 @@ template <int S, int SC>
 __global__ void __launch_bounds__(256, (step_min_blocks<S, false>())) prep_kernel(const StepArgs a, const PrepNode* nodes, int n)
 {
     using C = typename Store<S>::C;
+    // band_kernel, when launched as this grid's programmatic dependent, may
+    // start now: it waits for this grid's results itself
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const PrepNode pn = nodes[i];
@@ -855,6 +865,7 @@ struct BandArgs {
     const BandNode* nodes;
     const int2* work;       // per block: (first node, count <= kBandNodes); all of one net type
     const int* work_type;
+    const int* in_slot;     // per block, node and neighbour q: 2 slot + (reads the previous step), or -1
     BandNet net[8];
     StepArgs s;
 };
@@ -984,7 +995,9 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_kernel(const BandArgs ba
     const C* sm_cur = reinterpret_cast<const C*>(a.side_m) + (long long)a.par * a.nslots * 3;
     const C* sm_old = reinterpret_cast<const C*>(a.side_m) + (long long)(a.par ^ 1) * a.nslots * 3;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nin = ba.nodes[w.x].nin;
+    // the bulk kernel, when launched as this grid's programmatic dependent,
+    // may start once every block of this grid is resident
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
     if (tid == 0) {
 #pragma unroll
@@ -1002,22 +1015,34 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_kernel(const BandArgs ba
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    // inputs: (u_x, u_y, rho) of each neighbour cast to float (mesh.cpp:2805-2808)
-#pragma unroll
-    for (int i = tid; i < kBandNodes * kBandIn; i += kBandThreads) {
-        const int n = i / kBandIn, q = i % kBandIn;
-        float v = 0.f;
-        if (n < w.y && q < nin) {
-            const BandNode& bn = ba.nodes[w.x + n];
-            const int nb = q / 3, comp = q % 3;
-            const C* m = ((bn.nb_stale >> nb) & 1) ? sm_old : sm_cur;
-            const C* mm = m + (long long)bn.nb_slot[nb] * 3;
-            v = float(comp == 0 ? mm[1] : (comp == 1 ? mm[2] : mm[0]));
+    // inputs: (u_x, u_y, rho) of each neighbour cast to float (mesh.cpp:2805-2808);
+    // thread t < 5 kBandNodes fills inputs 3 q .. 3 q + 2 of node t / 5 (q =
+    // t % 5), the next kBandNodes threads the zero padding (input 15)
+    static_assert(kBandIn == 16 && 6 * kBandNodes <= kBandThreads, "input staging");
+    // prep_kernel's moments and populations: complete once its grid is (a
+    // no-op without a programmatic primary)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (tid < 5 * kBandNodes) {
+        const int n = tid / 5, q = tid % 5;
+        const int code = __ldg(ba.in_slot + (size_t)blockIdx.x * kBandNodes * 5 + tid);
+        float v[3] = {0.f, 0.f, 0.f};
+        if (code >= 0) {
+            const C* mm = ((code & 1) ? sm_old : sm_cur) + (long long)(code >> 1) * 3;
+            v[0] = float(mm[1]);
+            v[1] = float(mm[2]);
+            v[2] = float(mm[0]);
         }
-        __half hi, lo;
-        f16_split(v, hi, lo);
-        *reinterpret_cast<__half*>(band_smem + kBandSmAH + band_a_offset(n, q)) = hi;
-        *reinterpret_cast<__half*>(band_smem + kBandSmAL + band_a_offset(n, q)) = lo;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            __half hi, lo;
+            f16_split(v[c], hi, lo);
+            *reinterpret_cast<__half*>(band_smem + kBandSmAH + band_a_offset(n, 3 * q + c)) = hi;
+            *reinterpret_cast<__half*>(band_smem + kBandSmAL + band_a_offset(n, 3 * q + c)) = lo;
+        }
+    } else if (tid < 6 * kBandNodes) {
+        const int n = tid - 5 * kBandNodes;
+        *reinterpret_cast<__half*>(band_smem + kBandSmAH + band_a_offset(n, 15)) = __float2half_rn(0.f);
+        *reinterpret_cast<__half*>(band_smem + kBandSmAL + band_a_offset(n, 15)) = __float2half_rn(0.f);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
