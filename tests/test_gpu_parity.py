@@ -85,6 +85,29 @@ def test_plate_fp64_with_boundary_nets():
         assert np.array_equal(g.download(ip.FIELD_NNFLAG), o.get(po.NNFLAG))
 
 
+def test_boundary_net_outputs_match_torch_forward():
+    """The nets' outputs themselves (tau where a net set it, after one step
+    from rest and after a few): the tensor-core evaluation (FP16 hi/lo
+    operand parts, FP32 sums) against the oracle's FP32 forward, pinned to
+    torch's outputs, within 5e-7 absolute on outputs near 0.5 (8 FP32 ulp;
+    1.2e-7 measured on a B200)."""
+    o, g = pair(416, 12, tau0=0.52)
+    for t, w in NETS.items():
+        o.load_band_net(t, w)
+        g.load_band_net(t, w)
+    worst = 0.0
+    for n in (1, 3):
+        o.step(n, 1)
+        g.step(n, 1)
+        flag = g.download(ip.FIELD_NNFLAG)
+        assert np.array_equal(flag, o.get(po.NNFLAG))
+        net = flag > 0
+        assert net.any()
+        worst = max(worst, float(np.abs(g.download(ip.FIELD_TAU)[net] - o.get(po.TAU)[net]).max()))
+    print(f"largest net-output difference {worst:.3e}")
+    assert worst <= 5e-7
+
+
 def test_plate_fp32_one_step_tolerance():
     o, g = pair(416, 24, storage=ip.F32, collision=ip.MRT, tau0=0.53)
     rng = np.random.default_rng(1)
