@@ -194,6 +194,24 @@ def test_graph_and_single_launches_agree():
     assert np.array_equal(a.download(ip.FIELD_F), b.download(ip.FIELD_F))
 
 
+@pytest.mark.parametrize("storage", [ip.F32, ip.F64])
+def test_net_step_chain_matches_side_stream_form(storage):
+    """The plate step with boundary nets runs prep, nets and bulk kernels as
+    a chain of programmatic dependent launches; the timed form
+    (ippi_profile_steps) runs the same kernels with the nets on a side
+    stream joined by events.  Both orders must give the same bits: the nets
+    read prep's moments only after its grid completed, and the step ends
+    only after the nets."""
+    (_, a), (_, b) = pair(416, 24, storage, tau0=0.52), pair(416, 24, storage, tau0=0.52)
+    for t, w in NETS.items():
+        a.load_band_net(t, w)
+        b.load_band_net(t, w)
+    a.step(12, 1)
+    b.profile_steps(12, 1)
+    for fld in (ip.FIELD_F, ip.FIELD_TAU, ip.FIELD_NNFLAG):
+        assert np.array_equal(a.download(fld), b.download(fld))
+
+
 def test_divergence_is_reported_not_faulted():
     g = ip.Lattice(64, 16, storage=ip.F64)
     rho = np.ones((16, 64))
