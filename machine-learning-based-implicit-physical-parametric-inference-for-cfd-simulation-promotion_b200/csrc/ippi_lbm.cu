@@ -93,7 +93,7 @@ struct ippi_lbm {
     BandNode* band_nodes_d = nullptr;
     int2* band_work_d = nullptr;
     int* band_type_d = nullptr;
-    int* band_in_d = nullptr;  // [blocks][kBandNodes][5] net input slots
+    int* band_in_d = nullptr;  // [blocks][band_nodes][5] net input slots
     int band_blocks = 0;
     // immersed boundary
     int nmark = 0, nbody = 0, nforced = 0, hist_cap = 0;
@@ -644,6 +644,7 @@ int rebuild(ippi_lbm* h)
         std::vector<int2> work;
         std::vector<int> wtype;
         std::vector<int> in_slot;  // per block, node and neighbour: 2 slot + stale, or -1
+        const int nb_blk = band_nodes(h->p.storage);  // band nodes per block of band_kernel
         for (int t = 0; t < 8; t++) {
             int first = (int)nodes.size();
             for (auto& kv : band) {
@@ -661,10 +662,10 @@ int rebuild(ippi_lbm* h)
                 }
                 nodes.push_back(b);
             }
-            for (int s0 = first; s0 < (int)nodes.size(); s0 += kBandNodes) {
-                work.push_back(make_int2(s0, std::min(kBandNodes, (int)nodes.size() - s0)));
+            for (int s0 = first; s0 < (int)nodes.size(); s0 += nb_blk) {
+                work.push_back(make_int2(s0, std::min(nb_blk, (int)nodes.size() - s0)));
                 wtype.push_back(t);
-                for (int n = 0; n < kBandNodes; n++)
+                for (int n = 0; n < nb_blk; n++)
                     for (int q = 0; q < 5; q++) {
                         int code = -1;
                         if (s0 + n < (int)nodes.size() && 3 * q < nodes[s0 + n].nin)

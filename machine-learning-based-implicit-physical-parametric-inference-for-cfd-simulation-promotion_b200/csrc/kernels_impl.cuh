@@ -89,7 +89,7 @@ static void launch_band(const LaunchSet& L, cudaStream_t st, bool pdl)
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(L.band_blocks);
     cfg.blockDim = dim3(kBandThreads);
-    cfg.dynamicSmemBytes = kBandSmemBytes;
+    cfg.dynamicSmemBytes = BandShapeOf<S>::SmemBytes;
     cfg.stream = st;
     cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributePriority;
@@ -216,11 +216,11 @@ template <int S>
 static cudaError_t band_setup()
 {
     for (cudaError_t e : {cudaFuncSetAttribute(band_kernel<S, CO_BGK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)kBandSmemBytes),
+                                               (int)BandShapeOf<S>::SmemBytes),
                           cudaFuncSetAttribute(band_kernel<S, CO_MRT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)kBandSmemBytes),
+                                               (int)BandShapeOf<S>::SmemBytes),
                           cudaFuncSetAttribute(band_kernel<S, CO_RR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)kBandSmemBytes)})
+                                               (int)BandShapeOf<S>::SmemBytes)})
         if (e != cudaSuccess) return e;
     return cudaSuccess;
 }

@@ -775,10 +775,10 @@ __global__ void __launch_bounds__(256, (step_min_blocks<S, false>())) prep_kerne
 // boundary nets (Mesh::NNmodel_Type00..07, mesh.cpp:2767-3259)
 //
 // One block evaluates one net (Linear(nin,128)+ReLU, 6 x (Linear(128,128)+
-// ReLU), Linear(128,1)) on up to kBandNodes band nodes, each linear layer as
-// tensor-core products D[128 outputs][48 nodes] = W x act^T by tcgen05.mma
+// ReLU), Linear(128,1)) on up to band_nodes band nodes, each linear layer as
+// tensor-core products D[128 outputs][N nodes] = W x act^T by tcgen05.mma
 // (kind::f16: FP16 operands, FP32 accumulators in tensor memory; M = 128,
-// N = 48, K = 16 per instruction).  FP32 accuracy from two FP16 parts: every
+// N = 48 or 96, K = 16 per instruction).  FP32 accuracy from two FP16 parts: every
 // operand is x = hi + lo 2^-11 with hi = fp16(x) and lo = fp16((x - hi) 2^11)
 // (round to nearest; the scaled remainder stays clear of FP16's subnormals),
 // and a product is hi.hi + (hi.lo + lo.hi) 2^-11 (lo.lo is below FP32
@@ -796,10 +796,9 @@ __global__ void __launch_bounds__(256, (step_min_blocks<S, false>())) prep_kerne
 // as layer l's products are done), the activation planes (B operand, hi and
 // lo), the output layer's partial sums and the mbarriers.  One thread issues
 // the products; sixteen warps run the epilogue (warp w reads accumulator
-// lanes 32 (w % 4) .. and nodes 12 (w / 4) ..).  Every wait is bounded.
+// lanes 32 (w % 4) .. and a quarter of the nodes).  Every wait is bounded.
 // ---------------------------------------------------------------------------
 constexpr int kBandWarps = 16;
-constexpr int kBandNodes = 48;                     // N of each product: band nodes per block
 constexpr int kBandThreads = 32 * kBandWarps;
 constexpr int kHidden = 128;                       // M of each product: one layer's outputs
 constexpr int kBandIn = 16;                        // layer-1 inputs, zero-padded
@@ -820,33 +819,55 @@ __host__ __device__ constexpr int band_w_index(int m, int k)  // half index in a
 {
     return (k >> 3) * (int)(kBandWLbo / 2) + (m >> 3) * 64 + (m & 7) * 8 + (k & 7);
 }
-// B operand (activations), the same form with N = 48 nodes; the k-group
-// stride is padded by 16 B so that a warp's 32 features land in 16 banks
-constexpr uint32_t kBandASbo = 128, kBandALbo = (kBandNodes / 8) * 128 + 16;
-constexpr int kBandActPlane = (kHidden / 8) * kBandALbo;
-__device__ __forceinline__ uint32_t band_a_offset(int n, int k)  // byte offset in an activation plane
-{
-    return (uint32_t)(k >> 3) * kBandALbo + (uint32_t)(n >> 3) * 128 + (uint32_t)(n & 7) * 16 + (uint32_t)(k & 7) * 2;
-}
 // shared memory (bytes): weight buffer b at b * kBandSmWBuf, hi plane then lo
 constexpr int kBandSmWPlane = kBandLayerPlane * 2;
 constexpr int kBandSmWBuf = 2 * kBandSmWPlane;
-constexpr int kBandSmAH = 2 * kBandSmWBuf;
-constexpr int kBandSmAL = kBandSmAH + kBandActPlane;
-constexpr int kBandSmRed = kBandSmAL + kBandActPlane;        // [4][kBandNodes] output partial sums
-constexpr int kBandSmOut = kBandSmRed + 4 * kBandNodes * 4;  // [kBandNodes] net outputs
-constexpr int kBandSmBar = kBandSmOut + kBandNodes * 4;      // 3 mbarriers, tensor-memory address
-constexpr size_t kBandSmemBytes = (size_t)kBandSmBar + 3 * 8 + 8;
-static_assert(kBandActPlane % 16 == 0 && kBandSmBar % 8 == 0, "band_kernel shared-memory layout");
-static_assert(kBandSmemBytes <= 227 * 1024, "band_kernel shared memory");
-static_assert(kBandSmemBytes > 114 * 1024, "one band block per SM");
-// tensor memory: big accumulators at columns 0 and 64, the small one at 128
-constexpr uint32_t kBandTmemCols = 256;
-constexpr uint32_t kBandAccSmall = 128;
-// instruction descriptor (kind::f16): D F32 (bit 4), A and B F16 (0 at bits
-// 7, 10), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
-constexpr uint32_t kBandIdesc = (1u << 4) | ((uint32_t)(kBandNodes >> 3) << 17) | ((uint32_t)(kHidden >> 4) << 24);
-static_assert(kBandNodes % 16 == 0 && kBandNodes <= 64, "tcgen05 N, accumulators 64 columns apart");
+
+// Band nodes per block, N of each product: 96 with FP64 storage (there the
+// bulk step is the longer leg, and fewer band blocks leave it more of the
+// GPU), 48 otherwise (there the nets are the longer leg).
+__host__ __device__ constexpr int band_nodes(int storage) { return storage == ST_F64 ? 96 : 48; }
+
+// The block's layout for N = NB nodes.
+template <int NB>
+struct BandShape {
+    // B operand (activations), K-major no swizzle with N = NB rows; the
+    // k-group stride is padded by 16 B so that a warp's 32 features land in
+    // 16 banks
+    static constexpr uint32_t ASbo = 128, ALbo = (NB / 8) * 128 + 16;
+    static constexpr int ActPlane = (kHidden / 8) * ALbo;
+    // shared memory (bytes): the two weight buffers, the activation planes,
+    // [4][NB] output partial sums, [NB] net outputs, 3 mbarriers and the
+    // tensor-memory address
+    static constexpr int SmAH = 2 * kBandSmWBuf;
+    static constexpr int SmAL = SmAH + ActPlane;
+    static constexpr int SmRed = SmAL + ActPlane;
+    static constexpr int SmOut = SmRed + 4 * NB * 4;
+    static constexpr int SmBar = SmOut + NB * 4;
+    static constexpr size_t SmemBytes = (size_t)SmBar + 3 * 8 + 8;
+    // tensor memory: big accumulators at columns 0 and Acc, the small one at 2 Acc
+    static constexpr uint32_t Acc = NB <= 64 ? 64 : 128;
+    static constexpr uint32_t TmemCols = NB <= 64 ? 256 : 512;
+    static constexpr uint32_t AccSmall = 2 * Acc;
+    // the epilogue: warp w takes features 32 (w % 4) .. of nodes WarpNodes
+    // (w / 4) .., in chunks of 12
+    static constexpr int WarpNodes = NB / 4;
+    // instruction descriptor (kind::f16): D F32 (bit 4), A and B F16 (0 at
+    // bits 7, 10), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+    static constexpr uint32_t Idesc = (1u << 4) | ((uint32_t)(NB >> 3) << 17) | ((uint32_t)(kHidden >> 4) << 24);
+    static_assert(NB % 16 == 0 && NB <= 128, "tcgen05 N, accumulators Acc columns apart");
+    static_assert(WarpNodes % 12 == 0, "epilogue chunks");
+    static_assert(ActPlane % 16 == 0 && SmBar % 8 == 0, "band_kernel shared-memory layout");
+    static_assert(SmemBytes <= 227 * 1024, "band_kernel shared memory");
+    static_assert(SmemBytes > 114 * 1024, "one band block per SM: two would share tensor memory");
+    // byte offset of (node n, feature k) in an activation plane
+    __device__ static uint32_t a_offset(int n, int k)
+    {
+        return (uint32_t)(k >> 3) * ALbo + (uint32_t)(n >> 3) * 128 + (uint32_t)(n & 7) * 16 + (uint32_t)(k & 7) * 2;
+    }
+};
+template <int S>
+using BandShapeOf = BandShape<band_nodes(S)>;
 
 struct BandNode {
     int x, y, slot, nin;   // nin = 15 or 9
@@ -863,7 +884,7 @@ struct BandNet {
 
 struct BandArgs {
     const BandNode* nodes;
-    const int2* work;       // per block: (first node, count <= kBandNodes); all of one net type
+    const int2* work;       // per block: (first node, count <= band_nodes); all of one net type
     const int* work_type;
     const int* in_slot;     // per block, node and neighbour q: 2 slot + (reads the previous step), or -1
     BandNet net[8];
@@ -930,12 +951,12 @@ __device__ __forceinline__ uint64_t band_desc(uint32_t saddr, uint32_t lbo, uint
 }
 
 // D (tensor memory) = A x B^T (+ D when acc), issued by one thread
-__device__ __forceinline__ void band_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc)
+__device__ __forceinline__ void band_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
 {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(d), "l"(a), "l"(b), "r"(kBandIdesc), "r"(acc)
+        ::"r"(d), "l"(a), "l"(b), "r"(idesc), "r"(acc)
         : "memory");
 }
 
@@ -960,19 +981,21 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 // one layer's products from weight buffer `wb` (K = 16 ksteps): big
 // accumulator c <- hi.hi of inputs 64 c .. 64 c + 63; the small one <- hi.lo
 // + lo.hi (scaled by 2^11); the mbarrier arrives when all are done
+template <int NB>
 __device__ __forceinline__ void band_layer_mma(uint32_t tmem, uint32_t wb, uint32_t ah, uint32_t al, int ksteps,
                                                uint64_t* bar)
 {
+    using B = BandShape<NB>;
     const uint32_t wl = wb + kBandSmWPlane;
     for (int ks = 0; ks < ksteps; ks++)
-        band_mma(tmem + 64u * (uint32_t)(ks >> 2), band_desc(wb + ks * 2 * kBandWLbo, kBandWLbo, kBandWSbo),
-                 band_desc(ah + ks * 2 * kBandALbo, kBandALbo, kBandASbo), (ks & 3) != 0);
+        band_mma(tmem + B::Acc * (uint32_t)(ks >> 2), band_desc(wb + ks * 2 * kBandWLbo, kBandWLbo, kBandWSbo),
+                 band_desc(ah + ks * 2 * B::ALbo, B::ALbo, B::ASbo), B::Idesc, (ks & 3) != 0);
     for (int ks = 0; ks < ksteps; ks++)
-        band_mma(tmem + kBandAccSmall, band_desc(wb + ks * 2 * kBandWLbo, kBandWLbo, kBandWSbo),
-                 band_desc(al + ks * 2 * kBandALbo, kBandALbo, kBandASbo), ks != 0);
+        band_mma(tmem + B::AccSmall, band_desc(wb + ks * 2 * kBandWLbo, kBandWLbo, kBandWSbo),
+                 band_desc(al + ks * 2 * B::ALbo, B::ALbo, B::ASbo), B::Idesc, ks != 0);
     for (int ks = 0; ks < ksteps; ks++)
-        band_mma(tmem + kBandAccSmall, band_desc(wl + ks * 2 * kBandWLbo, kBandWLbo, kBandWSbo),
-                 band_desc(ah + ks * 2 * kBandALbo, kBandALbo, kBandASbo), 1u);
+        band_mma(tmem + B::AccSmall, band_desc(wl + ks * 2 * kBandWLbo, kBandWLbo, kBandWSbo),
+                 band_desc(ah + ks * 2 * B::ALbo, B::ALbo, B::ASbo), B::Idesc, 1u);
     band_commit(bar);
 }
 
@@ -984,13 +1007,15 @@ template <int S, int CO>
 __global__ void __launch_bounds__(kBandThreads, S == ST_F64 ? 2 : 1) band_kernel(const BandArgs ba)
 {
     using C = typename Store<S>::C;
+    constexpr int NB = band_nodes(S);
+    using BS = BandShape<NB>;
     const StepArgs& a = ba.s;
     extern __shared__ __align__(1024) unsigned char band_smem[];
     const uint32_t sb = smem_u32(band_smem);
-    float* red = reinterpret_cast<float*>(band_smem + kBandSmRed);
-    float* outv = reinterpret_cast<float*>(band_smem + kBandSmOut);
+    float* red = reinterpret_cast<float*>(band_smem + BS::SmRed);
+    float* outv = reinterpret_cast<float*>(band_smem + BS::SmOut);
     // bar[0] / bar[1]: weight buffer 0 / 1 landed; bar[2]: a layer's products done
-    uint64_t* bar = reinterpret_cast<uint64_t*>(band_smem + kBandSmBar);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(band_smem + BS::SmBar);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 3);
     const int2 w = ba.work[blockIdx.x];
     const BandNet& net = ba.net[ba.work_type[blockIdx.x]];
@@ -1015,38 +1040,41 @@ __global__ void __launch_bounds__(kBandThreads, S == ST_F64 ? 2 : 1) band_kernel
     __syncwarp();
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                     "r"(kBandTmemCols)
+                     "r"(BS::TmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     // inputs: (u_x, u_y, rho) of each neighbour cast to float (mesh.cpp:2805-2808);
-    // thread t < 5 kBandNodes fills inputs 3 q .. 3 q + 2 of node t / 5 (q =
-    // t % 5), the next kBandNodes threads the zero padding (input 15)
-    static_assert(kBandIn == 16 && 6 * kBandNodes <= kBandThreads, "input staging");
+    // item i < 5 NB fills inputs 3 q .. 3 q + 2 of node i / 5 (q =
+    // i % 5), the next NB items the zero padding (input 15)
+    static_assert(kBandIn == 16, "input staging");
     // prep_kernel's moments and populations: complete once its grid is (a
     // no-op without a programmatic primary)
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    if (tid < 5 * kBandNodes) {
-        const int n = tid / 5, q = tid % 5;
-        const int code = __ldg(ba.in_slot + (size_t)blockIdx.x * kBandNodes * 5 + tid);
-        float v[3] = {0.f, 0.f, 0.f};
-        if (code >= 0) {
-            const C* mm = ((code & 1) ? sm_old : sm_cur) + (long long)(code >> 1) * 3;
-            v[0] = float(mm[1]);
-            v[1] = float(mm[2]);
-            v[2] = float(mm[0]);
-        }
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            __half hi, lo;
-            f16_split(v[c], hi, lo);
-            *reinterpret_cast<__half*>(band_smem + kBandSmAH + band_a_offset(n, 3 * q + c)) = hi;
-            *reinterpret_cast<__half*>(band_smem + kBandSmAL + band_a_offset(n, 3 * q + c)) = lo;
+    for (int i = tid; i < 6 * NB; i += kBandThreads) {
+        if (i < 5 * NB) {
+            const int n = i / 5, q = i % 5;
+            const int code = __ldg(ba.in_slot + (size_t)blockIdx.x * NB * 5 + i);
+            float v[3] = {0.f, 0.f, 0.f};
+            if (code >= 0) {
+                const C* mm = ((code & 1) ? sm_old : sm_cur) + (long long)(code >> 1) * 3;
+                v[0] = float(mm[1]);
+                v[1] = float(mm[2]);
+                v[2] = float(mm[0]);
+            }
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                __half hi, lo;
+                f16_split(v[c], hi, lo);
+                *reinterpret_cast<__half*>(band_smem + BS::SmAH + BS::a_offset(n, 3 * q + c)) = hi;
+                *reinterpret_cast<__half*>(band_smem + BS::SmAL + BS::a_offset(n, 3 * q + c)) = lo;
+            }
+        } else {
+            const int n = i - 5 * NB;
+            *reinterpret_cast<__half*>(band_smem + BS::SmAH + BS::a_offset(n, 15)) = __float2half_rn(0.f);
+            *reinterpret_cast<__half*>(band_smem + BS::SmAL + BS::a_offset(n, 15)) = __float2half_rn(0.f);
         }
-    } else if (tid < 6 * kBandNodes) {
-        const int n = tid - 5 * kBandNodes;
-        *reinterpret_cast<__half*>(band_smem + kBandSmAH + band_a_offset(n, 15)) = __float2half_rn(0.f);
-        *reinterpret_cast<__half*>(band_smem + kBandSmAL + band_a_offset(n, 15)) = __float2half_rn(0.f);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
@@ -1056,8 +1084,8 @@ __global__ void __launch_bounds__(kBandThreads, S == ST_F64 ? 2 : 1) band_kernel
 
     bool ok = true;
     const int qd = warp & 3, k = 32 * qd + lane;  // this thread's output feature in the epilogue
-    const int nb = 12 * (warp >> 2);              // and its first node
-    const uint32_t trow = tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)nb;
+    const int nb0 = BS::WarpNodes * (warp >> 2);  // and its first node
+    const uint32_t trow0 = tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)nb0;
     const float wo = __ldg(w32 + kBandF32Wo + k);
     float bias = __ldg(w32 + kBandF32B1 + k);
 #pragma unroll 1
@@ -1068,7 +1096,7 @@ __global__ void __launch_bounds__(kBandThreads, S == ST_F64 ? 2 : 1) band_kernel
         if (tid == 0) {
             ok = band_wait(&bar[b], (l >> 1) & 1) && ok;
             tc_fence_after();
-            band_layer_mma(tmem, sb + b * kBandSmWBuf, sb + kBandSmAH, sb + kBandSmAL,
+            band_layer_mma<NB>(tmem, sb + b * kBandSmWBuf, sb + BS::SmAH, sb + BS::SmAL,
                            l == 0 ? kBandIn / 16 : kHidden / 16, &bar[2]);
             if (l + 2 < 7) {
                 // layer l + 2 into this buffer once the products here are done
@@ -1084,55 +1112,59 @@ __global__ void __launch_bounds__(kBandThreads, S == ST_F64 ? 2 : 1) band_kernel
         // epilogue: bias + the three accumulators, ReLU; split into the next
         // layer's activation planes, or (last layer) the output layer's
         // partial sums over this warp's 32 features
-        uint32_t r[3][3][4];
+#pragma unroll 1
+        for (int h = 0; h < BS::WarpNodes / 12; h++) {
+            const int nb = nb0 + 12 * h;
+            const uint32_t trow = trow0 + 12u * (uint32_t)h;
+            uint32_t r[3][3][4];
 #pragma unroll
-        for (int p = 0; p < 3; p++)
+            for (int p = 0; p < 3; p++)
 #pragma unroll
-            for (int c = 0; c < 3; c++) tmem_ld4(trow + 64u * (uint32_t)c + 4u * (uint32_t)p, r[p][c]);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        float v[16];
+                for (int c = 0; c < 3; c++) tmem_ld4(trow + BS::Acc * (uint32_t)c + 4u * (uint32_t)p, r[p][c]);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            float v[16];
 #pragma unroll
-        for (int p = 0; p < 3; p++)
+            for (int p = 0; p < 3; p++)
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                float x = bias + __uint_as_float(r[p][0][j]);
-                if (l > 0) x += __uint_as_float(r[p][1][j]);
-                v[4 * p + j] = fmaxf(fmaf(__uint_as_float(r[p][2][j]), 1.f / kBandLoScale, x), 0.f);
-            }
-        if (l < 6) {
-#pragma unroll
-            for (int j = 0; j < 12; j++) {
-                __half hi, lo;
-                f16_split(v[j], hi, lo);
-                *reinterpret_cast<__half*>(band_smem + kBandSmAH + band_a_offset(nb + j, k)) = hi;
-                *reinterpret_cast<__half*>(band_smem + kBandSmAL + band_a_offset(nb + j, k)) = lo;
-            }
-        } else {
-            // output layer: the warp's 32 features of v * wo summed per node
-            // by a reduce-scatter (lane L ends with node L % 16)
-#pragma unroll
-            for (int j = 0; j < 16; j++) v[j] = j < 12 ? v[j] * wo : 0.f;
-#pragma unroll
-            for (int o = 8; o >= 1; o >>= 1) {
-                const bool up = lane & o;
-#pragma unroll
-                for (int i = 0; i < o; i++) {
-                    const float send = up ? v[i] : v[i + o];
-                    const float keep = up ? v[i + o] : v[i];
-                    v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+                for (int j = 0; j < 4; j++) {
+                    float x = bias + __uint_as_float(r[p][0][j]);
+                    if (l > 0) x += __uint_as_float(r[p][1][j]);
+                    v[4 * p + j] = fmaxf(fmaf(__uint_as_float(r[p][2][j]), 1.f / kBandLoScale, x), 0.f);
                 }
+            if (l < 6) {
+#pragma unroll
+                for (int j = 0; j < 12; j++) {
+                    __half hi, lo;
+                    f16_split(v[j], hi, lo);
+                    *reinterpret_cast<__half*>(band_smem + BS::SmAH + BS::a_offset(nb + j, k)) = hi;
+                    *reinterpret_cast<__half*>(band_smem + BS::SmAL + BS::a_offset(nb + j, k)) = lo;
+                }
+            } else {
+                // output layer: the warp's 32 features of v * wo summed per
+                // node by a reduce-scatter (lane L ends with node L % 16)
+#pragma unroll
+                for (int j = 0; j < 16; j++) v[j] = j < 12 ? v[j] * wo : 0.f;
+#pragma unroll
+                for (int o = 8; o >= 1; o >>= 1) {
+                    const bool up = lane & o;
+#pragma unroll
+                    for (int i = 0; i < o; i++) {
+                        const float send = up ? v[i] : v[i + o];
+                        const float keep = up ? v[i + o] : v[i];
+                        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+                    }
+                }
+                v[0] += __shfl_xor_sync(0xffffffffu, v[0], 16);
+                if (lane < 12) red[qd * NB + nb + lane] = v[0];
             }
-            v[0] += __shfl_xor_sync(0xffffffffu, v[0], 16);
-            if (lane < 12) red[qd * kBandNodes + nb + lane] = v[0];
         }
         bias = bias_next;
         tc_fence_before();
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
     }
-    if (tid < kBandNodes)
-        outv[tid] = ((red[tid] + red[kBandNodes + tid]) + (red[2 * kBandNodes + tid] + red[3 * kBandNodes + tid])) +
-                    net.bo;
+    for (int n = tid; n < NB; n += kBandThreads)
+        outv[n] = ((red[n] + red[NB + n]) + (red[2 * NB + n] + red[3 * NB + n])) + net.bo;
     if (!ok && tid == 0) {
         // a wait ran out: report it, and give what may still be in flight one
         // more bounded wait before the tensor memory is freed
@@ -1144,7 +1176,7 @@ __global__ void __launch_bounds__(kBandThreads, S == ST_F64 ? 2 : 1) band_kernel
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kBandTmemCols)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BS::TmemCols)
                      : "memory");
     }
 
