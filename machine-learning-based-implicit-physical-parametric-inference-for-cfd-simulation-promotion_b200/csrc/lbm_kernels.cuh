@@ -1001,8 +1001,8 @@ __device__ __forceinline__ void band_layer_mma(uint32_t tmem, uint32_t wb, uint3
 
 // (FP64 storage: 2 in the launch bounds caps the kernel at 64 registers, so a
 // band block leaves room for four of the bulk kernel's longer FP64 blocks on
-// its SM -- plate step 47.1 -> 45.4 us; the FP32 step is faster at 72
-// registers, 29.4 against 30.5 us.  Shared memory keeps band blocks one per SM.)
+// its SM; the FP32-class instances keep their registers, as the nets are the
+// longer leg there.  Shared memory keeps band blocks one per SM.)
 template <int S, int CO>
 __global__ void __launch_bounds__(kBandThreads, S == ST_F64 ? 2 : 1) band_kernel(const BandArgs ba)
 {
