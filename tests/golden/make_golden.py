@@ -1,6 +1,7 @@
 """Generate the committed golden fixtures under tests/golden/.
 
-Run here, where the reference project is mounted (default /root/reference):
+Run where the reference project is mounted (the root is the argument, else
+$IPPI_REFERENCE_DIR, else the reference's mount point /root/reference):
 
     python tests/golden/make_golden.py [reference-root]
 
@@ -169,7 +170,7 @@ def ib_golden():
 
 def main():
     refroot = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("IPPI_REFERENCE_DIR",
-                                                                   "/root/reference")
+                                                                   "/root/reference")  # its mount point
     import pyoracle as po
 
     nets = export_nets(refroot)
