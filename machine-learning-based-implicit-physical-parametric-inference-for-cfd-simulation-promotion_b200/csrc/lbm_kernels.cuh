@@ -825,7 +825,9 @@ constexpr int kBandSmWBuf = 2 * kBandSmWPlane;
 
 // Band nodes per block, N of each product: 96 with FP64 storage (there the
 // bulk step is the longer leg, and fewer band blocks leave it more of the
-// GPU), 48 otherwise (there the nets are the longer leg).
+// GPU), 48 otherwise (there the nets are the longer leg; on the 2401 x 501
+// plate 64 and 96 nodes per block made the FP32 step 30.1 and 34.2 us
+// against 29.5).
 __host__ __device__ constexpr int band_nodes(int storage) { return storage == ST_F64 ? 96 : 48; }
 
 // The block's layout for N = NB nodes.
@@ -850,13 +852,14 @@ struct BandShape {
     static constexpr uint32_t TmemCols = NB <= 64 ? 256 : 512;
     static constexpr uint32_t AccSmall = 2 * Acc;
     // the epilogue: warp w takes features 32 (w % 4) .. of nodes WarpNodes
-    // (w / 4) .., in chunks of 12
+    // (w / 4) .., in chunks of Chunk (at most 16: one reduce-scatter)
     static constexpr int WarpNodes = NB / 4;
+    static constexpr int Chunk = WarpNodes <= 16 ? WarpNodes : 12;
     // instruction descriptor (kind::f16): D F32 (bit 4), A and B F16 (0 at
     // bits 7, 10), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
     static constexpr uint32_t Idesc = (1u << 4) | ((uint32_t)(NB >> 3) << 17) | ((uint32_t)(kHidden >> 4) << 24);
     static_assert(NB % 16 == 0 && NB <= 128, "tcgen05 N, accumulators Acc columns apart");
-    static_assert(WarpNodes % 12 == 0, "epilogue chunks");
+    static_assert(WarpNodes % Chunk == 0 && Chunk % 4 == 0, "epilogue chunks");
     static_assert(ActPlane % 16 == 0 && SmBar % 8 == 0, "band_kernel shared-memory layout");
     static_assert(SmemBytes <= 227 * 1024, "band_kernel shared memory");
     static_assert(SmemBytes > 114 * 1024, "one band block per SM: two would share tensor memory");
@@ -1112,19 +1115,20 @@ __global__ void __launch_bounds__(kBandThreads, S == ST_F64 ? 2 : 1) band_kernel
         // epilogue: bias + the three accumulators, ReLU; split into the next
         // layer's activation planes, or (last layer) the output layer's
         // partial sums over this warp's 32 features
+        constexpr int CH = BS::Chunk, NP = CH / 4;
 #pragma unroll 1
-        for (int h = 0; h < BS::WarpNodes / 12; h++) {
-            const int nb = nb0 + 12 * h;
-            const uint32_t trow = trow0 + 12u * (uint32_t)h;
-            uint32_t r[3][3][4];
+        for (int h = 0; h < BS::WarpNodes / CH; h++) {
+            const int nb = nb0 + CH * h;
+            const uint32_t trow = trow0 + (uint32_t)(CH * h);
+            uint32_t r[NP][3][4];
 #pragma unroll
-            for (int p = 0; p < 3; p++)
+            for (int p = 0; p < NP; p++)
 #pragma unroll
                 for (int c = 0; c < 3; c++) tmem_ld4(trow + BS::Acc * (uint32_t)c + 4u * (uint32_t)p, r[p][c]);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             float v[16];
 #pragma unroll
-            for (int p = 0; p < 3; p++)
+            for (int p = 0; p < NP; p++)
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     float x = bias + __uint_as_float(r[p][0][j]);
@@ -1133,7 +1137,7 @@ __global__ void __launch_bounds__(kBandThreads, S == ST_F64 ? 2 : 1) band_kernel
                 }
             if (l < 6) {
 #pragma unroll
-                for (int j = 0; j < 12; j++) {
+                for (int j = 0; j < CH; j++) {
                     __half hi, lo;
                     f16_split(v[j], hi, lo);
                     *reinterpret_cast<__half*>(band_smem + BS::SmAH + BS::a_offset(nb + j, k)) = hi;
@@ -1143,7 +1147,7 @@ __global__ void __launch_bounds__(kBandThreads, S == ST_F64 ? 2 : 1) band_kernel
                 // output layer: the warp's 32 features of v * wo summed per
                 // node by a reduce-scatter (lane L ends with node L % 16)
 #pragma unroll
-                for (int j = 0; j < 16; j++) v[j] = j < 12 ? v[j] * wo : 0.f;
+                for (int j = 0; j < 16; j++) v[j] = j < CH ? v[j] * wo : 0.f;
 #pragma unroll
                 for (int o = 8; o >= 1; o >>= 1) {
                     const bool up = lane & o;
@@ -1155,7 +1159,7 @@ __global__ void __launch_bounds__(kBandThreads, S == ST_F64 ? 2 : 1) band_kernel
                     }
                 }
                 v[0] += __shfl_xor_sync(0xffffffffu, v[0], 16);
-                if (lane < 12) red[qd * NB + nb + lane] = v[0];
+                if (lane < CH) red[qd * NB + nb + lane] = v[0];
             }
         }
         bias = bias_next;
