@@ -825,9 +825,9 @@ constexpr int kBandSmWBuf = 2 * kBandSmWPlane;
 
 // Band nodes per block, N of each product: 96 with FP64 storage (there the
 // bulk step is the longer leg, and fewer band blocks leave it more of the
-// GPU), 48 otherwise (there the nets are the longer leg; on the 2401 x 501
+// GPU), 48 otherwise (there the nets are the longer leg).  On the 2401 x 501
 // plate 64 and 96 nodes per block made the FP32 step 30.1 and 34.2 us
-// against 29.5).
+// against 29.5; 48 and 128 made the FP64 step 45.4 and 44.2 us against 41.0.
 __host__ __device__ constexpr int band_nodes(int storage) { return storage == ST_F64 ? 96 : 48; }
 
 // The block's layout for N = NB nodes.
@@ -854,7 +854,7 @@ struct BandShape {
     // the epilogue: warp w takes features 32 (w % 4) .. of nodes WarpNodes
     // (w / 4) .., in chunks of Chunk (at most 16: one reduce-scatter)
     static constexpr int WarpNodes = NB / 4;
-    static constexpr int Chunk = WarpNodes <= 16 ? WarpNodes : 12;
+    static constexpr int Chunk = WarpNodes <= 16 ? WarpNodes : (WarpNodes % 16 == 0 ? 16 : 12);
     // instruction descriptor (kind::f16): D F32 (bit 4), A and B F16 (0 at
     // bits 7, 10), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
     static constexpr uint32_t Idesc = (1u << 4) | ((uint32_t)(NB >> 3) << 17) | ((uint32_t)(kHidden >> 4) << 24);
