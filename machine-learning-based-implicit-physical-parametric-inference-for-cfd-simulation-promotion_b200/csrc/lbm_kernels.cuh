@@ -1169,9 +1169,9 @@ __global__ void __launch_bounds__(kBandThreads, S == ST_F64 ? 2 : 1) band_kernel
     }
     for (int n = tid; n < NB; n += kBandThreads)
         outv[n] = ((red[n] + red[NB + n]) + (red[2 * NB + n] + red[3 * NB + n])) + net.bo;
-    if (!ok && tid == 0) {
-        // a wait ran out: report it, and give what may still be in flight one
-        // more bounded wait before the tensor memory is freed
+    if (__syncthreads_or(!ok) && tid == 0) {
+        // a wait of some thread ran out: report it, and give what may still
+        // be in flight one more bounded wait before the tensor memory is freed
         atomicExch(&a.ctr->err, 3);
         band_wait(&bar[2], 0);
         band_wait(&bar[0], 1);
